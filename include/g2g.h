@@ -1,0 +1,130 @@
+/*
+ * g2g C ABI of the B200 XC grid-integration library (lio_b200/libg2g_b200.so).
+ *
+ * The first block is the entry-point set lioamber's Fortran SCF/TD drivers bind
+ * (Fortran name mangling: lower case + trailing underscore, every scalar passed
+ * by reference, `bool` is one byte read from a Fortran LOGICAL). Each entry
+ * cites the reference function it replaces; argument meaning, array layouts and
+ * output semantics are the reference's:
+ *   - the caller owns every array; the library keeps the pointers it is given
+ *     at g2g_parameter_init_ and re-reads the density at every solve;
+ *   - the Kohn-Sham (Fock) output is ACCUMULATED (+=) into the caller's packed
+ *     vector(s); the energy is OVERWRITTEN;
+ *   - packed storage is the lower triangle in Fortran 'L' order, packed index
+ *     of 0-based (i <= j) = i*M - i*(i-1)/2 + (j-i); densities carry doubled
+ *     off-diagonal elements, Fock vectors do not.
+ * The library never throws or exits across this boundary: failures set a sticky
+ * status readable through g2g_last_error_ (an addition; the reference throws
+ * std::runtime_error or calls exit(1)).
+ *
+ * The second block holds additions with no counterpart in the reference ABI.
+ */
+#ifndef LIO_B200_G2G_H
+#define LIO_B200_G2G_H
+
+#ifdef __cplusplus
+#include <cstddef>
+extern "C" {
+#else
+#include <stdbool.h>
+#include <stddef.h>
+#endif
+
+/* ---- entry points of the reference ABI ---------------------------------- */
+
+/* g2g/init.cpp:38-61 (g2g_init_): device discovery. */
+void g2g_init_(void);
+
+/* g2g/init.cpp:409-433 (g2g_set_options_): free_global_memory, little_cube_size,
+ * sphere_radius, assign_all_functions, energy_all_iterations,
+ * remove_zero_weights, min_points_per_cube, max_function_exponent, timer level,
+ * verbose. */
+void g2g_set_options_(double* fort_fgm, double* fort_lcs, double* fort_sr,
+                      bool* fort_aaf, bool* fort_eai, bool* fort_rzw,
+                      unsigned int* fort_mppc, unsigned int* fort_mfe,
+                      unsigned int* fort_time, unsigned int* fort_verbose);
+
+/* g2g/init.cpp:69-219 (g2g_parameter_init_): binds the caller's arrays.
+ * r: natom x 3 column-major, leading dimension max_atoms (bohr).
+ * Rm, Nr, Nr2: indexed by atomic number (0..54). Iz, Nuc, ncont: 1-based.
+ * c, a: M x 13 column-major, leading dimension ngaussians.
+ * nshell[0] = #s, nshell[1] = 3 * #p, nshell[2] = 6 * #d.
+ * e/e2/e3: 50/116/194 x 3 column-major angular directions; wang/wang2/wang3
+ * their weights (already multiplied by 4*pi). */
+void g2g_parameter_init_(const unsigned int* norm, const unsigned int* natom,
+                         const unsigned int* max_atoms, const unsigned int* ngaussians,
+                         double* r, double* Rm, const unsigned int* Iz,
+                         const unsigned int* Nr, const unsigned int* Nr2,
+                         unsigned int* Nuc, const unsigned int* M, unsigned int* ncont,
+                         const unsigned int* nshell, double* c, double* a,
+                         double* rho_vec, double* fock_vec, double* fockb_vec,
+                         double* rhoalpha, double* rhobeta, const unsigned int* nco,
+                         bool* OPEN, const unsigned int* nunp, const unsigned int* nopt,
+                         const unsigned int* Iexch, double* e, double* e2, double* e3,
+                         double* wang, double* wang2, double* wang3, bool* use_libxc,
+                         const unsigned int* ex_functional_id,
+                         const unsigned int* ec_functional_id);
+
+/* g2g/init.cpp:282-306 (g2g_reload_atom_positions_): re-reads the positions
+ * and rebuilds the grid partition for grid_type (0/1/2 -> 50/116/194 points;
+ * types >= 3 are tables registered with g2g_set_angular_grid_). */
+void g2g_reload_atom_positions_(const unsigned int* grid_type);
+
+/* g2g/init.cpp:308-315 (g2g_new_grid_): rebuilds only if grid_type changed. */
+void g2g_new_grid_(const unsigned int* grid_type);
+
+/* g2g/init.cpp:332-391 (g2g_solve_groups_): computation_type 0 = Fock (RMM)
+ * update, 1 = energy only, 2 = energy + forces, 3 = forces only. */
+void g2g_solve_groups_(const unsigned int* computation_type, double* fort_energy_ptr,
+                       double* fort_forces_ptr);
+
+/* g2g/init.cpp:221-236 (g2g_deinit_): releases the partition and device state. */
+void g2g_deinit_(void);
+
+/* g2g/timer.cpp:125-296: Fortran-named timers (hidden length argument). */
+void g2g_timer_start_(const char* timer_name, unsigned int length_arg);
+void g2g_timer_stop_(const char* timer_name, unsigned int length_arg);
+void g2g_timer_pause_(const char* timer_name, unsigned int length_arg);
+void g2g_timer_sum_start_(const char* timer_name, unsigned int length_arg);
+void g2g_timer_sum_stop_(const char* timer_name, unsigned int length_arg);
+void g2g_timer_sum_pause_(const char* timer_name, unsigned int length_arg);
+void g2g_timer_clear_(void);
+void g2g_timer_summary_(void);
+
+/* ---- additions (no counterpart in the reference ABI) --------------------- */
+
+/* Sticky status of the last failing call: 0 = ok. Copies up to len-1 bytes of
+ * the message into msg (NUL-terminated) when msg != NULL. Reading clears it. */
+int g2g_last_error_(char* msg, const unsigned int* len);
+
+/* Registers an angular table for grid_type >= 3 (e: npoints x 3 column-major
+ * unit directions, wang: weights summing to 4*pi); such grid types use the
+ * Nr2 radial shell counts, as grid types 1 and 2 do. The reference supports
+ * only its three compiled-in tables (g2g/init.h:10-14, g2g/init.cpp:238-266). */
+void g2g_set_angular_grid_(const unsigned int* grid_type, const unsigned int* npoints,
+                           const double* e, const double* wang);
+
+/* Arithmetic of the two contractions (density and Kohn-Sham update):
+ * 0 = FP64 on the CUDA cores (the plain form), 1 = tensor-core form. */
+void g2g_set_precision_(const unsigned int* mode);
+
+/* Partition statistics of the current grid: out[0] = groups, out[1] = cubes,
+ * out[2] = spheres, out[3] = points kept, out[4] = sum over groups of
+ * points * functions, out[5] = sum of points * functions^2. */
+void g2g_partition_stats_(long long* out);
+
+/* Copies group g of the current partition (groups numbered cubes first, then
+ * spheres, each in cost order): meta[0..7] = points, simple functions, s, p, d,
+ * total functions, nuclei, is_sphere; when non-NULL, ids (points x 3: atom,
+ * shell, angular point), xyzw (points x 4: x, y, z, weight), funcs (simple
+ * functions, 0-based global index of the first component). Returns 0 or -1. */
+int g2g_partition_group_(const int* g, int* meta, int* ids, double* xyzw, int* funcs);
+
+/* Device time of the last g2g_solve_groups_ (ms, CUDA events around the
+ * device work) and of the last partition build (ms, host clock). */
+void g2g_last_timings_(double* solve_ms, double* grid_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LIO_B200_G2G_H */

@@ -1,0 +1,685 @@
+// Device engine: HBM layout, kernels and per-solve orchestration (FP64 form).
+//
+// HBM layout of one molecule (built once per geometry by upload()):
+//   groups[]      GroupDev records, cubes first then spheres (cost order)
+//   px/py/pz/pw   point coordinates and weights, each group padded to ldp
+//                 (a multiple of 64) slots; padded slots have weight 0
+//   fn_glob[]     per group, the global (expanded) index of every local function
+//   sf_glob/type  per group, its simple functions (s, p shell, d shell)
+//   basis cache   per group NK x m x ldp doubles, function-major (points
+//                 contiguous): NK = 1 (F) for LDA, 10 for GGA
+//                 (F, dx, dy, dz, dxx, dyy, dzz, dxy, dxz, dyz)
+// Per solve: packed density(ies) uploaded, partial densities per
+// (function tile, quantity, point), per-point factors w*v_xc, the packed
+// Kohn-Sham accumulator (FP64) and per-block energy partials.
+//
+// Math (g2g/cpu/iteration.cpp:90-291 restated as GEMMs): with D the dense
+// symmetric group density (packed value, halved off the diagonal),
+//   G = F D, Ga = (dF/da) D                               (tensor-shaped)
+//   rho = sum_i F_i G_i, d rho/da = 2 sum_i dF_i/da G_i,
+//   d2 rho/da db = 2 sum_i (d2F_i/da db G_i + dF_i/da Gb_i)  (row-dot epilogue)
+//   K_ij += sum_p F_ip (w_p v_p) F_jp                      (tensor-shaped)
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "xc_functionals.cuh"
+
+namespace lio {
+
+#define LIO_CUDA(x)                                                                           \
+  do {                                                                                        \
+    cudaError_t err_ = (x);                                                                   \
+    if (err_ != cudaSuccess)                                                                  \
+      throw std::runtime_error(std::string("CUDA error ") + cudaGetErrorString(err_) + " at " + \
+                               __FILE__ + ":" + std::to_string(__LINE__));                    \
+  } while (0)
+
+namespace {
+
+constexpr int kTile = 64;    // points / functions per GEMM tile
+constexpr int kKStep = 16;   // reduction step of the FP64 GEMMs
+constexpr int kBasisBlock = 128;
+constexpr int kFuncBlock = 128;
+constexpr int kNQ = 10;      // rho, grad[3], (xx,yy,zz), (xy,xz,yz)
+
+struct GroupDev {
+  int npts, ldp, m, nsimple;
+  int nft, pad0, pad1, pad2;
+  long long pt_off;    // point arrays
+  long long fn_off;    // fn_glob
+  long long sf_off;    // sf_glob / sf_type
+  long long bas_off;   // basis cache (elements)
+  long long part_off;  // partial densities (elements, one spin)
+};
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    free();
+    if (count == 0) count = 1;
+    LIO_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    n = count;
+  }
+  void upload(const std::vector<T>& v) {
+    alloc(v.size());
+    if (!v.empty()) LIO_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  }
+  void free() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DevBuf() { free(); }
+};
+
+__device__ __forceinline__ long long packed_index(int gi, int gj, int M) {
+  const long long lo = gi < gj ? gi : gj, hi = gi < gj ? gj : gi;
+  return lo * M - (lo * (lo - 1)) / 2 + (hi - lo);
+}
+
+// ------------------------------------------------------------------ basis values
+// Cartesian component exponents: s; p x,y,z; d xx,xy,yy,xz,yz,zz
+__constant__ int c_comp_l[10][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {2, 0, 0},
+                                    {1, 1, 0}, {0, 2, 0}, {1, 0, 1}, {0, 1, 1}, {0, 0, 2}};
+
+__device__ __forceinline__ double ipow(double x, int n) { return n == 0 ? 1.0 : (n == 1 ? x : x * x); }
+__device__ __forceinline__ double dpow(double x, int n) {  // d/dx x^n
+  return n == 0 ? 0.0 : (n == 1 ? 1.0 : 2.0 * x);
+}
+__device__ __forceinline__ double d2pow(int n) { return n == 2 ? 2.0 : 0.0; }
+
+// One thread per (group, point). For every simple function of the group the
+// contracted radial part t = sum_k c_k exp(-a_k r^2) (primitives with
+// a_k r^2 > 70 skipped, g2g/cpu/functions.cpp:68-79), tg = sum a_k t_k and
+// th = sum a_k^2 t_k give, for the monomial P = x^lx y^ly z^lz,
+//   F = P t,  dF/da = P_a t - 2 r_a P tg,
+//   d2F/da db = P_ab t - 2 (r_b P_a + r_a P_b + delta_ab P) tg + 4 r_a r_b P th,
+// the closed forms of g2g/cpu/functions.cpp:81-352; d xx/yy/zz carry dnorm.
+__global__ void k_basis(const int2* __restrict__ tiles, const GroupDev* __restrict__ groups,
+                        const double* __restrict__ px, const double* __restrict__ py,
+                        const double* __restrict__ pz, const int* __restrict__ sf_glob,
+                        const int* __restrict__ sf_type, const int* __restrict__ nuc,
+                        const int* __restrict__ ncont, const double* __restrict__ ca,
+                        const double* __restrict__ cc, const double* __restrict__ ax,
+                        const double* __restrict__ ay, const double* __restrict__ az, double dnorm,
+                        int gga, double* __restrict__ basis) {
+  const int2 t = tiles[blockIdx.x];
+  const GroupDev G = groups[t.x];
+  const int p = t.y * kBasisBlock + threadIdx.x;
+  if (p >= G.ldp) return;
+  const bool valid = p < G.npts;
+  const double x = px[G.pt_off + p], y = py[G.pt_off + p], z = pz[G.pt_off + p];
+  double* out = basis + G.bas_off;
+  const long long kstride = (long long)G.m * G.ldp;
+  int ii = 0;
+  for (int sf = 0; sf < G.nsimple; sf++) {
+    const int gf = sf_glob[G.sf_off + sf];
+    const int type = sf_type[G.sf_off + sf];
+    const int atom = nuc[gf];
+    const double r[3] = {x - ax[atom], y - ay[atom], z - az[atom]};
+    const double dist = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    double tt = 0.0, tg = 0.0, th = 0.0;
+    const int nc = ncont[gf];
+    for (int k = 0; k < nc; k++) {
+      const double a = ca[gf * 13 + k], c = cc[gf * 13 + k];
+      const double expo = a * dist;
+      if (expo > 70.0) continue;
+      const double t0 = exp(-expo) * c;
+      tt += t0;
+      tg += t0 * a;
+      th += t0 * (a * a);
+    }
+    const int c0 = type == 0 ? 0 : (type == 1 ? 1 : 4);
+    const int nc_comp = type == 0 ? 1 : (type == 1 ? 3 : 6);
+    for (int q = 0; q < nc_comp; q++, ii++) {
+      const int* l = c_comp_l[c0 + q];
+      const double scale = (type == 2 && (q == 0 || q == 2 || q == 5)) ? dnorm : 1.0;
+      const double P = ipow(r[0], l[0]) * ipow(r[1], l[1]) * ipow(r[2], l[2]);
+      const long long o = (long long)ii * G.ldp + p;
+      out[o] = valid ? scale * P * tt : 0.0;
+      if (!gga) continue;
+      double Pa[3];
+      Pa[0] = dpow(r[0], l[0]) * ipow(r[1], l[1]) * ipow(r[2], l[2]);
+      Pa[1] = ipow(r[0], l[0]) * dpow(r[1], l[1]) * ipow(r[2], l[2]);
+      Pa[2] = ipow(r[0], l[0]) * ipow(r[1], l[1]) * dpow(r[2], l[2]);
+      for (int a = 0; a < 3; a++)
+        out[(1 + a) * kstride + o] = valid ? scale * (Pa[a] * tt - 2.0 * r[a] * P * tg) : 0.0;
+      // Hessian: (xx, yy, zz) then (xy, xz, yz)
+      const int ha[6] = {0, 1, 2, 0, 0, 1}, hb[6] = {0, 1, 2, 1, 2, 2};
+      for (int h = 0; h < 6; h++) {
+        const int a = ha[h], b = hb[h];
+        double Pab;
+        if (a == b) {
+          Pab = (a == 0 ? d2pow(l[0]) * ipow(r[1], l[1]) * ipow(r[2], l[2])
+                        : (a == 1 ? ipow(r[0], l[0]) * d2pow(l[1]) * ipow(r[2], l[2])
+                                  : ipow(r[0], l[0]) * ipow(r[1], l[1]) * d2pow(l[2])));
+        } else {
+          int e[3] = {0, 0, 0};
+          e[a] = 1;
+          e[b] = 1;
+          Pab = (e[0] ? dpow(r[0], l[0]) : ipow(r[0], l[0])) * (e[1] ? dpow(r[1], l[1]) : ipow(r[1], l[1])) *
+                (e[2] ? dpow(r[2], l[2]) : ipow(r[2], l[2]));
+        }
+        double v = Pab * tt - 2.0 * (r[b] * Pa[a] + r[a] * Pa[b] + (a == b ? P : 0.0)) * tg +
+                   4.0 * r[a] * r[b] * P * th;
+        out[(4 + h) * kstride + o] = valid ? scale * v : 0.0;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------- density (FP64 GEMMs)
+// Tile = (group, point tile, function tile); 256 threads, each 4 points x 4
+// functions of the 64 x 64 output, NA = 1 (LDA: G) or 4 (GGA: G, Gx, Gy, Gz).
+template <int NA>
+__global__ void __launch_bounds__(256) k_density_fp64(const int4* __restrict__ tiles,
+                                                      const GroupDev* __restrict__ groups,
+                                                      const int* __restrict__ fn_glob,
+                                                      const double* __restrict__ basis,
+                                                      const double* __restrict__ P, int M,
+                                                      double* __restrict__ partial) {
+  constexpr int NQ = NA == 1 ? 1 : kNQ;
+  __shared__ double As[NA][kKStep][kTile];
+  __shared__ double Bs[kKStep][kTile + 1];
+  const int4 t = tiles[blockIdx.x];
+  const GroupDev G = groups[t.x];
+  const int pt0 = t.y * kTile, ft = t.z, ft0 = ft * kTile;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const long long kstride = (long long)G.m * G.ldp;
+  const double* bas = basis + G.bas_off;
+  const int* fg = fn_glob + G.fn_off;
+  double acc[NA][4][4];
+#pragma unroll
+  for (int a = 0; a < NA; a++)
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+      for (int c = 0; c < 4; c++) acc[a][r][c] = 0.0;
+
+  for (int j0 = 0; j0 < G.m; j0 += kKStep) {
+#pragma unroll
+    for (int a = 0; a < NA; a++)
+#pragma unroll
+      for (int rr = 0; rr < 4; rr++) {
+        const int idx = tid + 256 * rr, kk = idx >> 6, pp = idx & 63;
+        const int j = j0 + kk;
+        As[a][kk][pp] = j < G.m ? bas[a * kstride + (long long)j * G.ldp + pt0 + pp] : 0.0;
+      }
+#pragma unroll
+    for (int rr = 0; rr < 4; rr++) {
+      const int idx = tid + 256 * rr, kk = idx >> 6, ii = idx & 63;
+      const int j = j0 + kk, i = ft0 + ii;
+      double v = 0.0;
+      if (j < G.m && i < G.m) {
+        const int gj = fg[j], gi = fg[i];
+        v = P[packed_index(gi, gj, M)];
+        if (gi != gj) v *= 0.5;
+      }
+      Bs[kk][ii] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kKStep; kk++) {
+      double b[4];
+#pragma unroll
+      for (int c = 0; c < 4; c++) b[c] = Bs[kk][tx + 16 * c];
+#pragma unroll
+      for (int a = 0; a < NA; a++)
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+          const double av = As[a][kk][ty + 16 * r];
+#pragma unroll
+          for (int c = 0; c < 4; c++) acc[a][r][c] = fma(av, b[c], acc[a][r][c]);
+        }
+    }
+    __syncthreads();
+  }
+
+  // row-dot epilogue
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int p = pt0 + ty + 16 * r;
+    double q[NQ];
+#pragma unroll
+    for (int k = 0; k < NQ; k++) q[k] = 0.0;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const int i = ft0 + tx + 16 * c;
+      if (i >= G.m) continue;
+      const long long o = (long long)i * G.ldp + p;
+      const double F = bas[o];
+      q[0] += F * acc[0][r][c];
+      if (NA == 4) {
+        const double gx = bas[kstride + o], gy = bas[2 * kstride + o], gz = bas[3 * kstride + o];
+        const double hxx = bas[4 * kstride + o], hyy = bas[5 * kstride + o], hzz = bas[6 * kstride + o];
+        const double hxy = bas[7 * kstride + o], hxz = bas[8 * kstride + o], hyz = bas[9 * kstride + o];
+        const double g0 = acc[0][r][c], gX = acc[NA > 1 ? 1 : 0][r][c], gY = acc[NA > 2 ? 2 : 0][r][c],
+                     gZ = acc[NA > 3 ? 3 : 0][r][c];
+        q[1] += 2.0 * gx * g0;
+        q[2] += 2.0 * gy * g0;
+        q[3] += 2.0 * gz * g0;
+        q[4] += 2.0 * (gx * gX + hxx * g0);
+        q[5] += 2.0 * (gy * gY + hyy * g0);
+        q[6] += 2.0 * (gz * gZ + hzz * g0);
+        q[7] += 2.0 * (gx * gY + hxy * g0);
+        q[8] += 2.0 * (gx * gZ + hxz * g0);
+        q[9] += 2.0 * (gy * gZ + hyz * g0);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < NQ; k++) {
+      double v = q[k];
+      v += __shfl_xor_sync(0xffffffffu, v, 8);
+      v += __shfl_xor_sync(0xffffffffu, v, 4);
+      v += __shfl_xor_sync(0xffffffffu, v, 2);
+      v += __shfl_xor_sync(0xffffffffu, v, 1);
+      q[k] = v;
+    }
+    if (tx == 0) {
+      double* dst = partial + G.part_off;
+#pragma unroll
+      for (int k = 0; k < NQ; k++) dst[((long long)ft * NQ + k) * G.ldp + p] = q[k];
+    }
+  }
+}
+
+// ------------------------------------------------------------- point functional
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  const int nw = blockDim.x >> 5;
+  v = threadIdx.x < nw ? sh[threadIdx.x] : 0.0;
+  if (w == 0)
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// One thread per point: reduce the function-tile partials, evaluate the
+// functional, write factor = w * v_xc, and a per-block energy sum of
+// rho * w * (ex + ec) (g2g/cpu/iteration.cpp:106-114, 199-208, 482-492).
+__global__ void k_functional(const int2* __restrict__ tiles, const GroupDev* __restrict__ groups,
+                             const double* __restrict__ pw, const double* __restrict__ part_a,
+                             const double* __restrict__ part_b, int lda, int open, int iexch,
+                             double* __restrict__ fac_a, double* __restrict__ fac_b,
+                             double* __restrict__ energy_blocks) {
+  __shared__ double sh[32];
+  const int2 t = tiles[blockIdx.x];
+  const GroupDev G = groups[t.x];
+  const int p = t.y * kFuncBlock + threadIdx.x;
+  double e = 0.0;
+  if (p < G.ldp) {
+    const double w = pw[G.pt_off + p];
+    const int NQ = lda ? 1 : kNQ;
+    double qa[kNQ], qb[kNQ];
+    for (int k = 0; k < kNQ; k++) qa[k] = qb[k] = 0.0;
+    for (int f = 0; f < G.nft; f++)
+      for (int k = 0; k < NQ; k++) {
+        const long long o = G.part_off + ((long long)f * NQ + k) * G.ldp + p;
+        qa[k] += part_a[o];
+        if (open) qb[k] += part_b[o];
+      }
+    double va = 0.0, vb = 0.0;
+    if (p < G.npts) {
+      if (open) {
+        if (!lda) {
+          const xc::GgaOpenOut o = xc::pbe_open(qa[0], qb[0], qa + 1, qb + 1, qa + 4, qb + 4, qa + 7, qb + 7);
+          e = ((qa[0] + qb[0]) * w) * (o.ex + o.ec);
+          va = w * o.va;
+          vb = w * o.vb;
+        }
+        // open-shell LDA: the reference CPU path has no branch for it
+        // (g2g/cpu/iteration.cpp:362-363); energy and potential stay zero.
+      } else if (lda) {
+        const xc::LdaOut o = xc::lda_closed(qa[0], iexch);
+        e = (qa[0] * w) * (o.ex + o.ec);
+        va = w * o.v;
+      } else {
+        const xc::GgaOut o = xc::pbe_closed(qa[0], qa + 1, qa + 4, qa + 7);
+        e = (qa[0] * w) * (o.ex + o.ec);
+        va = w * o.v;
+      }
+    }
+    fac_a[G.pt_off + p] = va;
+    if (open) fac_b[G.pt_off + p] = vb;
+  }
+  const double s = block_sum(e, sh);
+  if (threadIdx.x == 0) energy_blocks[blockIdx.x] = s;
+}
+
+__global__ void k_sum_blocks(const double* __restrict__ in, int n, double* __restrict__ out) {
+  __shared__ double sh[32];
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v += in[i];
+  v = block_sum(v, sh);
+  if (threadIdx.x == 0) *out = v;
+}
+
+// ------------------------------------------------ Kohn-Sham update (FP64 GEMM)
+// Tile = (group, i tile, j tile) with i tile <= j tile; K_ij = sum_p F_ip f_p F_jp
+// for i <= j, scattered with FP64 atomics into the packed accumulator(s).
+template <int NS>
+__global__ void __launch_bounds__(256) k_fock_fp64(const int4* __restrict__ tiles,
+                                                   const GroupDev* __restrict__ groups,
+                                                   const int* __restrict__ fn_glob,
+                                                   const double* __restrict__ basis,
+                                                   const double* __restrict__ fac_a,
+                                                   const double* __restrict__ fac_b, int M,
+                                                   double* __restrict__ K_a, double* __restrict__ K_b) {
+  __shared__ double As[kKStep][kTile + 1];
+  __shared__ double Bs[NS][kKStep][kTile + 1];
+  const int4 t = tiles[blockIdx.x];
+  const GroupDev G = groups[t.x];
+  const int i0 = t.y * kTile, j0 = t.z * kTile;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const double* F = basis + G.bas_off;
+  double acc[NS][4][4];
+#pragma unroll
+  for (int s = 0; s < NS; s++)
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+      for (int c = 0; c < 4; c++) acc[s][r][c] = 0.0;
+  for (int p0 = 0; p0 < G.ldp; p0 += kKStep) {
+#pragma unroll
+    for (int rr = 0; rr < 4; rr++) {
+      const int idx = tid + 256 * rr, row = idx >> 4, kk = idx & 15;
+      const int i = i0 + row, j = j0 + row, p = p0 + kk;
+      As[kk][row] = i < G.m ? F[(long long)i * G.ldp + p] : 0.0;
+      const double fj = j < G.m ? F[(long long)j * G.ldp + p] : 0.0;
+      Bs[0][kk][row] = fj * fac_a[G.pt_off + p];
+      if (NS == 2) Bs[NS - 1][kk][row] = fj * fac_b[G.pt_off + p];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kKStep; kk++) {
+      double av[4];
+#pragma unroll
+      for (int r = 0; r < 4; r++) av[r] = As[kk][ty + 16 * r];
+#pragma unroll
+      for (int s = 0; s < NS; s++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+          const double bv = Bs[s][kk][tx + 16 * c];
+#pragma unroll
+          for (int r = 0; r < 4; r++) acc[s][r][c] = fma(av[r], bv, acc[s][r][c]);
+        }
+    }
+    __syncthreads();
+  }
+  const int* fg = fn_glob + G.fn_off;
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int i = i0 + ty + 16 * r;
+    if (i >= G.m) continue;
+    const int gi = fg[i];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const int j = j0 + tx + 16 * c;
+      if (j >= G.m || (t.y == t.z && i > j)) continue;
+      const long long o = packed_index(gi, fg[j], M);
+      atomicAdd(K_a + o, acc[0][r][c]);
+      if (NS == 2) atomicAdd(K_b + o, acc[NS - 1][r][c]);
+    }
+  }
+}
+
+}  // namespace
+
+// ============================================================================ Impl
+struct DeviceEngine::Impl {
+  int M = 0, natoms = 0;
+  bool lda = false, open = false;
+  int iexch = 9;
+  int nk = 1;
+  long long npoints = 0, ngroups = 0, total_ldp = 0;
+  std::vector<GroupDev> hgroups;
+  DevBuf<GroupDev> groups;
+  DevBuf<double> px, py, pz, pw;
+  DevBuf<int> fn_glob, sf_glob, sf_type, nuc, ncont;
+  DevBuf<double> ca, cc, ax, ay, az;
+  DevBuf<double> basis;
+  DevBuf<int2> basis_tiles, func_tiles;
+  DevBuf<int4> dens_tiles, fock_tiles;
+  DevBuf<double> P_a, P_b, K_a, K_b, part_a, part_b, fac_a, fac_b, eblocks, energy;
+  std::vector<double> hK;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  Impl() {
+    LIO_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    LIO_CUDA(cudaEventCreate(&ev0));
+    LIO_CUDA(cudaEventCreate(&ev1));
+  }
+  ~Impl() {
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+DeviceEngine::DeviceEngine() : impl_(new Impl) {}
+
+bool DeviceEngine::available() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return n > 0;
+}
+DeviceEngine::~DeviceEngine() = default;
+
+void DeviceEngine::release() {
+  Impl* d = impl_.get();
+  d->basis.free();
+  d->part_a.free();
+  d->part_b.free();
+  d->ngroups = d->npoints = 0;
+}
+
+long long DeviceEngine::points() const { return impl_->npoints; }
+long long DeviceEngine::groups() const { return impl_->ngroups; }
+
+void DeviceEngine::upload(const System& sys, const Partition& part) {
+  Impl* d = impl_.get();
+  d->M = sys.M;
+  d->natoms = sys.natoms;
+  d->lda = sys.lda;
+  d->open = sys.open;
+  d->iexch = sys.iexch;
+  d->nk = sys.lda ? 1 : 10;
+  const int NQ = sys.lda ? 1 : kNQ;
+
+  std::vector<GroupDev> gd;
+  std::vector<double> hx, hy, hz, hw;
+  std::vector<int> hfn, hsf, hst;
+  std::vector<int2> btiles, ftiles;
+  std::vector<int4> dtiles, ktiles;
+  long long pt_off = 0, fn_off = 0, sf_off = 0, bas_off = 0, part_off = 0;
+  long long npts_total = 0;
+  const int ngr = part.total_groups();
+  for (int g = 0; g < ngr; g++) {
+    const PointGroup& pg = part.group(g);
+    GroupDev G{};
+    G.npts = (int)pg.points.size();
+    G.ldp = ((G.npts + kTile - 1) / kTile) * kTile;
+    G.m = pg.total_functions();
+    G.nsimple = (int)pg.funcs.size();
+    G.nft = (G.m + kTile - 1) / kTile;
+    G.pt_off = pt_off;
+    G.fn_off = fn_off;
+    G.sf_off = sf_off;
+    G.bas_off = bas_off;
+    G.part_off = part_off;
+    for (int p = 0; p < G.ldp; p++) {
+      if (p < G.npts) {
+        const GridPoint& q = pg.points[p];
+        hx.push_back(q.x);
+        hy.push_back(q.y);
+        hz.push_back(q.z);
+        hw.push_back(q.w);
+      } else {  // padded slot: a copy of the first point with zero weight
+        hx.push_back(pg.points[0].x);
+        hy.push_back(pg.points[0].y);
+        hz.push_back(pg.points[0].z);
+        hw.push_back(0.0);
+      }
+    }
+    for (size_t i = 0; i < pg.funcs.size(); i++) {
+      const int f = pg.funcs[i];
+      const int type = f < sys.s_funcs ? 0 : (f < sys.s_funcs + 3 * sys.p_funcs ? 1 : 2);
+      hsf.push_back(f);
+      hst.push_back(type);
+      const int ncomp = type == 0 ? 1 : (type == 1 ? 3 : 6);
+      for (int k = 0; k < ncomp; k++) hfn.push_back(f + k);
+    }
+    for (int b = 0; b < G.ldp / kBasisBlock + (G.ldp % kBasisBlock ? 1 : 0); b++) btiles.push_back({g, b});
+    for (int b = 0; b < (G.ldp + kFuncBlock - 1) / kFuncBlock; b++) ftiles.push_back({g, b});
+    for (int pt = 0; pt < G.ldp / kTile; pt++)
+      for (int ft = 0; ft < G.nft; ft++) dtiles.push_back({g, pt, ft, 0});
+    for (int it = 0; it < G.nft; it++)
+      for (int jt = it; jt < G.nft; jt++) ktiles.push_back({g, it, jt, 0});
+    pt_off += G.ldp;
+    fn_off += G.m;
+    sf_off += G.nsimple;
+    bas_off += (long long)d->nk * G.m * G.ldp;
+    part_off += (long long)G.nft * NQ * G.ldp;
+    npts_total += G.npts;
+    gd.push_back(G);
+  }
+  d->hgroups = gd;
+  d->ngroups = ngr;
+  d->npoints = npts_total;
+  d->total_ldp = pt_off;
+
+  std::vector<int> hnuc(sys.M), hnc(sys.M);
+  for (int i = 0; i < sys.M; i++) {
+    hnuc[i] = sys.nuc[i];
+    hnc[i] = sys.ncont[i];
+  }
+  d->groups.upload(gd);
+  d->px.upload(hx);
+  d->py.upload(hy);
+  d->pz.upload(hz);
+  d->pw.upload(hw);
+  d->fn_glob.upload(hfn);
+  d->sf_glob.upload(hsf);
+  d->sf_type.upload(hst);
+  d->nuc.upload(hnuc);
+  d->ncont.upload(hnc);
+  d->ca.upload(sys.a);
+  d->cc.upload(sys.c);
+  d->ax.upload(sys.ax);
+  d->ay.upload(sys.ay);
+  d->az.upload(sys.az);
+  d->basis_tiles.upload(btiles);
+  d->func_tiles.upload(ftiles);
+  d->dens_tiles.upload(dtiles);
+  d->fock_tiles.upload(ktiles);
+
+  const size_t npacked = (size_t)sys.M * (sys.M + 1) / 2;
+  d->P_a.alloc(npacked);
+  d->K_a.alloc(npacked);
+  d->part_a.alloc(part_off);
+  d->fac_a.alloc(pt_off);
+  if (sys.open) {
+    d->P_b.alloc(npacked);
+    d->K_b.alloc(npacked);
+    d->part_b.alloc(part_off);
+    d->fac_b.alloc(pt_off);
+  } else {
+    d->P_b.free();
+    d->K_b.free();
+    d->part_b.free();
+    d->fac_b.free();
+  }
+  d->eblocks.alloc(ftiles.size());
+  d->energy.alloc(1);
+  d->hK.resize(npacked);
+
+  // basis values, computed once per geometry and kept resident
+  d->basis.alloc(bas_off);
+  if (!btiles.empty()) {
+    k_basis<<<(unsigned)btiles.size(), kBasisBlock, 0, d->stream>>>(
+        d->basis_tiles.p, d->groups.p, d->px.p, d->py.p, d->pz.p, d->sf_glob.p, d->sf_type.p, d->nuc.p,
+        d->ncont.p, d->ca.p, d->cc.p, d->ax.p, d->ay.p, d->az.p, sys.d_norm, sys.lda ? 0 : 1, d->basis.p);
+    LIO_CUDA(cudaGetLastError());
+  }
+  LIO_CUDA(cudaStreamSynchronize(d->stream));
+}
+
+SolveResult DeviceEngine::solve(const SolveRequest& req) {
+  Impl* d = impl_.get();
+  SolveResult res;
+  const size_t npacked = (size_t)d->M * (d->M + 1) / 2;
+  if (d->ngroups == 0) return res;
+  cudaStream_t st = d->stream;
+  LIO_CUDA(cudaEventRecord(d->ev0, st));
+  if (d->open) {
+    LIO_CUDA(cudaMemcpyAsync(d->P_a.p, req.rho_a, npacked * sizeof(double), cudaMemcpyHostToDevice, st));
+    LIO_CUDA(cudaMemcpyAsync(d->P_b.p, req.rho_b, npacked * sizeof(double), cudaMemcpyHostToDevice, st));
+  } else {
+    LIO_CUDA(cudaMemcpyAsync(d->P_a.p, req.rho, npacked * sizeof(double), cudaMemcpyHostToDevice, st));
+  }
+  const unsigned nd = (unsigned)d->dens_tiles.n, nf = (unsigned)d->func_tiles.n,
+                 nk = (unsigned)d->fock_tiles.n;
+  const int nspin = d->open ? 2 : 1;
+  for (int s = 0; s < nspin; s++) {
+    const double* P = s == 0 ? d->P_a.p : d->P_b.p;
+    double* part = s == 0 ? d->part_a.p : d->part_b.p;
+    if (d->lda)
+      k_density_fp64<1><<<nd, 256, 0, st>>>(d->dens_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, P, d->M, part);
+    else
+      k_density_fp64<4><<<nd, 256, 0, st>>>(d->dens_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, P, d->M, part);
+    LIO_CUDA(cudaGetLastError());
+  }
+  k_functional<<<nf, kFuncBlock, 0, st>>>(d->func_tiles.p, d->groups.p, d->pw.p, d->part_a.p,
+                                          d->open ? d->part_b.p : nullptr, d->lda ? 1 : 0, d->open ? 1 : 0,
+                                          d->iexch, d->fac_a.p, d->open ? d->fac_b.p : nullptr, d->eblocks.p);
+  LIO_CUDA(cudaGetLastError());
+  k_sum_blocks<<<1, 1024, 0, st>>>(d->eblocks.p, (int)nf, d->energy.p);
+  LIO_CUDA(cudaGetLastError());
+  if (req.compute_rmm) {
+    LIO_CUDA(cudaMemsetAsync(d->K_a.p, 0, npacked * sizeof(double), st));
+    if (d->open) LIO_CUDA(cudaMemsetAsync(d->K_b.p, 0, npacked * sizeof(double), st));
+    if (d->open)
+      k_fock_fp64<2><<<nk, 256, 0, st>>>(d->fock_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, d->fac_a.p,
+                                         d->fac_b.p, d->M, d->K_a.p, d->K_b.p);
+    else
+      k_fock_fp64<1><<<nk, 256, 0, st>>>(d->fock_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, d->fac_a.p,
+                                         nullptr, d->M, d->K_a.p, nullptr);
+    LIO_CUDA(cudaGetLastError());
+  }
+  double e = 0.0;
+  LIO_CUDA(cudaMemcpyAsync(&e, d->energy.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+  LIO_CUDA(cudaEventRecord(d->ev1, st));
+  if (req.compute_rmm) {
+    for (int s = 0; s < nspin; s++) {
+      LIO_CUDA(cudaMemcpyAsync(d->hK.data(), s == 0 ? d->K_a.p : d->K_b.p, npacked * sizeof(double),
+                               cudaMemcpyDeviceToHost, st));
+      LIO_CUDA(cudaStreamSynchronize(st));
+      double* dst = s == 0 ? req.fock : req.fock_b;
+      for (size_t i = 0; i < npacked; i++) dst[i] += d->hK[i];
+    }
+  }
+  LIO_CUDA(cudaStreamSynchronize(st));
+  float ms = 0.f;
+  LIO_CUDA(cudaEventElapsedTime(&ms, d->ev0, d->ev1));
+  res.energy = e;
+  res.device_ms = ms;
+  return res;
+}
+
+}  // namespace lio

@@ -1,0 +1,64 @@
+// Device engine for the XC grid integration (one molecule, one GPU).
+//
+// Host code hands it a built partition once per geometry (upload_partition)
+// and then calls solve() once per SCF/TD step with the caller's packed density
+// matrices; solve() accumulates the Kohn-Sham (Fock) contributions into the
+// caller's packed vectors and returns E_xc. No CUDA types appear here so the
+// C-ABI layer compiles with the host compiler.
+#pragma once
+#include <cstddef>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "partition.h"
+#include "system.h"
+
+namespace lio {
+
+enum class Precision { FP64 = 0, TensorCore = 1 };
+
+struct SolveRequest {
+  bool compute_rmm = true;      // accumulate into the Fock vector(s)
+  bool compute_energy = true;
+  const double* rho = nullptr;  // closed shell: packed total density (doubled off-diagonals)
+  const double* rho_a = nullptr;  // open shell
+  const double* rho_b = nullptr;
+  double* fock = nullptr;       // closed shell, or alpha when open
+  double* fock_b = nullptr;     // open shell beta
+};
+
+struct SolveResult {
+  double energy = 0.0;
+  double device_ms = 0.0;
+};
+
+class DeviceEngine {
+ public:
+  DeviceEngine();
+  ~DeviceEngine();
+  DeviceEngine(const DeviceEngine&) = delete;
+  DeviceEngine& operator=(const DeviceEngine&) = delete;
+
+  // Uploads basis parameters, points and function lists; evaluates and caches
+  // the basis values of every group that fits the cache budget.
+  void upload(const System& sys, const Partition& part);
+  SolveResult solve(const SolveRequest& req);
+  void set_precision(Precision p) { precision_ = p; }
+  Precision precision() const { return precision_; }
+  void release();
+
+  // true when a CUDA device can be used from this process
+  static bool available();
+
+  // statistics of the uploaded partition
+  long long points() const;
+  long long groups() const;
+
+ private:
+  struct Impl;
+  std::unique_ptr<Impl> impl_;
+  Precision precision_ = Precision::FP64;
+};
+
+}  // namespace lio

@@ -1,0 +1,418 @@
+// The g2g C ABI (Fortran calling convention) over the B200 device engine.
+//
+// Process-global state, single caller thread, like the reference
+// (g2g/init.cpp:27-33). Every entry point catches all exceptions: failures are
+// recorded in a sticky status (g2g_last_error_) and, at verbose > 0, printed;
+// nothing is thrown across the boundary and nothing calls exit().
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#pragma GCC visibility push(default)
+#include "../../include/g2g.h"
+#pragma GCC visibility pop
+#include "engine.h"
+#include "partition.h"
+#include "system.h"
+
+namespace {
+
+using lio::AngularGrid;
+using lio::Options;
+using lio::Partition;
+using lio::System;
+
+struct BoundArrays {  // caller-owned arrays (g2g/init.h:16-52)
+  unsigned natoms = 0, max_atoms = 0, ngaussians = 0, M = 0;
+  double* r = nullptr;
+  unsigned* nuc = nullptr;
+  unsigned* ncont = nullptr;
+  double *a = nullptr, *c = nullptr;
+  double *rho = nullptr, *fock = nullptr, *fockb = nullptr, *rhoa = nullptr, *rhob = nullptr;
+  bool open = false;
+};
+
+struct State {
+  Options opt;
+  System sys;
+  BoundArrays arr;
+  bool params_set = false;
+  std::map<unsigned, AngularGrid> grids;  // by grid_type
+  int grid_type = -1;
+  Partition part;
+  std::unique_ptr<lio::DeviceEngine> engine;
+  lio::Precision precision = lio::Precision::FP64;
+  int status = 0;
+  std::string message;
+  double last_solve_ms = 0.0, last_grid_ms = 0.0;
+  bool device_ready = false;
+};
+
+State& st() {
+  static State s;
+  return s;
+}
+
+void fail(const std::string& msg, int code = 1) {
+  State& s = st();
+  s.status = code;
+  s.message = msg;
+  if (s.opt.verbose > 0) std::fprintf(stderr, "g2g error: %s\n", msg.c_str());
+}
+
+template <class F>
+void guarded(const char* where, F&& f) {
+  try {
+    f();
+  } catch (const std::exception& e) {
+    fail(std::string(where) + ": " + e.what());
+  } catch (...) {
+    fail(std::string(where) + ": unknown error");
+  }
+}
+
+AngularGrid grid_from_fortran(const double* e, const double* w, unsigned n) {
+  AngularGrid g;
+  g.x.resize(n);
+  g.y.resize(n);
+  g.z.resize(n);
+  g.w.resize(n);
+  for (unsigned i = 0; i < n; i++) {  // column-major n x 3
+    g.x[i] = e[i];
+    g.y[i] = e[n + i];
+    g.z[i] = e[2 * n + i];
+    g.w[i] = w[i];
+  }
+  return g;
+}
+
+// Copies positions and basis parameters out of the bound arrays
+// (g2g/init.cpp:286-294 re-reads the positions at every reload).
+void refresh_system() {
+  State& s = st();
+  System& y = s.sys;
+  const BoundArrays& b = s.arr;
+  y.natoms = (int)b.natoms;
+  y.ax.resize(b.natoms);
+  y.ay.resize(b.natoms);
+  y.az.resize(b.natoms);
+  for (unsigned i = 0; i < b.natoms; i++) {
+    y.ax[i] = b.r[i];
+    y.ay[i] = b.r[b.max_atoms + i];
+    y.az[i] = b.r[2 * (size_t)b.max_atoms + i];
+  }
+  y.atom_dist.assign((size_t)b.natoms * b.natoms, 0.0);
+  for (unsigned i = 0; i < b.natoms; i++)
+    for (unsigned j = 0; j < b.natoms; j++) {
+      const double dx = y.ax[i] - y.ax[j], dy = y.ay[i] - y.ay[j], dz = y.az[i] - y.az[j];
+      y.atom_dist[(size_t)i * b.natoms + j] = std::sqrt(dx * dx + dy * dy + dz * dz);
+    }
+  y.M = (int)b.M;
+  y.nuc.resize(b.M);
+  y.ncont.resize(b.M);
+  y.a.assign((size_t)b.M * lio::kMaxContractions, 0.0);
+  y.c.assign((size_t)b.M * lio::kMaxContractions, 0.0);
+  for (unsigned i = 0; i < b.M; i++) {
+    y.nuc[i] = (int)b.nuc[i] - 1;
+    y.ncont[i] = (int)b.ncont[i];
+    for (unsigned k = 0; k < b.ncont[i] && k < (unsigned)lio::kMaxContractions; k++) {
+      y.a[(size_t)i * lio::kMaxContractions + k] = b.a[(size_t)k * b.ngaussians + i];
+      y.c[(size_t)i * lio::kMaxContractions + k] = b.c[(size_t)k * b.ngaussians + i];
+    }
+  }
+}
+
+void build_grid(unsigned grid_type) {
+  State& s = st();
+  if (!s.params_set) throw std::runtime_error("g2g_parameter_init_ has not been called");
+  auto it = s.grids.find(grid_type);
+  if (it == s.grids.end()) throw std::runtime_error("unknown grid type " + std::to_string(grid_type));
+  const auto t0 = std::chrono::steady_clock::now();
+  refresh_system();
+  lio::build_partition(s.sys, s.opt, it->second, (int)grid_type, s.part);
+  s.grid_type = (int)grid_type;
+  s.last_grid_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  // The partition is host work and is kept even without a GPU (so it can be
+  // inspected); the device upload and every solve need a CUDA device.
+  if (!lio::DeviceEngine::available()) {
+    s.device_ready = false;
+    throw std::runtime_error("no CUDA device: the grid partition was built but the device engine is unavailable");
+  }
+  if (!s.engine) s.engine.reset(new lio::DeviceEngine());
+  s.engine->set_precision(s.precision);
+  s.engine->upload(s.sys, s.part);
+  s.device_ready = true;
+  s.last_grid_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// ---- Fortran-named timers (g2g/timer.cpp:117-296): host wall clock
+struct NamedTimer {
+  double total = 0.0;
+  std::chrono::steady_clock::time_point start;
+  bool running = false;
+};
+std::map<std::string, NamedTimer>& timers() {
+  static std::map<std::string, NamedTimer> t;
+  return t;
+}
+void timer_start(const char* n, unsigned len) {
+  NamedTimer& t = timers()[std::string(n, len)];
+  t.start = std::chrono::steady_clock::now();
+  t.running = true;
+}
+double timer_pause(const char* n, unsigned len) {
+  NamedTimer& t = timers()[std::string(n, len)];
+  if (t.running) {
+    t.total += std::chrono::duration<double>(std::chrono::steady_clock::now() - t.start).count();
+    t.running = false;
+  }
+  return t.total;
+}
+
+}  // namespace
+
+extern "C" {
+
+void g2g_init_(void) {
+  guarded("g2g_init_", [] {
+    if (!lio::DeviceEngine::available()) throw std::runtime_error("no CUDA device visible");
+    if (!st().engine) st().engine.reset(new lio::DeviceEngine());
+  });
+}
+
+void g2g_set_options_(double* fgm, double* lcs, double* sr, bool* aaf, bool* eai, bool* rzw, unsigned* mppc,
+                      unsigned* mfe, unsigned* time, unsigned* verbose) {
+  Options& o = st().opt;
+  o.free_global_memory = *fgm;
+  o.little_cube_size = *lcs;
+  o.sphere_radius = *sr;
+  o.assign_all_functions = *aaf;
+  o.energy_all_iterations = *eai;
+  o.remove_zero_weights = *rzw;
+  o.min_points_per_cube = *mppc;
+  o.max_function_exponent = *mfe;
+  o.timer_level = *time;
+  o.verbose = *verbose;
+}
+
+void g2g_parameter_init_(const unsigned* norm, const unsigned* natom, const unsigned* max_atoms,
+                         const unsigned* ngaussians, double* r, double* Rm, const unsigned* Iz,
+                         const unsigned* Nr, const unsigned* Nr2, unsigned* Nuc, const unsigned* M,
+                         unsigned* ncont, const unsigned* nshell, double* c, double* a, double* rho_vec,
+                         double* fock_vec, double* fockb_vec, double* rhoalpha, double* rhobeta,
+                         const unsigned* nco, bool* OPEN, const unsigned* nunp, const unsigned* nopt,
+                         const unsigned* Iexch, double* e, double* e2, double* e3, double* wang,
+                         double* wang2, double* wang3, bool* use_libxc, const unsigned* ex_functional_id,
+                         const unsigned* ec_functional_id) {
+  guarded("g2g_parameter_init_", [&] {
+    State& s = st();
+    BoundArrays& b = s.arr;
+    b.natoms = *natom;
+    b.max_atoms = *max_atoms;
+    b.ngaussians = *ngaussians;
+    b.M = *M;
+    b.r = r;
+    b.nuc = Nuc;
+    b.ncont = ncont;
+    b.a = a;
+    b.c = c;
+    b.rho = rho_vec;
+    b.fock = fock_vec;
+    b.fockb = fockb_vec;
+    b.rhoa = rhoalpha;
+    b.rhob = rhobeta;
+    b.open = *OPEN;
+    for (unsigned i = 0; i < *M; i++)
+      if (ncont[i] > (unsigned)lio::kMaxContractions)
+        throw std::runtime_error("Maximum functions per contraction reached!");
+    if (*Iexch < 1 || *Iexch > 9) throw std::runtime_error("Iexch out of range 1..9");
+    if (*Iexch != 1 && *Iexch != 2 && *Iexch != 3 && *Iexch != 9)
+      throw std::runtime_error("Iexch " + std::to_string(*Iexch) +
+                               " is not implemented on the device (supported: 1, 2, 3 LDA; 9 PBE)");
+    if (*use_libxc) throw std::runtime_error("libxc functionals are not supported");
+    System& y = s.sys;
+    y.s_funcs = (int)nshell[0];
+    y.p_funcs = (int)nshell[1] / 3;
+    y.d_funcs = (int)nshell[2] / 6;
+    y.d_norm = *norm ? (1.0 / std::sqrt(3)) : 1.0;
+    y.iexch = (int)*Iexch;
+    y.lda = (*Iexch <= 3);
+    y.open = *OPEN;
+    y.atom_type.resize(*natom);
+    y.shells_grid0.resize(*natom);
+    y.shells_grid12.resize(*natom);
+    y.rm.resize(*natom);
+    for (unsigned i = 0; i < *natom; i++) {
+      y.atom_type[i] = (int)Iz[i] - 1;
+      y.shells_grid0[i] = Nr[Iz[i]];
+      y.shells_grid12[i] = Nr2[Iz[i]];
+      y.rm[i] = Rm[Iz[i]];
+    }
+    s.grids[0] = grid_from_fortran(e, wang, 50);
+    s.grids[1] = grid_from_fortran(e2, wang2, 116);
+    s.grids[2] = grid_from_fortran(e3, wang3, 194);
+    s.params_set = true;
+    s.grid_type = -1;
+    (void)nco;
+    (void)nunp;
+    (void)nopt;
+    (void)ex_functional_id;
+    (void)ec_functional_id;
+  });
+}
+
+void g2g_set_angular_grid_(const unsigned* grid_type, const unsigned* npoints, const double* e,
+                           const double* wang) {
+  guarded("g2g_set_angular_grid_", [&] {
+    if (*grid_type < 3) throw std::runtime_error("grid types 0-2 are bound by g2g_parameter_init_");
+    st().grids[*grid_type] = grid_from_fortran(e, wang, *npoints);
+  });
+}
+
+void g2g_reload_atom_positions_(const unsigned* grid_type) {
+  guarded("g2g_reload_atom_positions_", [&] { build_grid(*grid_type); });
+}
+
+void g2g_new_grid_(const unsigned* grid_type) {
+  guarded("g2g_new_grid_", [&] {
+    if ((int)*grid_type != st().grid_type) build_grid(*grid_type);
+  });
+}
+
+void g2g_solve_groups_(const unsigned* computation_type, double* fort_energy_ptr, double* fort_forces_ptr) {
+  guarded("g2g_solve_groups_", [&] {
+    State& s = st();
+    if (s.grid_type < 0) throw std::runtime_error("no grid: call g2g_reload_atom_positions_ first");
+    if (!s.engine || !s.device_ready) throw std::runtime_error("no CUDA device engine for the current grid");
+    const unsigned ct = *computation_type;
+    bool compute_energy = (ct == 1 || ct == 2);
+    const bool compute_forces = (ct == 2 || ct == 3);
+    const bool compute_rmm = (ct == 0);
+    if (s.opt.energy_all_iterations) compute_energy = true;
+    if (compute_forces) throw std::runtime_error("XC forces (computation types 2, 3) are not implemented");
+    lio::SolveRequest req;
+    req.compute_rmm = compute_rmm;
+    req.compute_energy = compute_energy;
+    if (s.sys.open) {
+      req.rho_a = s.arr.rhoa;
+      req.rho_b = s.arr.rhob;
+      req.fock = s.arr.fock;
+      req.fock_b = s.arr.fockb;
+    } else {
+      req.rho = s.arr.rho;
+      req.fock = s.arr.fock;
+    }
+    s.engine->set_precision(s.precision);
+    const lio::SolveResult r = s.engine->solve(req);
+    s.last_solve_ms = r.device_ms;
+    *fort_energy_ptr = compute_energy ? r.energy : 0.0;
+    if (std::isnan(*fort_energy_ptr)) fail("XC energy is NaN", 2);
+    (void)fort_forces_ptr;
+  });
+}
+
+void g2g_deinit_(void) {
+  guarded("g2g_deinit_", [] {
+    State& s = st();
+    s.part.cubes.clear();
+    s.part.spheres.clear();
+    if (s.engine) s.engine->release();
+    s.grid_type = -1;
+  });
+}
+
+int g2g_last_error_(char* msg, const unsigned* len) {
+  State& s = st();
+  const int code = s.status;
+  if (msg && len && *len > 0) {
+    std::strncpy(msg, s.message.c_str(), *len - 1);
+    msg[*len - 1] = 0;
+  }
+  s.status = 0;
+  s.message.clear();
+  return code;
+}
+
+void g2g_set_precision_(const unsigned* mode) {
+  st().precision = *mode == 1 ? lio::Precision::TensorCore : lio::Precision::FP64;
+}
+
+void g2g_partition_stats_(long long* out) {
+  const Partition& p = st().part;
+  long long pts = 0, pm = 0, pm2 = 0;
+  for (int g = 0; g < p.total_groups(); g++) {
+    const lio::PointGroup& pg = p.group(g);
+    const long long n = (long long)pg.points.size(), m = pg.total_functions();
+    pts += n;
+    pm += n * m;
+    pm2 += n * m * m;
+  }
+  out[0] = p.total_groups();
+  out[1] = (long long)p.cubes.size();
+  out[2] = (long long)p.spheres.size();
+  out[3] = pts;
+  out[4] = pm;
+  out[5] = pm2;
+}
+
+int g2g_partition_group_(const int* g, int* meta, int* ids, double* xyzw, int* funcs) {
+  const Partition& p = st().part;
+  if (*g < 0 || *g >= p.total_groups()) return -1;
+  const lio::PointGroup& pg = p.group(*g);
+  meta[0] = (int)pg.points.size();
+  meta[1] = (int)pg.funcs.size();
+  meta[2] = pg.s;
+  meta[3] = pg.p;
+  meta[4] = pg.d;
+  meta[5] = pg.total_functions();
+  meta[6] = (int)pg.nucs.size();
+  meta[7] = pg.sphere ? 1 : 0;
+  for (size_t i = 0; i < pg.points.size(); i++) {
+    const lio::GridPoint& q = pg.points[i];
+    if (ids) {
+      ids[3 * i] = q.atom;
+      ids[3 * i + 1] = q.shell;
+      ids[3 * i + 2] = q.point;
+    }
+    if (xyzw) {
+      xyzw[4 * i] = q.x;
+      xyzw[4 * i + 1] = q.y;
+      xyzw[4 * i + 2] = q.z;
+      xyzw[4 * i + 3] = q.w;
+    }
+  }
+  if (funcs)
+    for (size_t i = 0; i < pg.funcs.size(); i++) funcs[i] = pg.funcs[i];
+  return 0;
+}
+
+void g2g_last_timings_(double* solve_ms, double* grid_ms) {
+  *solve_ms = st().last_solve_ms;
+  *grid_ms = st().last_grid_ms;
+}
+
+void g2g_timer_start_(const char* n, unsigned len) { timer_start(n, len); }
+void g2g_timer_stop_(const char* n, unsigned len) {
+  const double t = timer_pause(n, len);
+  if (st().opt.timer_level % 2 == 1) std::printf("TIMER [%.*s]: %.6f s\n", (int)len, n, t);
+  timers().erase(std::string(n, len));
+}
+void g2g_timer_pause_(const char* n, unsigned len) { timer_pause(n, len); }
+void g2g_timer_sum_start_(const char* n, unsigned len) { timer_start(n, len); }
+void g2g_timer_sum_stop_(const char* n, unsigned len) { timer_pause(n, len); }
+void g2g_timer_sum_pause_(const char* n, unsigned len) { timer_pause(n, len); }
+void g2g_timer_clear_(void) { timers().clear(); }
+void g2g_timer_summary_(void) {
+  if (st().opt.timer_level > 1)
+    for (const auto& kv : timers()) std::printf("TIMER SUMMARY [%s]: %.6f s\n", kv.first.c_str(), kv.second.total);
+}
+
+}  // extern "C"

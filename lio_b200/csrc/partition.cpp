@@ -1,0 +1,305 @@
+// Grid generation, significant-function screening and Becke weights.
+//
+// Every floating-point expression below keeps the operand order of the
+// reference so that points, weights and function lists come out bit-for-bit
+// equal (this file is compiled with -ffp-contract=off and no -march, so no
+// fused multiply-add is formed). The reference steps each function follows are
+// cited inline.
+#include "partition.h"
+
+#include <omp.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <limits>
+#include <set>
+#include <stdexcept>
+
+namespace lio {
+namespace {
+
+// g2g/partition.cpp:230-254
+bool is_significative(int type /*1,3,6*/, double exponent, double d2, unsigned mfe) {
+  if (type == 1) {
+    return (exponent * d2 < mfe - std::log(std::pow((2. * exponent / M_PI), 3)) / 4);
+  }
+  double x = 1;
+  double delta;
+  const double e = 0.1;
+  double factor = std::pow((2.0 * exponent / M_PI), 3);
+  factor = std::sqrt(factor * 4.0 * exponent);
+  double norm = (type == 3 ? std::sqrt(factor) : std::fabs(factor));
+  do {
+    double div = (type == 3 ? std::log(x) : 2 * std::log(x));
+    double x1 = std::sqrt((mfe - std::log(norm) + div) / exponent);
+    delta = std::fabs(x - x1);
+    x = x1;
+  } while (delta > e);
+  return (std::sqrt(d2) < x);
+}
+
+inline double len3(double x, double y, double z) { return std::sqrt(x * x + y * y + z * z); }
+
+// g2g/classify_functions.cpp:13-65: walks s, then p (stride 3), then d (stride 6).
+void assign_functions(const System& sys, const Options& opt, const std::vector<double>& dists,
+                      const std::vector<double>& min_exps, PointGroup& g) {
+  std::set<int> nuc_set;
+  g.funcs.clear();
+  int f = 0;
+  const int s_end = sys.s_funcs, p_end = sys.s_funcs + sys.p_funcs * 3,
+            d_end = sys.s_funcs + sys.p_funcs * 3 + sys.d_funcs * 6;
+  for (; f < s_end; f++) {
+    int atom = sys.nuc[f];
+    if (opt.assign_all_functions ||
+        is_significative(1, min_exps[f], dists[atom], opt.max_function_exponent)) {
+      g.funcs.push_back(f);
+      g.s++;
+      nuc_set.insert(atom);
+    }
+  }
+  for (; f < p_end; f += 3) {
+    int atom = sys.nuc[f];
+    if (opt.assign_all_functions ||
+        is_significative(3, min_exps[f], dists[atom], opt.max_function_exponent)) {
+      g.funcs.push_back(f);
+      g.p++;
+      nuc_set.insert(atom);
+    }
+  }
+  for (; f < d_end; f += 6) {
+    int atom = sys.nuc[f];
+    if (opt.assign_all_functions ||
+        is_significative(6, min_exps[f], dists[atom], opt.max_function_exponent)) {
+      g.funcs.push_back(f);
+      g.d++;
+      nuc_set.insert(atom);
+    }
+  }
+  g.nucs.assign(nuc_set.begin(), nuc_set.end());
+}
+
+// Becke fuzzy-cell partition with the atomic-size adjustment, restricted to the
+// group's nuclei: g2g/cpu/weight.cpp:13-112.
+inline double becke_step(double u, double rm_j, double rm_k) {
+  double x = rm_j / rm_k;
+  x = (x - 1.0) / (x + 1.0);
+  u += (x / (x * x - 1.0)) * (1.0 - u * u);
+  u = 1.5 * u - 0.5 * (u * u * u);
+  u = 1.5 * u - 0.5 * (u * u * u);
+  u = 1.5 * u - 0.5 * (u * u * u);
+  return 0.5 * (1.0 - u);
+}
+
+void compute_weights(const System& sys, const Options& opt, PointGroup& g) {
+  const int nn = (int)g.nucs.size();
+  const int np = (int)g.points.size();
+  const int* nucs = g.nucs.data();
+#pragma omp parallel for schedule(static) if (np > 2048)
+  for (int pi = 0; pi < np; pi++) {
+    GridPoint& pt = g.points[pi];
+    const int atom = pt.atom;
+    double P_total = 0.0, P_atom = 0.0;
+    bool own_found = false;
+    for (int j = 0; j < nn; ++j) {
+      double P_curr = 1.0;
+      const int aj = nucs[j];
+      const double dj = len3(pt.x - sys.ax[aj], pt.y - sys.ay[aj], pt.z - sys.az[aj]);
+      for (int k = 0; k < nn; ++k) {
+        const int ak = nucs[k];
+        if (ak == aj) continue;
+        double u = (dj - len3(pt.x - sys.ax[ak], pt.y - sys.ay[ak], pt.z - sys.az[ak])) /
+                   sys.atom_dist[(size_t)aj * sys.natoms + ak];
+        P_curr *= becke_step(u, sys.rm[aj], sys.rm[ak]);
+        if (P_curr == 0.0) break;
+      }
+      if (aj == atom) {
+        own_found = true;
+        P_atom = P_curr;
+        if (P_atom == 0.0) break;
+      }
+      P_total += P_curr;
+    }
+    if (!own_found) {
+      // the point's own atom is not among the group's nuclei (weight.cpp:67-96)
+      P_atom = 1.0;
+      const double da = len3(pt.x - sys.ax[atom], pt.y - sys.ay[atom], pt.z - sys.az[atom]);
+      for (int k = 0; k < nn; ++k) {
+        const int ak = nucs[k];
+        double u = (da - len3(pt.x - sys.ax[ak], pt.y - sys.ay[ak], pt.z - sys.az[ak])) /
+                   sys.atom_dist[(size_t)atom * sys.natoms + ak];
+        P_atom *= becke_step(u, sys.rm[atom], sys.rm[ak]);
+        if (P_atom == 0.0) break;
+      }
+    }
+    const double atom_weight = (P_total == 0.0 ? 0.0 : (P_atom / P_total));
+    pt.w *= atom_weight;
+  }
+  if (opt.remove_zero_weights) {
+    std::vector<GridPoint> kept;
+    kept.reserve(g.points.size());
+    for (const GridPoint& p : g.points)
+      if (p.w != 0.0) kept.push_back(p);
+    g.points.swap(kept);
+  }
+}
+
+long long env_int(const char* name, long long dflt) {
+  const char* v = std::getenv(name);
+  return v ? std::strtol(v, nullptr, 10) : dflt;
+}
+
+}  // namespace
+
+void build_partition(const System& sys, const Options& opt, const AngularGrid& ang,
+                     int grid_type, Partition& out) {
+  out.cubes.clear();
+  out.spheres.clear();
+  const int natoms = sys.natoms;
+  const std::vector<unsigned>& shells = grid_type == 0 ? sys.shells_grid0 : sys.shells_grid12;
+
+  // smallest exponent per element and per function (regenerate_partition.cpp:165-186)
+  std::vector<double> min_exps_type(120, std::numeric_limits<double>::max());
+  for (int i = 0; i < sys.M; i++) {
+    const int t = sys.atom_type[sys.nuc[i]];
+    for (int j = 0; j < sys.ncont[i]; j++)
+      min_exps_type[t] = std::min(min_exps_type[t], sys.a[(size_t)i * kMaxContractions + j]);
+  }
+  std::vector<double> min_exps_func(sys.M, std::numeric_limits<double>::max());
+  for (int i = 0; i < sys.M; i++)
+    for (int j = 0; j < sys.ncont[i]; j++)
+      if (sys.a[(size_t)i * kMaxContractions + j] < min_exps_func[i])
+        min_exps_func[i] = sys.a[(size_t)i * kMaxContractions + j];
+
+  // bounding prism (:189-219)
+  double x0[3] = {0, 0, 0}, x1[3] = {0, 0, 0};
+  for (int atom = 0; atom < natoms; atom++) {
+    const double pos[3] = {sys.ax[atom], sys.ay[atom], sys.az[atom]};
+    const double r = 2 * std::sqrt(opt.max_function_exponent / min_exps_type[sys.atom_type[atom]]);
+    for (int d = 0; d < 3; d++) {
+      if (atom == 0) {
+        x0[d] = pos[d] - r;
+        x1[d] = pos[d] + r;
+      } else {
+        x0[d] = std::min(x0[d], pos[d] - r);
+        x1[d] = std::max(x1[d], pos[d] + r);
+      }
+    }
+  }
+  const double lcs = opt.little_cube_size;
+  unsigned psize[3];
+  for (int d = 0; d < 3; d++) psize[d] = (unsigned)std::ceil((x1[d] - x0[d]) / lcs);
+
+  // sphere radii (:227-248)
+  std::vector<double> sphere_r(natoms, 0.0);
+  if (opt.sphere_radius > 0) {
+    for (int atom = 0; atom < natoms; atom++) {
+      const unsigned ns = shells[atom];
+      const unsigned inc = (unsigned)std::ceil(opt.sphere_radius * ns);
+      if (inc == 0) {
+        sphere_r[atom] = 0;
+      } else {
+        const double x = std::cos((M_PI / (ns + 1)) * (ns - inc + 1));
+        sphere_r[atom] = sys.rm[atom] * (1.0 + x) / (1.0 - x);
+      }
+    }
+  }
+
+  // points: Gauss-Chebyshev radial (Becke mapping) x angular (:274-322)
+  const size_t ncubes_all = (size_t)psize[0] * psize[1] * psize[2];
+  std::vector<std::vector<GridPoint>> prism(ncubes_all);
+  std::vector<std::vector<GridPoint>> sph(opt.sphere_radius > 0 ? natoms : 0);
+  for (int atom = 0; atom < natoms; atom++) {
+    const unsigned ns = shells[atom];
+    const double t0 = M_PI / (ns + 1);
+    const double rm = sys.rm[atom];
+    const unsigned inc = (unsigned)std::ceil(opt.sphere_radius * ns);
+    for (unsigned shell = 0; shell < ns; shell++) {
+      const double t1 = t0 * (shell + 1);
+      const double x = std::cos(t1);
+      const double w = t0 * std::fabs(std::sin(t1));
+      const double r1 = rm * (1.0 + x) / (1.0 - x);
+      const double wrad = w * (r1 * r1) * rm * 2.0 / ((1.0 - x) * (1.0 - x));
+      for (int p = 0; p < ang.size(); p++) {
+        const double px = sys.ax[atom] + ang.x[p] * r1;
+        const double py = sys.ay[atom] + ang.y[p] * r1;
+        const double pz = sys.az[atom] + ang.z[p] * r1;
+        const bool inside = (x0[0] <= px && px <= x1[0]) && (x0[1] <= py && py <= x1[1]) &&
+                            (x0[2] <= pz && pz <= x1[2]);
+        if (!inside) continue;
+        GridPoint gp{atom, (int)shell, p, px, py, pz, wrad * ang.w[p]};
+        if (shell >= (ns - inc)) {
+          sph[atom].push_back(gp);
+        } else {
+          const unsigned cx = (unsigned)std::floor((px - x0[0]) / lcs);
+          const unsigned cy = (unsigned)std::floor((py - x0[1]) / lcs);
+          const unsigned cz = (unsigned)std::floor((pz - x0[2]) / lcs);
+          if (cx >= psize[0] || cy >= psize[1] || cz >= psize[2])
+            throw std::runtime_error("grid point outside the cube prism");
+          prism[((size_t)cx * psize[1] + cy) * psize[2] + cz].push_back(gp);
+        }
+      }
+    }
+  }
+  out.mincost = env_int("LIO_MINCOST_OFFSET", 250000);
+
+  // cubes (:331-399): screening against the cube box, then weights
+  std::vector<double> dists(natoms);
+  for (unsigned i = 0; i < psize[0]; i++)
+    for (unsigned j = 0; j < psize[1]; j++)
+      for (unsigned k = 0; k < psize[2]; k++) {
+        std::vector<GridPoint>& pts = prism[((size_t)i * psize[1] + j) * psize[2] + k];
+        const double cc[3] = {x0[0] + i * lcs, x0[1] + j * lcs, x0[2] + k * lcs};
+        for (int a = 0; a < natoms; a++) {
+          const double pos[3] = {sys.ax[a], sys.ay[a], sys.az[a]};
+          double dv[3];
+          for (int d = 0; d < 3; d++) {
+            if (pos[d] < cc[d])
+              dv[d] = cc[d] - pos[d];
+            else if (pos[d] > (cc[d] + lcs))
+              dv[d] = pos[d] - (cc[d] + lcs);
+            else
+              dv[d] = 0;
+          }
+          dists[a] = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
+        }
+        PointGroup g;
+        g.sphere = false;
+        assign_functions(sys, opt, dists, min_exps_func, g);
+        if (g.funcs.empty() || pts.size() < opt.min_points_per_cube) continue;
+        g.points.swap(pts);
+        compute_weights(sys, opt, g);
+        if (g.points.size() < opt.min_points_per_cube) continue;
+        out.cubes.push_back(std::move(g));
+      }
+
+  // spheres (:402-462)
+  if (opt.sphere_radius > 0) {
+    for (int a = 0; a < natoms; a++) {
+      for (int o = 0; o < natoms; o++) {
+        if (o == a) {
+          dists[o] = 0;
+        } else {
+          const double d = len3(sys.ax[o] - sys.ax[a], sys.ay[o] - sys.ay[a], sys.az[o] - sys.az[a]);
+          const double dd = (sphere_r[a] > d ? 0 : d - sphere_r[a]);
+          dists[o] = dd * dd;
+        }
+      }
+      PointGroup g;
+      g.sphere = true;
+      assign_functions(sys, opt, dists, min_exps_func, g);
+      if (sph[a].size() < opt.min_points_per_cube) continue;
+      g.points.swap(sph[a]);
+      compute_weights(sys, opt, g);
+      if (g.points.size() < opt.min_points_per_cube) continue;
+      out.spheres.push_back(std::move(g));
+    }
+  }
+
+  const long long mc = out.mincost;
+  auto by_cost = [mc](const PointGroup& l, const PointGroup& r) { return l.cost(mc) < r.cost(mc); };
+  std::stable_sort(out.cubes.begin(), out.cubes.end(), by_cost);
+  std::stable_sort(out.spheres.begin(), out.spheres.end(), by_cost);
+}
+
+}  // namespace lio

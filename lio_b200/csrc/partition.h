@@ -1,0 +1,44 @@
+// Grid generation and partition into cubes/spheres (host, FP64, bit-exact with
+// the reference's g2g/regenerate_partition.cpp:161-481, classify_functions.cpp
+// and cpu/weight.cpp).
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "system.h"
+
+namespace lio {
+
+struct GridPoint {
+  int atom, shell, point;
+  double x, y, z, w;
+};
+
+struct PointGroup {
+  bool sphere = false;
+  std::vector<GridPoint> points;
+  std::vector<int> funcs;  // simple functions: global index of the first component
+  std::vector<int> nucs;   // sorted global nuclei of the significant functions
+  int s = 0, p = 0, d = 0;
+  int total_functions() const { return s + 3 * p + 6 * d; }
+  long long cost(long long mincost) const {  // g2g/partition.cpp:257-260
+    long long np = (long long)points.size(), gm = total_functions();
+    return 10 * ((np * gm * (1 + gm)) / 2) + mincost;
+  }
+};
+
+struct Partition {
+  std::vector<PointGroup> cubes, spheres;  // each sorted by cost
+  long long mincost = 250000;
+  int total_groups() const { return (int)(cubes.size() + spheres.size()); }
+  const PointGroup& group(int g) const {
+    return g < (int)cubes.size() ? cubes[g] : spheres[g - cubes.size()];
+  }
+};
+
+// Builds the partition. `grid_type` selects the radial shell table (0: Nr,
+// otherwise Nr2) exactly as g2g/init.cpp:238-266 does.
+void build_partition(const System& sys, const Options& opt, const AngularGrid& ang,
+                     int grid_type, Partition& out);
+
+}  // namespace lio
