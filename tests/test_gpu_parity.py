@@ -1,0 +1,30 @@
+"""FP64 device path vs the reference CPU g2g path (E_xc and the packed Kohn-Sham matrix)."""
+import numpy as np
+import pytest
+
+from lio_b200 import workloads as W
+
+from . import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    ("cfg1-lda-vwn", lambda: W.config(1)),
+    ("pbe-closed-12", lambda: W.small_workload(12, 21, 9, False)),
+    ("pbe-open-10", lambda: W.small_workload(10, 31, 9, True)),
+    ("lda-gl-8", lambda: W.small_workload(8, 41, 2, False)),
+    ("slater-8", lambda: W.small_workload(8, 43, 1, False)),
+]
+
+
+@pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
+def test_fp64_matches_reference(name, make):
+    wl = make()
+    E_ref, K_ref, Kb_ref = H.reference(wl)
+    P = H.lib(H.os.path.join(H.ROOT, "lio_b200", "libg2g_b200.so"), True)
+    E, K, Kb = H.run(P, wl, precision=0)
+    assert abs(E - E_ref) <= H.E_TOL, (E, E_ref)
+    assert np.max(np.abs(K - K_ref)) <= H.K_TOL
+    if wl.open_shell:
+        assert np.max(np.abs(Kb - Kb_ref)) <= H.K_TOL
+    print(name, E, E_ref, abs(E - E_ref), np.max(np.abs(K - K_ref)))
