@@ -1,0 +1,333 @@
+"""XC grid-integration throughput (grid points per second of one Kohn-Sham XC build).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the 256-atom open-shell PBE cluster (64 C, 16 N, 16 O, 160 H in a
+22 A box, seeded), H 2s1p / C,N,O 3s2p1d contracted Cartesian basis, 40 radial
+shells x 302-point Lebedev angular grid per atom, random orthonormal-orbital
+alpha/beta densities (N_alpha = N_beta + 2). Synthetic, seeded data; no public
+dataset is involved.
+
+A step is one XC build of that molecule: the g2g_solve_groups_(0) work
+(density and its derivatives from the packed density matrices, the PBE point
+functional, E_xc, and accumulation into the packed Kohn-Sham matrices).
+  value : points / (device time per build) with the density already in HBM
+          and the Kohn-Sham accumulators left in HBM (g2g_solve_resident_),
+          timed with CUDA events on the library's stream;
+  e2e   : the same metric through the public C ABI (g2g_solve_groups_) with
+          the caller's host arrays: density H2D, Kohn-Sham D2H and the +=
+          into the caller's packed vectors inside the timed region.
+With --gpus N > 1 (one process per GPU under torchrun) every rank builds its
+own molecule of the same composition (seed offset by rank): molecules are
+independent, no collective is on the data path, scaling is weak.
+
+--impl reference times the reference's own CPU g2g path (compiled from its
+sources by oracle/Makefile) on the same molecule with all host cores; the
+reference supports only its 50/116/194-point angular tables, so it runs the
+40 x 194 grid of that molecule (stated in the line).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from lio_b200 import workloads as W  # noqa: E402
+from lio_b200.g2g import G2GLibrary, angular_tables  # noqa: E402
+
+METRIC = "grid pts/s XC build (FP32-TC vs FP64 plain, |dE|<1e-6 Ha); served p50/p99 ms"
+UNIT = "grid points/s"
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libg2g_ref.so")
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def bind(lib: G2GLibrary, wl: W.Workload):
+    e, w = angular_tables(wl.n_ang)
+    lib.set_options(eai=True)
+    if wl.n_ang == 194:
+        lib.bind_workload(wl, {2: (e, w)})
+        return 2
+    lib.bind_workload(wl, {})
+    lib.set_angular_grid(3, e, w)
+    return 3
+
+
+def workload(rank: int) -> W.Workload:
+    if rank == 0:
+        return W.config(3)
+    return W.make_workload(f"cfg3-rank{rank}", {"C": 64, "N": 16, "O": 16, "H": 160}, 22.0, 3000 + 17 * rank, 9,
+                           True, 302, 40)
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return None
+    wl = W.config(3)
+    wl.n_ang = 194
+    cores = os.cpu_count()
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    if not os.path.exists(REF_LIB):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libg2g_ref.so not built (needs the reference sources)"}
+    L = G2GLibrary(REF_LIB, product=False)
+    L.init()
+    gt = bind(L, wl)
+    t0 = time.perf_counter()
+    L.reload_atom_positions(gt)
+    grid_s = time.perf_counter() - t0
+    npts = sum(int(L.partition_group(g, ref=True)["meta"][0]) for g in range(L.num_groups(ref=True)))
+    for _ in range(args.warmup):
+        L.solve_groups(0)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        L.solve_groups(0)
+    dt = (time.perf_counter() - t0) / args.steps
+    value = npts / dt
+    sample = (f"full XC build of the 256-atom open-shell PBE molecule on its 40x194 grid ({npts} points; the "
+              f"reference has no 302-point table), g2g_solve_groups_(0) with energy, OpenMP on all host cores")
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "cfg3: 256 atoms 64C16N16O160H open-shell PBE, reference grid 40x194",
+                       "points": npts, "grid_build_s": grid_s},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def cpu_baseline(wl: W.Workload):
+    """Reference CPU g2g path on the same molecule (194-point grid), one warm-up and one timed build."""
+    if not os.path.exists(REF_LIB):
+        return None
+    wl = W.Workload(**{**wl.__dict__, "n_ang": 194})
+    cores = os.cpu_count()
+    L = G2GLibrary(REF_LIB, product=False)
+    L.init()
+    gt = bind(L, wl)
+    L.reload_atom_positions(gt)
+    npts = sum(int(L.partition_group(g, ref=True)["meta"][0]) for g in range(L.num_groups(ref=True)))
+    L.solve_groups(0)
+    t0 = time.perf_counter()
+    L.solve_groups(0)
+    dt = time.perf_counter() - t0
+    L.deinit()
+    return {"value": npts / dt, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"one timed full XC build (after one warm-up) of the same molecule on the reference's "
+                      f"40x194 grid, {npts} points, {dt:.2f} s"}
+
+
+def ours(args, rank, world):
+    import torch
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+    wl = workload(rank)
+    lib = G2GLibrary()
+    L = lib.lib
+    L.g2g_set_stream_(C.c_void_p(stream.cuda_stream))
+    lib.check("g2g_set_stream_")
+    gt = bind(lib, wl)
+    lib.set_precision(args.precision)
+    t0 = time.perf_counter()
+    msg = lib.reload_atom_positions(gt)
+    if msg:
+        raise RuntimeError(msg)
+    grid_s = time.perf_counter() - t0
+    st = lib.partition_stats()
+    npts = st["points"]
+    npacked = wl.basis.M * (wl.basis.M + 1) // 2
+    nspin = 2 if wl.open_shell else 1
+
+    # end-to-end through the public ABI (host arrays, H2D + D2H + += inside)
+    for _ in range(args.warmup):
+        lib.solve_groups(0)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        E = lib.solve_groups(0)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+
+    # device-resident throughput
+    L.g2g_solve_resident_.restype = C.c_int
+    for _ in range(args.warmup):
+        launches = L.g2g_solve_resident_()
+    lib.check("g2g_solve_resident_")
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            L.g2g_solve_resident_()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms, e2e_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+        tot = torch.tensor([float(npts)], device="cuda")
+        torch.distributed.all_reduce(tot)
+        total_pts = float(tot[0])
+    else:
+        total_pts = float(npts)
+
+    # per-stage times (separate profiled pass: events between stages)
+    L.g2g_profile_(C.byref(C.c_uint(1)))
+    for _ in range(args.steps):
+        L.g2g_solve_resident_()
+    torch.cuda.synchronize()
+    stage = (C.c_double * 3)()
+    nsol = C.c_int(0)
+    L.g2g_stage_times_(stage, C.byref(nsol))
+    L.g2g_profile_(C.byref(C.c_uint(0)))
+    stage_ms = [stage[i] / max(1, nsol.value) for i in range(3)]
+
+    if rank != 0:
+        return None
+    hbm, bf16, src = load_peaks()
+    # dominant kernel: the density contraction (stage 0), nspin launches per build
+    pm = st["pm"]
+    pm2 = st["pm2"]
+    nk = 10 if wl.iexch > 3 else 1
+    na = 4 if wl.iexch > 3 else 1
+    dens_flops = 2.0 * na * pm2 * nspin
+    dens_bytes = (nk * pm * 8.0 + 10 * 8.0 * npts) * nspin
+    t_dens = stage_ms[0] * 1e-3
+    result = {
+        "metric": METRIC, "value": total_pts / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == 0 else "i8-split/f64", "data": "synthetic",
+        "config": {"workload": "cfg3: 256 atoms 64C16N16O160H, 40x302 grid, open-shell PBE (Iexch 9)",
+                   "points": npts, "groups": st["groups"], "M": wl.basis.M,
+                   "precision": "fp64" if args.precision == 0 else "tensor",
+                   "l2": "inputs larger than L2 (resident basis cache of %.1f GB)" % (nk * pm * 8 / 1e9),
+                   "grid_build_s": round(grid_s, 3), "E_xc": E},
+        "e2e": {"value": total_pts / (e2e_ms * 1e-3), "unit": UNIT,
+                "h2d_bytes_per_step": npacked * 8 * nspin, "d2h_bytes_per_step": npacked * 8 * nspin + 8},
+        "gpu_launches": int(launches) * args.steps,
+        "stage_ms": {"density": stage_ms[0], "functional": stage_ms[1], "fock": stage_ms[2]},
+        "roofline": {"bound": "hbm", "achieved": dens_bytes / t_dens / 1e9, "peak": hbm,
+                     "unit": "GB/s", "frac": dens_bytes / t_dens / 1e9 / hbm, "traffic": None,
+                     "kernel": "k_density (GGA, %d launches per build)" % nspin,
+                     "peak_source": src,
+                     "fp64_tflops": dens_flops / t_dens / 1e12},
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(wl)
+    return result
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", type=int, default=0, help="0 = FP64 plain, 1 = tensor-core form")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        res = reference_arm(args, rank, world)
+        if res is not None:
+            print(json.dumps(res), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    res = ours(args, rank, world)
+    if res is not None:
+        print(json.dumps(res), flush=True)
+    if world > 1:
+        import torch
+
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

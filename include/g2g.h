@@ -124,6 +124,25 @@ int g2g_partition_group_(const int* g, int* meta, int* ids, double* xyzw, int* f
  * device work) and of the last partition build (ms, host clock). */
 void g2g_last_timings_(double* solve_ms, double* grid_ms);
 
+/* Runs all device work of this library on the given cudaStream_t (NULL: the
+ * library's own stream). */
+void g2g_set_stream_(void* cuda_stream);
+
+/* Device-resident solve: same work as g2g_solve_groups_(0) on the density that
+ * the last g2g_solve_groups_ uploaded, with the Kohn-Sham accumulator and the
+ * energy left in device memory and no host synchronisation (for callers that
+ * keep the SCF state on the GPU, and for throughput measurement). Returns the
+ * number of kernel launches it enqueued. */
+int g2g_solve_resident_(void);
+
+/* Per-stage device timing with CUDA events recorded between the stages of
+ * every solve. g2g_profile_(on) resets the sums; g2g_stage_times_ writes the
+ * accumulated ms of stage 0 = density contraction(s), 1 = point functional and
+ * energy sum, 2 = Kohn-Sham contraction, and the number of solves timed.
+ * Returns the number of stages. */
+void g2g_profile_(const unsigned int* on);
+int g2g_stage_times_(double* ms, int* solves);
+
 #ifdef __cplusplus
 }
 #endif

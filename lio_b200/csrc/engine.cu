@@ -454,18 +454,43 @@ struct DeviceEngine::Impl {
   DevBuf<int4> dens_tiles, fock_tiles;
   DevBuf<double> P_a, P_b, K_a, K_b, part_a, part_b, fac_a, fac_b, eblocks, energy;
   std::vector<double> hK;
+  cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int launches = 0;
+  bool profiling = false;
+  cudaEvent_t sev[4] = {nullptr, nullptr, nullptr, nullptr};
+  double stage_ms[3] = {0, 0, 0};
+  int profiled = 0;
+  bool pending = false;
+  void collect() {
+    if (!pending) return;
+    LIO_CUDA(cudaEventSynchronize(sev[3]));
+    for (int i = 0; i < 3; i++) {
+      float ms = 0.f;
+      LIO_CUDA(cudaEventElapsedTime(&ms, sev[i], sev[i + 1]));
+      stage_ms[i] += ms;
+    }
+    profiled++;
+    pending = false;
+  }
+  void mark(int i) {
+    if (profiling) LIO_CUDA(cudaEventRecord(sev[i], stream));
+  }
 
   Impl() {
-    LIO_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    LIO_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+    stream = own_stream;
     LIO_CUDA(cudaEventCreate(&ev0));
     LIO_CUDA(cudaEventCreate(&ev1));
+    for (auto& e : sev) LIO_CUDA(cudaEventCreate(&e));
   }
   ~Impl() {
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
-    if (stream) cudaStreamDestroy(stream);
+    for (auto& e : sev)
+      if (e) cudaEventDestroy(e);
+    if (own_stream) cudaStreamDestroy(own_stream);
   }
 };
 
@@ -490,6 +515,22 @@ void DeviceEngine::release() {
 }
 
 long long DeviceEngine::points() const { return impl_->npoints; }
+void DeviceEngine::set_stream(void* s) {
+  impl_->stream = s ? (cudaStream_t)s : impl_->own_stream;
+}
+int DeviceEngine::launches_per_solve() const { return impl_->launches; }
+void DeviceEngine::set_profiling(bool on) {
+  impl_->collect();
+  impl_->profiling = on;
+  impl_->profiled = 0;
+  for (double& v : impl_->stage_ms) v = 0.0;
+}
+int DeviceEngine::stage_times(double* ms, int max_stages, int* solves) const {
+  impl_->collect();
+  for (int i = 0; i < 3 && i < max_stages; i++) ms[i] = impl_->stage_ms[i];
+  if (solves) *solves = impl_->profiled;
+  return 3;
+}
 long long DeviceEngine::groups() const { return impl_->ngroups; }
 
 void DeviceEngine::upload(const System& sys, const Partition& part) {
@@ -626,8 +667,11 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
   const size_t npacked = (size_t)d->M * (d->M + 1) / 2;
   if (d->ngroups == 0) return res;
   cudaStream_t st = d->stream;
+  int launches = 0;
   LIO_CUDA(cudaEventRecord(d->ev0, st));
-  if (d->open) {
+  if (req.resident) {
+    // density already on the device
+  } else if (d->open) {
     LIO_CUDA(cudaMemcpyAsync(d->P_a.p, req.rho_a, npacked * sizeof(double), cudaMemcpyHostToDevice, st));
     LIO_CUDA(cudaMemcpyAsync(d->P_b.p, req.rho_b, npacked * sizeof(double), cudaMemcpyHostToDevice, st));
   } else {
@@ -635,6 +679,8 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
   }
   const unsigned nd = (unsigned)d->dens_tiles.n, nf = (unsigned)d->func_tiles.n,
                  nk = (unsigned)d->fock_tiles.n;
+  d->collect();
+  d->mark(0);
   const int nspin = d->open ? 2 : 1;
   for (int s = 0; s < nspin; s++) {
     const double* P = s == 0 ? d->P_a.p : d->P_b.p;
@@ -644,13 +690,17 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
     else
       k_density_fp64<4><<<nd, 256, 0, st>>>(d->dens_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, P, d->M, part);
     LIO_CUDA(cudaGetLastError());
+    launches++;
   }
+  d->mark(1);
   k_functional<<<nf, kFuncBlock, 0, st>>>(d->func_tiles.p, d->groups.p, d->pw.p, d->part_a.p,
                                           d->open ? d->part_b.p : nullptr, d->lda ? 1 : 0, d->open ? 1 : 0,
                                           d->iexch, d->fac_a.p, d->open ? d->fac_b.p : nullptr, d->eblocks.p);
   LIO_CUDA(cudaGetLastError());
   k_sum_blocks<<<1, 1024, 0, st>>>(d->eblocks.p, (int)nf, d->energy.p);
   LIO_CUDA(cudaGetLastError());
+  launches += 2;
+  d->mark(2);
   if (req.compute_rmm) {
     LIO_CUDA(cudaMemsetAsync(d->K_a.p, 0, npacked * sizeof(double), st));
     if (d->open) LIO_CUDA(cudaMemsetAsync(d->K_b.p, 0, npacked * sizeof(double), st));
@@ -661,6 +711,14 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
       k_fock_fp64<1><<<nk, 256, 0, st>>>(d->fock_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, d->fac_a.p,
                                          nullptr, d->M, d->K_a.p, nullptr);
     LIO_CUDA(cudaGetLastError());
+    launches++;
+  }
+  d->launches = launches;
+  d->mark(3);
+  d->pending = d->profiling;
+  if (req.resident) {
+    LIO_CUDA(cudaEventRecord(d->ev1, st));
+    return res;
   }
   double e = 0.0;
   LIO_CUDA(cudaMemcpyAsync(&e, d->energy.p, sizeof(double), cudaMemcpyDeviceToHost, st));

@@ -26,6 +26,9 @@ struct SolveRequest {
   const double* rho_b = nullptr;
   double* fock = nullptr;       // closed shell, or alpha when open
   double* fock_b = nullptr;     // open shell beta
+  // Device-resident mode: reuse the density already on the device, leave the
+  // Kohn-Sham accumulator and the energy on the device, do not synchronise.
+  bool resident = false;
 };
 
 struct SolveResult {
@@ -45,6 +48,15 @@ class DeviceEngine {
   void upload(const System& sys, const Partition& part);
   SolveResult solve(const SolveRequest& req);
   void set_precision(Precision p) { precision_ = p; }
+  // Stream for all device work (nullptr: the engine's own stream).
+  void set_stream(void* cuda_stream);
+  // Kernel launches of one solve (for launch accounting).
+  int launches_per_solve() const;
+  // Per-stage device timing (CUDA events between the stages of every solve):
+  // stage 0 = density contraction(s), 1 = point functional + energy sum,
+  // 2 = Kohn-Sham contraction. Accumulated over solves until reset.
+  void set_profiling(bool on);
+  int stage_times(double* ms, int max_stages, int* solves) const;
   Precision precision() const { return precision_; }
   void release();
 

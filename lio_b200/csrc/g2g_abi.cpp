@@ -54,6 +54,7 @@ struct State {
   std::string message;
   double last_solve_ms = 0.0, last_grid_ms = 0.0;
   bool device_ready = false;
+  void* stream = nullptr;
 };
 
 State& st() {
@@ -147,6 +148,7 @@ void build_grid(unsigned grid_type) {
     throw std::runtime_error("no CUDA device: the grid partition was built but the device engine is unavailable");
   }
   if (!s.engine) s.engine.reset(new lio::DeviceEngine());
+  s.engine->set_stream(s.stream);
   s.engine->set_precision(s.precision);
   s.engine->upload(s.sys, s.part);
   s.device_ready = true;
@@ -317,6 +319,45 @@ void g2g_solve_groups_(const unsigned* computation_type, double* fort_energy_ptr
     if (std::isnan(*fort_energy_ptr)) fail("XC energy is NaN", 2);
     (void)fort_forces_ptr;
   });
+}
+
+void g2g_set_stream_(void* cuda_stream) {
+  guarded("g2g_set_stream_", [&] {
+    State& s = st();
+    s.stream = cuda_stream;
+    if (s.engine) s.engine->set_stream(cuda_stream);
+  });
+}
+
+int g2g_solve_resident_(void) {
+  int n = -1;
+  guarded("g2g_solve_resident_", [&] {
+    State& s = st();
+    if (s.grid_type < 0 || !s.engine || !s.device_ready) throw std::runtime_error("no device grid");
+    lio::SolveRequest req;
+    req.resident = true;
+    s.engine->set_precision(s.precision);
+    s.engine->solve(req);
+    n = s.engine->launches_per_solve();
+  });
+  return n;
+}
+
+void g2g_profile_(const unsigned* on) {
+  guarded("g2g_profile_", [&] {
+    State& s = st();
+    if (s.engine) s.engine->set_profiling(*on != 0);
+  });
+}
+
+int g2g_stage_times_(double* ms, int* solves) {
+  int n = 0;
+  guarded("g2g_stage_times_", [&] {
+    State& s = st();
+    if (!s.engine) throw std::runtime_error("no device engine");
+    n = s.engine->stage_times(ms, 3, solves);
+  });
+  return n;
 }
 
 void g2g_deinit_(void) {
