@@ -193,7 +193,10 @@ def ours(args, rank, world):
 
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the legacy default stream (handle 0) would select the
+    # library's own stream, which torch's events do not see
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     wl = workload(rank)
     lib = G2GLibrary()
     L = lib.lib

@@ -28,3 +28,23 @@ def test_fp64_matches_reference(name, make):
     if wl.open_shell:
         assert np.max(np.abs(Kb - Kb_ref)) <= H.K_TOL
     print(name, E, E_ref, abs(E - E_ref), np.max(np.abs(K - K_ref)))
+
+
+# The 302-point configurations cannot run on the compiled reference (its angular
+# tables are compile-time), so their checker is the C restatement, which the
+# CPU tests pin to the reference on the 194-point grid.
+BIG = [("cfg2-302-closed-pbe", lambda: W.config(2)), ("cfg3-302-open-pbe", lambda: W.config(3))]
+
+
+@pytest.mark.parametrize("name,make", BIG, ids=[c[0] for c in BIG])
+def test_fp64_matches_restatement_302(name, make):
+    wl = make()
+    E_ref, K_ref, Kb_ref, npts = H.restatement(wl)
+    P = H.lib(H.os.path.join(H.ROOT, "lio_b200", "libg2g_b200.so"), True)
+    E, K, Kb = H.run(P, wl, precision=0)
+    assert P.partition_stats()["points"] == npts
+    assert abs(E - E_ref) <= H.E_TOL, (E, E_ref)
+    assert np.max(np.abs(K - K_ref)) <= H.K_TOL
+    if wl.open_shell:
+        assert np.max(np.abs(Kb - Kb_ref)) <= H.K_TOL
+    print(name, npts, E, E_ref, abs(E - E_ref), np.max(np.abs(K - K_ref)))
