@@ -124,8 +124,9 @@ int g2g_partition_group_(const int* g, int* meta, int* ids, double* xyzw, int* f
  * device work) and of the last partition build (ms, host clock). */
 void g2g_last_timings_(double* solve_ms, double* grid_ms);
 
-/* Runs all device work of this library on the given cudaStream_t (NULL: the
- * library's own stream). */
+/* Runs all device work of this library on the given cudaStream_t. NULL (the
+ * legacy default stream's handle) selects the library's own non-blocking
+ * stream, which does not order with the legacy default stream. */
 void g2g_set_stream_(void* cuda_stream);
 
 /* Device-resident solve: same work as g2g_solve_groups_(0) on the density that
@@ -142,6 +143,28 @@ int g2g_solve_resident_(void);
  * Returns the number of stages. */
 void g2g_profile_(const unsigned int* on);
 int g2g_stage_times_(double* ms, int* solves);
+
+/* No counterpart in the reference: an XC build that allocates no device
+ * memory, for callers that cannot call cudaMalloc (a host program whose
+ * allocator already owns all of the GPU's memory, or code that must not
+ * allocate while it runs). It performs the work of g2g_solve_groups_(0) on the
+ * current grid with device pointers: d_rho_a (closed shell: the packed total
+ * density; open shell: alpha) and d_rho_b (open shell: beta, else NULL) in the
+ * packed, doubled-off-diagonal layout; d_fock_a/d_fock_b receive the packed
+ * Kohn-Sham contributions ACCUMULATED (+=); d_energy (one double) is
+ * overwritten with E_xc. Every intermediate lives in one fixed 32 MiB device
+ * array inside the library (held by each GPU that loads it until the process
+ * exits); groups are processed in batches that fit, and a grid whose single
+ * largest group does not fit is rejected with an error (status -1, message in
+ * g2g_last_error_). The first call on a device looks up that array's device
+ * address (with the device current); make that first call before any stream
+ * capture. All calls share the array: calls that overlap on the GPU (on
+ * different streams or from different threads) race and corrupt each other.
+ * The grid itself (points, basis values) must already be resident, built by
+ * g2g_reload_atom_positions_. stream: a cudaStream_t, or NULL for the
+ * library's own stream. Returns 0 on success. */
+int g2g_solve_device_noalloc_(const double* d_rho_a, const double* d_rho_b, double* d_fock_a,
+                              double* d_fock_b, double* d_energy, void* stream);
 
 #ifdef __cplusplus
 }

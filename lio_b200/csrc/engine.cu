@@ -27,6 +27,8 @@
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <cstdint>
+#include <mutex>
 #include <vector>
 
 #include "engine.h"
@@ -738,6 +740,134 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
   res.energy = e;
   res.device_ms = ms;
   return res;
+}
+
+// ======================================================= no-allocation variant
+// Callers that cannot allocate device memory (an MD engine or SCF driver that
+// hands all of the GPU's memory to its own pool, or code running where a
+// cudaMalloc is not allowed to happen) use this path: the per-solve scratch of
+// the density, functional and energy stages sits in the fixed array below,
+// which every GPU that loads this library holds until the process exits.
+namespace {
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB
+constexpr size_t kNoAllocDoubles = kNoAllocScratchBytes / sizeof(double);
+constexpr size_t kNoAllocEnergySlots = 4096;  // one partial energy per batch
+__device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+std::mutex g_noalloc_mutex;
+double* g_noalloc_ptr[128] = {nullptr};
+
+// The host-side name g_noalloc_scratch is only a stand-in for the symbol; the
+// device address is looked up once per device, with that device current.
+double* noalloc_scratch_address() {
+  int dev = 0;
+  LIO_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) throw std::runtime_error("device ordinal out of range for the no-alloc scratch table");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    LIO_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  return g_noalloc_ptr[dev];
+}
+
+template <class T>
+T* shift_base(T* region, long long offset) {  // base such that base + offset == region
+  return reinterpret_cast<T*>(reinterpret_cast<uintptr_t>(region) - (uintptr_t)offset * sizeof(T));
+}
+}  // namespace
+
+size_t DeviceEngine::noalloc_scratch_bytes() { return kNoAllocScratchBytes; }
+
+void DeviceEngine::solve_noalloc(const double* rho_a, const double* rho_b, double* fock_a, double* fock_b,
+                                 double* energy, void* cuda_stream) {
+  Impl* d = impl_.get();
+  if (d->ngroups == 0) throw std::runtime_error("no grid uploaded");
+  if (!rho_a || !fock_a || !energy || (d->open && (!rho_b || !fock_b)))
+    throw std::runtime_error("null device pointer");
+  double* scratch = noalloc_scratch_address();
+  cudaStream_t st = cuda_stream ? (cudaStream_t)cuda_stream : d->stream;
+  const int nspin = d->open ? 2 : 1;
+  const int NQ = d->lda ? 1 : kNQ;
+  const size_t usable = kNoAllocDoubles - kNoAllocEnergySlots;
+  double* eparts = scratch;  // one partial energy per batch, all written before they are read
+  double* region = scratch + kNoAllocEnergySlots;
+
+  // per-group tile counts in the order upload() generated the tile lists
+  auto ndt = [](const GroupDev& G) { return (long long)(G.ldp / kTile) * G.nft; };
+  auto nft_ = [](const GroupDev& G) { return (long long)((G.ldp + kFuncBlock - 1) / kFuncBlock); };
+  auto nkt = [](const GroupDev& G) { return (long long)G.nft * (G.nft + 1) / 2; };
+  auto need = [&](const GroupDev& G) {
+    return (size_t)nspin * ((size_t)G.nft * NQ * G.ldp + G.ldp) + (size_t)nft_(G);
+  };
+  long long dt0 = 0, ft0 = 0, kt0 = 0;
+  int nbatch = 0;
+  int g0 = 0;
+  const int ng = (int)d->ngroups;
+  while (g0 < ng) {
+    size_t used = 0;
+    int g1 = g0;
+    long long nd = 0, nf = 0, nk = 0;
+    while (g1 < ng && used + need(d->hgroups[g1]) <= usable) {
+      used += need(d->hgroups[g1]);
+      nd += ndt(d->hgroups[g1]);
+      nf += nft_(d->hgroups[g1]);
+      nk += nkt(d->hgroups[g1]);
+      g1++;
+    }
+    if (g1 == g0)
+      throw std::runtime_error("group " + std::to_string(g0) + " needs " +
+                               std::to_string(need(d->hgroups[g0]) * sizeof(double)) +
+                               " bytes of scratch; the no-alloc entry point holds " +
+                               std::to_string(kNoAllocScratchBytes - kNoAllocEnergySlots * sizeof(double)));
+    if (nbatch >= (int)kNoAllocEnergySlots) throw std::runtime_error("too many batches for the no-alloc scratch");
+    const GroupDev& first = d->hgroups[g0];
+    long long part_len = 0, fac_len = 0;
+    for (int g = g0; g < g1; g++) {
+      part_len += (long long)d->hgroups[g].nft * NQ * d->hgroups[g].ldp;
+      fac_len += d->hgroups[g].ldp;
+    }
+    double* part_a = region;
+    double* part_b = part_a + part_len;
+    double* fac_a = part_b + (nspin == 2 ? part_len : 0);
+    double* fac_b = fac_a + fac_len;
+    double* eblk = fac_b + (nspin == 2 ? fac_len : 0);
+    double* pa = shift_base(part_a, first.part_off);
+    double* pb = shift_base(part_b, first.part_off);
+    double* fa = shift_base(fac_a, first.pt_off);
+    double* fb = shift_base(fac_b, first.pt_off);
+    for (int s = 0; s < nspin; s++) {
+      const double* P = s == 0 ? rho_a : rho_b;
+      if (d->lda)
+        k_density_fp64<1><<<(unsigned)nd, 256, 0, st>>>(d->dens_tiles.p + dt0, d->groups.p, d->fn_glob.p, d->basis.p,
+                                                          P, d->M, s == 0 ? pa : pb);
+      else
+        k_density_fp64<4><<<(unsigned)nd, 256, 0, st>>>(d->dens_tiles.p + dt0, d->groups.p, d->fn_glob.p, d->basis.p,
+                                                          P, d->M, s == 0 ? pa : pb);
+      LIO_CUDA(cudaGetLastError());
+    }
+    k_functional<<<(unsigned)nf, kFuncBlock, 0, st>>>(d->func_tiles.p + ft0, d->groups.p, d->pw.p, pa,
+                                                       d->open ? pb : nullptr, d->lda ? 1 : 0, d->open ? 1 : 0,
+                                                       d->iexch, fa, d->open ? fb : nullptr, eblk);
+    LIO_CUDA(cudaGetLastError());
+    k_sum_blocks<<<1, 1024, 0, st>>>(eblk, (int)nf, eparts + nbatch);
+    LIO_CUDA(cudaGetLastError());
+    if (d->open)
+      k_fock_fp64<2><<<(unsigned)nk, 256, 0, st>>>(d->fock_tiles.p + kt0, d->groups.p, d->fn_glob.p, d->basis.p,
+                                                    fa, fb, d->M, fock_a, fock_b);
+    else
+      k_fock_fp64<1><<<(unsigned)nk, 256, 0, st>>>(d->fock_tiles.p + kt0, d->groups.p, d->fn_glob.p, d->basis.p,
+                                                    fa, nullptr, d->M, fock_a, nullptr);
+    LIO_CUDA(cudaGetLastError());
+    dt0 += nd;
+    ft0 += nf;
+    kt0 += nk;
+    nbatch++;
+    g0 = g1;
+  }
+  k_sum_blocks<<<1, 1024, 0, st>>>(eparts, nbatch, energy);
+  LIO_CUDA(cudaGetLastError());
 }
 
 }  // namespace lio

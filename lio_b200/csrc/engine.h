@@ -60,6 +60,16 @@ class DeviceEngine {
   Precision precision() const { return precision_; }
   void release();
 
+  // Device-pointer solve that allocates nothing: every per-solve scratch
+  // buffer lives in one file-scope __device__ array of kNoAllocScratchBytes
+  // (engine.cu); groups are processed in batches that fit it. Inputs: packed
+  // densities in device memory (rho_b only for open shell). Outputs: packed
+  // Kohn-Sham vectors in device memory, accumulated (+=); the energy (one
+  // double in device memory) is overwritten. Throws on sizes beyond the array.
+  void solve_noalloc(const double* rho_a, const double* rho_b, double* fock_a, double* fock_b,
+                     double* energy, void* cuda_stream);
+  static size_t noalloc_scratch_bytes();
+
   // true when a CUDA device can be used from this process
   static bool available();
 

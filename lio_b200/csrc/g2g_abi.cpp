@@ -360,6 +360,18 @@ int g2g_stage_times_(double* ms, int* solves) {
   return n;
 }
 
+int g2g_solve_device_noalloc_(const double* d_rho_a, const double* d_rho_b, double* d_fock_a, double* d_fock_b,
+                              double* d_energy, void* stream) {
+  int rc = -1;
+  guarded("g2g_solve_device_noalloc_", [&] {
+    State& s = st();
+    if (s.grid_type < 0 || !s.engine || !s.device_ready) throw std::runtime_error("no device grid");
+    s.engine->solve_noalloc(d_rho_a, d_rho_b, d_fock_a, d_fock_b, d_energy, stream);
+    rc = 0;
+  });
+  return rc;
+}
+
 void g2g_deinit_(void) {
   guarded("g2g_deinit_", [] {
     State& s = st();
