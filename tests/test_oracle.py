@@ -1,0 +1,50 @@
+"""The oracle itself: the C restatement against the reference's golden vectors
+(tests/golden, produced by the reference's own CPU g2g path) and, when the
+reference build is present, against the reference live."""
+import os
+
+import numpy as np
+import pytest
+
+from lio_b200 import workloads as W
+
+from . import helpers as H
+from .golden.make_golden import CASES
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_restatement_matches_golden(name):
+    g = np.load(os.path.join(GOLD, f"{name}.npz"))
+    wl = CASES[name]()
+    E, K, Kb, npts = H.restatement(wl)
+    assert abs(E - float(g["E"])) <= 1e-10
+    assert np.max(np.abs(K - g["K"])) <= 1e-11
+    if wl.open_shell:
+        assert np.max(np.abs(Kb - g["Kb"])) <= 1e-11
+    assert npts == int(np.sum(g["npts"]))
+
+
+@pytest.mark.skipif(not os.path.exists(H.REF_LIB), reason="reference build absent")
+@pytest.mark.parametrize("seed,natoms,iexch,open_shell", [(101, 9, 9, False), (102, 7, 9, True), (103, 9, 3, False)])
+def test_restatement_matches_reference_live(seed, natoms, iexch, open_shell):
+    wl = W.small_workload(natoms, seed, iexch, open_shell)
+    E_r, K_r, Kb_r = H.reference(wl)
+    E, K, Kb, _ = H.restatement(wl)
+    assert abs(E - E_r) <= 1e-10
+    assert np.max(np.abs(K - K_r)) <= 1e-11
+    if open_shell:
+        assert np.max(np.abs(Kb - Kb_r)) <= 1e-11
+
+
+def test_restatement_sampling_partitions_groups():
+    """Strided samples of groups add up to the full build (the bounded-sample
+    CPU baseline and any group sharding rely on this)."""
+    wl = W.small_workload(8, 55, 9, True)
+    E, K, Kb, n = H.restatement(wl)
+    parts = [H.restatement(wl, first=r, stride=3) for r in range(3)]
+    assert abs(sum(p[0] for p in parts) - E) <= 1e-10
+    assert np.max(np.abs(sum(p[1] for p in parts) - K)) <= 1e-11
+    assert np.max(np.abs(sum(p[2] for p in parts) - Kb)) <= 1e-11
+    assert sum(p[3] for p in parts) == n

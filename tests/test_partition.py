@@ -1,0 +1,75 @@
+"""Host grid partition of the product library vs the reference, bit for bit
+(runs without a GPU: the partition is host work and stays inspectable through
+g2g_partition_group_ even when no device is present)."""
+import os
+
+import numpy as np
+import pytest
+
+from lio_b200 import workloads as W
+
+from . import helpers as H
+from .golden.make_golden import CASES
+
+PROD = os.path.join(H.ROOT, "lio_b200", "libg2g_b200.so")
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def product_groups(wl, options=None):
+    L = H.lib(PROD, True)
+    gt = H.bind(L, wl, options=options)
+    L.reload_atom_positions(gt)  # without a GPU this reports the missing device after building the partition
+    out = {}
+    for g in range(L.num_groups()):
+        d = L.partition_group(g)
+        out[tuple(sorted(map(tuple, d["ids"].tolist())))] = d
+    return out
+
+
+def reference_groups(wl, options=None):
+    L = H.lib(H.REF_LIB, False)
+    L.init()
+    gt = H.bind(L, wl, options=options)
+    L.reload_atom_positions(gt)
+    out = {}
+    for g in range(L.num_groups(ref=True)):
+        d = L.partition_group(g, ref=True)
+        out[tuple(sorted(map(tuple, d["ids"].tolist())))] = d
+    L.deinit()
+    return out
+
+
+def assert_same(a, b):
+    assert set(a) == set(b)
+    for k in a:
+        x, y = a[k], b[k]
+        ix, iy = np.lexsort(x["ids"].T[::-1]), np.lexsort(y["ids"].T[::-1])
+        assert x["meta"][:6] == y["meta"][:6]
+        assert np.array_equal(x["funcs"], y["funcs"])
+        assert np.array_equal(x["xyzw"][ix].view(np.uint64), y["xyzw"][iy].view(np.uint64))  # bitwise
+
+
+@pytest.mark.skipif(not os.path.exists(H.REF_LIB), reason="reference build absent")
+@pytest.mark.parametrize("make,options", [
+    (lambda: W.config(1), None),
+    (lambda: W.small_workload(16, 7, 9, False), None),
+    (lambda: W.small_workload(12, 11, 9, True), dict(lcs=5.0, sr=0.4)),
+    (lambda: W.small_workload(10, 13, 9, False), dict(mfe=12, mppc=20)),
+    (lambda: W.small_workload(9, 17, 9, False), dict(rzw=False)),
+    (lambda: W.small_workload(8, 19, 3, False), dict(aaf=True, sr=0.0)),
+], ids=["cfg1", "pbe16", "small-cubes", "mfe12-mppc20", "keep-zero-weights", "all-functions-no-spheres"])
+def test_partition_bit_exact_vs_reference(make, options):
+    wl = make()
+    assert_same(product_groups(wl, options), reference_groups(wl, options))
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_partition_matches_golden_summary(name):
+    g = np.load(os.path.join(GOLD, f"{name}.npz"))
+    groups = product_groups(CASES[name]())
+    npts = np.array([d["meta"][0] for d in groups.values()])
+    nfun = np.array([d["meta"][5] for d in groups.values()])
+    wsum = np.array([float(np.sum(d["xyzw"][:, 3])) for d in groups.values()])
+    o = np.lexsort((wsum, nfun, npts))
+    assert np.array_equal(npts[o], g["npts"]) and np.array_equal(nfun[o], g["nfun"])
+    assert np.array_equal(wsum[o], g["wsum"])
