@@ -125,7 +125,9 @@ def bind(lib: G2GLibrary, wl: W.Workload):
     return 3
 
 
-def workload(rank: int) -> W.Workload:
+def workload(rank: int, name: str = "cfg3") -> W.Workload:
+    if name == "cfg2":  # 64-atom closed-shell PBE, 40x302 (small case for profiling)
+        return W.config(2)
     if rank == 0:
         return W.config(3)
     return W.make_workload(f"cfg3-rank{rank}", {"C": 64, "N": 16, "O": 16, "H": 160}, 22.0, 3000 + 17 * rank, 9,
@@ -197,7 +199,7 @@ def ours(args, rank, world):
     # library's own stream, which torch's events do not see
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    wl = workload(rank)
+    wl = workload(rank, args.workload)
     lib = G2GLibrary()
     L = lib.lib
     L.g2g_set_stream_(C.c_void_p(stream.cuda_stream))
@@ -279,7 +281,7 @@ def ours(args, rank, world):
         "metric": METRIC, "value": total_pts / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if args.precision == 0 else "i8-split/f64", "data": "synthetic",
-        "config": {"workload": "cfg3: 256 atoms 64C16N16O160H, 40x302 grid, open-shell PBE (Iexch 9)",
+        "config": {"workload": wl.name,
                    "points": npts, "groups": st["groups"], "M": wl.basis.M,
                    "precision": "fp64" if args.precision == 0 else "tensor",
                    "l2": "inputs larger than L2 (resident basis cache of %.1f GB)" % (nk * pm * 8 / 1e9),
@@ -308,6 +310,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", type=int, default=0, help="0 = FP64 plain, 1 = tensor-core form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="cfg3", choices=["cfg3", "cfg2"],
+                    help="cfg3 = the 256-atom headline workload; cfg2 = the 64-atom case used for ncu captures")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

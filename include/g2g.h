@@ -166,6 +166,13 @@ int g2g_stage_times_(double* ms, int* solves);
 int g2g_solve_device_noalloc_(const double* d_rho_a, const double* d_rho_b, double* d_fock_a,
                               double* d_fock_b, double* d_energy, void* stream);
 
+/* Diagnostic (no counterpart in the reference): runs one tcgen05 int8 tensor-
+ * core product D[128 x N] = A[128 x K] * B[N x K]^T (row-major host arrays,
+ * 16 <= N <= 256 with N % 16 == 0, 32 <= K <= 256 with K % 32 == 0) so the
+ * shared-memory descriptor and TMEM layouts can be checked exactly. Returns 0
+ * on success, 1 if the completion wait timed out, < 0 on a setup error. */
+int lio_tc_selftest_(int N, int K, const signed char* A, const signed char* B, int* D);
+
 #ifdef __cplusplus
 }
 #endif

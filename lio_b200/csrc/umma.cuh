@@ -1,0 +1,117 @@
+// Minimal sm_100a tensor-core (tcgen05 / UMMA) primitives in inline PTX.
+//
+// Shared-memory operands use the K-major, no-swizzle ("interleaved") canonical
+// layout: a core matrix is 8 rows x 16 bytes stored as 128 contiguous bytes
+// (row r at byte 16*r); core matrices of consecutive 8-row groups are SBO
+// bytes apart and the two 16-byte K halves of one 32-byte MMA K step are LBO
+// bytes apart. For an R-row operand holding the whole K extent we use
+//   offset(r, k) = (k / 16) * (16 * R) + (r / 8) * 128 + (r % 8) * 16 + (k % 16)
+// i.e. SBO = 128 and LBO = 16 * R, so K step kk starts at byte 32 * R * kk.
+//
+// Every wait on an mbarrier is bounded: after kSpinLimit polls it gives up and
+// reports failure to the caller, which records an error flag and returns
+// without hanging the GPU.
+#pragma once
+#include <cstdint>
+
+namespace lio {
+namespace umma {
+
+constexpr uint32_t kSpinLimit = 1u << 26;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// offset of element (r, k) of an R-row K-major operand in the layout above
+__host__ __device__ __forceinline__ uint32_t kmajor_offset(uint32_t r, uint32_t k, uint32_t R) {
+  return (k >> 4) * (16u * R) + (r >> 3) * 128u + (r & 7u) * 16u + (k & 15u);
+}
+
+// shared-memory matrix descriptor (sm_100 format: version 1, no swizzle)
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+  return d;                // base offset 0, legacy LBO mode, layout type 0 (no swizzle)
+}
+
+// instruction descriptor: s8 x s8 -> s32, both operands K-major, M x N
+__host__ __device__ constexpr uint32_t idesc_i8(uint32_t M, uint32_t N) {
+  return (2u << 4)            // D format S32
+         | (1u << 7)          // A signed 8-bit
+         | (1u << 10)         // B signed 8-bit
+         | ((N >> 3) << 17)   // N / 8
+         | ((M >> 4) << 24);  // M / 16
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+// arrives on the mbarrier once every MMA issued so far by this thread is done
+__device__ __forceinline__ void commit(uint64_t* mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
+}
+
+// bounded wait for the phase with the given parity; returns false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity) {
+  const uint32_t a = smem_u32(mbar);
+  for (uint32_t i = 0; i < kSpinLimit; i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P;\n\t}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void fence_before_sync() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_after_sync() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// warp-wide: allocate ncols TMEM columns (power of two >= 32), base address to *dst
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// warp-wide: 8 consecutive 32-bit columns of this warp's 32 TMEM lanes
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, int32_t (&v)[8]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+}  // namespace umma
+}  // namespace lio
