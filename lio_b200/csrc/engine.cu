@@ -47,6 +47,7 @@ namespace lio {
 namespace {
 
 constexpr int kTile = 64;    // points / functions per GEMM tile
+constexpr int kPointPad = 128;  // points per group padded to a multiple of this
 constexpr int kKStep = 16;   // reduction step of the FP64 GEMMs
 constexpr int kBasisBlock = 128;
 constexpr int kFuncBlock = 128;
@@ -54,12 +55,17 @@ constexpr int kNQ = 10;      // rho, grad[3], (xx,yy,zz), (xy,xz,yz)
 
 struct GroupDev {
   int npts, ldp, m, nsimple;
-  int nft, pad0, pad1, pad2;
+  int nft, m32, pad1, pad2;  // m32: m rounded up to 32 (tensor-core K extent)
   long long pt_off;    // point arrays
-  long long fn_off;    // fn_glob
+  long long fn_off;    // fn_glob, fn_sh, fn_cp
   long long sf_off;    // sf_glob / sf_type
   long long bas_off;   // basis cache (elements)
   long long part_off;  // partial densities (elements, one spin)
+  long long rad_off;   // radial cache (elements): 3 x nsimple x ldp
+  long long sl_off;    // int8 slices of the density A operands (bytes)
+  long long aexp_off;  // their per-point exponents (elements): NA x ldp
+  long long ds_off;    // int8 slices of the density matrix (bytes, one spin)
+  long long dexp_off;  // their per-function exponents (elements): nft x 64
 };
 
 template <class T>
@@ -437,6 +443,45 @@ __global__ void __launch_bounds__(256) k_fock_fp64(const int4* __restrict__ tile
   }
 }
 
+// radial parts (t, tg, th) of every simple function at every point (per
+// geometry), the input of the tensor-core epilogue's basis rebuild
+__global__ void k_radial(const int2* __restrict__ tiles, const GroupDev* __restrict__ groups,
+                         const double* __restrict__ px, const double* __restrict__ py, const double* __restrict__ pz,
+                         const int* __restrict__ sf_glob, const int* __restrict__ nuc, const int* __restrict__ ncont,
+                         const double* __restrict__ ca, const double* __restrict__ cc, const double* __restrict__ ax,
+                         const double* __restrict__ ay, const double* __restrict__ az, double* __restrict__ radial) {
+  const int2 t = tiles[blockIdx.x];
+  const GroupDev G = groups[t.x];
+  const int p = t.y * kBasisBlock + threadIdx.x;
+  if (p >= G.ldp) return;
+  const bool valid = p < G.npts;
+  const double x = px[G.pt_off + p], y = py[G.pt_off + p], z = pz[G.pt_off + p];
+  const long long rs = (long long)G.nsimple * G.ldp;
+  double* out = radial + G.rad_off;
+  for (int sf = 0; sf < G.nsimple; sf++) {
+    const int gf = sf_glob[G.sf_off + sf];
+    const int atom = nuc[gf];
+    const double dx = x - ax[atom], dy = y - ay[atom], dz = z - az[atom];
+    const double dist = dx * dx + dy * dy + dz * dz;
+    double tt = 0.0, tg = 0.0, th = 0.0;
+    for (int k = 0; k < ncont[gf]; k++) {
+      const double a = ca[gf * 13 + k], c = cc[gf * 13 + k];
+      const double expo = a * dist;
+      if (expo > 70.0) continue;
+      const double t0 = exp(-expo) * c;
+      tt += t0;
+      tg += t0 * a;
+      th += t0 * (a * a);
+    }
+    const long long o = (long long)sf * G.ldp + p;
+    out[o] = valid ? tt : 0.0;
+    out[rs + o] = valid ? tg : 0.0;
+    out[2 * rs + o] = valid ? th : 0.0;
+  }
+}
+
+#include "density_tc.cuh"
+
 }  // namespace
 
 // ============================================================================ Impl
@@ -449,7 +494,18 @@ struct DeviceEngine::Impl {
   std::vector<GroupDev> hgroups;
   DevBuf<GroupDev> groups;
   DevBuf<double> px, py, pz, pw;
-  DevBuf<int> fn_glob, sf_glob, sf_type, nuc, ncont;
+  DevBuf<int> fn_glob, sf_glob, sf_type, nuc, ncont, fn_sh;
+  DevBuf<int8_t> fn_cp;
+  // tensor-core form (built on first use per geometry)
+  DevBuf<int2> slice_basis_tiles, slice_dens_tiles;
+  DevBuf<int4> tc_tiles;
+  DevBuf<double> radial;
+  DevBuf<int8_t> aslices, dslices_a, dslices_b;
+  DevBuf<int16_t> aexp, dexp_a, dexp_b;
+  DevBuf<int> tc_err;
+  long long tc_sizes[5] = {0, 0, 0, 0, 0};
+  bool tc_ready = false;
+  double d_norm = 1.0;
   DevBuf<double> ca, cc, ax, ay, az;
   DevBuf<double> basis;
   DevBuf<int2> basis_tiles, func_tiles;
@@ -543,22 +599,27 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
   d->open = sys.open;
   d->iexch = sys.iexch;
   d->nk = sys.lda ? 1 : 10;
+  d->d_norm = sys.d_norm;
   const int NQ = sys.lda ? 1 : kNQ;
 
   std::vector<GroupDev> gd;
   std::vector<double> hx, hy, hz, hw;
-  std::vector<int> hfn, hsf, hst;
-  std::vector<int2> btiles, ftiles;
-  std::vector<int4> dtiles, ktiles;
+  std::vector<int> hfn, hsf, hst, hfsh;
+  std::vector<int8_t> hfcp;
+  std::vector<int2> btiles, ftiles, sbtiles, sdtiles;
+  std::vector<int4> dtiles, ktiles, tctiles;
   long long pt_off = 0, fn_off = 0, sf_off = 0, bas_off = 0, part_off = 0;
+  long long rad_off = 0, sl_off = 0, aexp_off = 0, ds_off = 0, dexp_off = 0;
   long long npts_total = 0;
+  const int NA = sys.lda ? 1 : 4;
   const int ngr = part.total_groups();
   for (int g = 0; g < ngr; g++) {
     const PointGroup& pg = part.group(g);
     GroupDev G{};
     G.npts = (int)pg.points.size();
-    G.ldp = ((G.npts + kTile - 1) / kTile) * kTile;
+    G.ldp = ((G.npts + kPointPad - 1) / kPointPad) * kPointPad;
     G.m = pg.total_functions();
+    G.m32 = ((G.m + 31) / 32) * 32;
     G.nsimple = (int)pg.funcs.size();
     G.nft = (G.m + kTile - 1) / kTile;
     G.pt_off = pt_off;
@@ -566,6 +627,11 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
     G.sf_off = sf_off;
     G.bas_off = bas_off;
     G.part_off = part_off;
+    G.rad_off = rad_off;
+    G.sl_off = sl_off;
+    G.aexp_off = aexp_off;
+    G.ds_off = ds_off;
+    G.dexp_off = dexp_off;
     for (int p = 0; p < G.ldp; p++) {
       if (p < G.npts) {
         const GridPoint& q = pg.points[p];
@@ -586,7 +652,13 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
       hsf.push_back(f);
       hst.push_back(type);
       const int ncomp = type == 0 ? 1 : (type == 1 ? 3 : 6);
-      for (int k = 0; k < ncomp; k++) hfn.push_back(f + k);
+      const int c0 = type == 0 ? 0 : (type == 1 ? 1 : 4);
+      for (int k = 0; k < ncomp; k++) {
+        hfn.push_back(f + k);
+        hfsh.push_back((int)i);
+        const bool normed = type == 2 && (k == 0 || k == 2 || k == 5);
+        hfcp.push_back((int8_t)((c0 + k) | (normed ? 16 : 0)));
+      }
     }
     for (int b = 0; b < G.ldp / kBasisBlock + (G.ldp % kBasisBlock ? 1 : 0); b++) btiles.push_back({g, b});
     for (int b = 0; b < (G.ldp + kFuncBlock - 1) / kFuncBlock; b++) ftiles.push_back({g, b});
@@ -594,14 +666,30 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
       for (int ft = 0; ft < G.nft; ft++) dtiles.push_back({g, pt, ft, 0});
     for (int it = 0; it < G.nft; it++)
       for (int jt = it; jt < G.nft; jt++) ktiles.push_back({g, it, jt, 0});
+    for (int T = 0; T < G.ldp / kTcPoints; T++) {
+      sbtiles.push_back({g, T});
+      for (int ft = 0; ft < G.nft; ft++) tctiles.push_back({g, T, ft, 0});
+    }
+    for (int ft = 0; ft < G.nft; ft++) sdtiles.push_back({g, ft});
     pt_off += G.ldp;
     fn_off += G.m;
     sf_off += G.nsimple;
     bas_off += (long long)d->nk * G.m * G.ldp;
     part_off += (long long)G.nft * NQ * G.ldp;
+    rad_off += 3LL * G.nsimple * G.ldp;
+    sl_off += (long long)kSlices * NA * G.ldp * G.m32;
+    aexp_off += (long long)NA * G.ldp;
+    ds_off += (long long)G.nft * kSlices * kTcFuncs * G.m32;
+    dexp_off += (long long)G.nft * kTcFuncs;
     npts_total += G.npts;
     gd.push_back(G);
   }
+  d->tc_sizes[0] = rad_off;
+  d->tc_sizes[1] = sl_off;
+  d->tc_sizes[2] = aexp_off;
+  d->tc_sizes[3] = ds_off;
+  d->tc_sizes[4] = dexp_off;
+  d->tc_ready = false;
   d->hgroups = gd;
   d->ngroups = ngr;
   d->npoints = npts_total;
@@ -618,6 +706,11 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
   d->pz.upload(hz);
   d->pw.upload(hw);
   d->fn_glob.upload(hfn);
+  d->fn_sh.upload(hfsh);
+  d->fn_cp.upload(hfcp);
+  d->slice_basis_tiles.upload(sbtiles);
+  d->slice_dens_tiles.upload(sdtiles);
+  d->tc_tiles.upload(tctiles);
   d->sf_glob.upload(hsf);
   d->sf_type.upload(hst);
   d->nuc.upload(hnuc);
@@ -663,6 +756,39 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
   LIO_CUDA(cudaStreamSynchronize(d->stream));
 }
 
+// Builds the tensor-core operands of the current geometry: radial cache and
+// int8 slices of the density A operands (F, and for GGA its gradient).
+void DeviceEngine::prepare_tensor_core() {
+  Impl* d = impl_.get();
+  cudaStream_t st = d->stream;
+  d->radial.alloc(d->tc_sizes[0]);
+  d->aslices.alloc(d->tc_sizes[1]);
+  d->aexp.alloc(d->tc_sizes[2]);
+  d->dslices_a.alloc(d->tc_sizes[3]);
+  d->dexp_a.alloc(d->tc_sizes[4]);
+  if (d->open) {
+    d->dslices_b.alloc(d->tc_sizes[3]);
+    d->dexp_b.alloc(d->tc_sizes[4]);
+  }
+  d->tc_err.alloc(1);
+  LIO_CUDA(cudaMemsetAsync(d->tc_err.p, 0, sizeof(int), st));
+  k_radial<<<(unsigned)d->basis_tiles.n, kBasisBlock, 0, st>>>(d->basis_tiles.p, d->groups.p, d->px.p, d->py.p,
+                                                               d->pz.p, d->sf_glob.p, d->nuc.p, d->ncont.p, d->ca.p,
+                                                               d->cc.p, d->ax.p, d->ay.p, d->az.p, d->radial.p);
+  LIO_CUDA(cudaGetLastError());
+  if (d->lda)
+    k_slice_basis<1><<<(unsigned)d->slice_basis_tiles.n, kTcPoints, 0, st>>>(d->slice_basis_tiles.p, d->groups.p,
+                                                                            d->basis.p, d->aslices.p, d->aexp.p);
+  else
+    k_slice_basis<4><<<(unsigned)d->slice_basis_tiles.n, kTcPoints, 0, st>>>(d->slice_basis_tiles.p, d->groups.p,
+                                                                            d->basis.p, d->aslices.p, d->aexp.p);
+  LIO_CUDA(cudaGetLastError());
+  const int smem = (int)(kTcSmemA + kTcSmemB);
+  LIO_CUDA(cudaFuncSetAttribute(k_density_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  LIO_CUDA(cudaFuncSetAttribute(k_density_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  d->tc_ready = true;
+}
+
 SolveResult DeviceEngine::solve(const SolveRequest& req) {
   Impl* d = impl_.get();
   SolveResult res;
@@ -684,15 +810,39 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
   d->collect();
   d->mark(0);
   const int nspin = d->open ? 2 : 1;
+  const bool tc = precision_ == Precision::TensorCore;
+  if (tc && !d->tc_ready) {
+    prepare_tensor_core();
+    d->mark(0);
+  }
   for (int s = 0; s < nspin; s++) {
     const double* P = s == 0 ? d->P_a.p : d->P_b.p;
     double* part = s == 0 ? d->part_a.p : d->part_b.p;
-    if (d->lda)
-      k_density_fp64<1><<<nd, 256, 0, st>>>(d->dens_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, P, d->M, part);
-    else
-      k_density_fp64<4><<<nd, 256, 0, st>>>(d->dens_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, P, d->M, part);
-    LIO_CUDA(cudaGetLastError());
-    launches++;
+    if (tc) {
+      int8_t* dsl = s == 0 ? d->dslices_a.p : d->dslices_b.p;
+      int16_t* dex = s == 0 ? d->dexp_a.p : d->dexp_b.p;
+      k_slice_density<<<(unsigned)d->slice_dens_tiles.n, kTcFuncs, 0, st>>>(d->slice_dens_tiles.p, d->groups.p,
+                                                                          d->fn_glob.p, P, d->M, dsl, dex);
+      LIO_CUDA(cudaGetLastError());
+      const size_t smem = kTcSmemA + kTcSmemB;
+      if (d->lda)
+        k_density_tc<1><<<(unsigned)d->tc_tiles.n, 128, smem, st>>>(
+            d->tc_tiles.p, d->groups.p, d->aslices.p, d->aexp.p, dsl, dex, d->radial.p, d->px.p, d->py.p, d->pz.p,
+            d->fn_sh.p, d->fn_cp.p, d->sf_glob.p, d->nuc.p, d->ax.p, d->ay.p, d->az.p, d->d_norm, part, d->tc_err.p);
+      else
+        k_density_tc<4><<<(unsigned)d->tc_tiles.n, 128, smem, st>>>(
+            d->tc_tiles.p, d->groups.p, d->aslices.p, d->aexp.p, dsl, dex, d->radial.p, d->px.p, d->py.p, d->pz.p,
+            d->fn_sh.p, d->fn_cp.p, d->sf_glob.p, d->nuc.p, d->ax.p, d->ay.p, d->az.p, d->d_norm, part, d->tc_err.p);
+      LIO_CUDA(cudaGetLastError());
+      launches += 2;
+    } else {
+      if (d->lda)
+        k_density_fp64<1><<<nd, 256, 0, st>>>(d->dens_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, P, d->M, part);
+      else
+        k_density_fp64<4><<<nd, 256, 0, st>>>(d->dens_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, P, d->M, part);
+      LIO_CUDA(cudaGetLastError());
+      launches++;
+    }
   }
   d->mark(1);
   k_functional<<<nf, kFuncBlock, 0, st>>>(d->func_tiles.p, d->groups.p, d->pw.p, d->part_a.p,
@@ -735,6 +885,11 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
     }
   }
   LIO_CUDA(cudaStreamSynchronize(st));
+  if (tc) {
+    int flag = 0;
+    LIO_CUDA(cudaMemcpy(&flag, d->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) throw std::runtime_error("tensor-core density: an MMA completion wait timed out");
+  }
   float ms = 0.f;
   LIO_CUDA(cudaEventElapsedTime(&ms, d->ev0, d->ev1));
   res.energy = e;

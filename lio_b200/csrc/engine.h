@@ -78,6 +78,7 @@ class DeviceEngine {
   long long groups() const;
 
  private:
+  void prepare_tensor_core();
   struct Impl;
   std::unique_ptr<Impl> impl_;
   Precision precision_ = Precision::FP64;

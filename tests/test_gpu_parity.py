@@ -48,3 +48,31 @@ def test_fp64_matches_restatement_302(name, make):
     if wl.open_shell:
         assert np.max(np.abs(Kb - Kb_ref)) <= H.K_TOL
     print(name, npts, E, E_ref, abs(E - E_ref), np.max(np.abs(K - K_ref)))
+
+
+# Tensor-core form (precision 1): the density contraction runs as int8
+# Ozaki-slice products on tcgen05; same tolerances as the FP64 form.
+@pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
+def test_tensor_core_matches_reference(name, make):
+    wl = make()
+    E_ref, K_ref, Kb_ref = H.reference(wl)
+    P = H.lib(H.os.path.join(H.ROOT, "lio_b200", "libg2g_b200.so"), True)
+    E, K, Kb = H.run(P, wl, precision=1)
+    print(name, "tc", E, E_ref, abs(E - E_ref), np.max(np.abs(K - K_ref)))
+    assert abs(E - E_ref) <= H.E_TOL, (E, E_ref)
+    assert np.max(np.abs(K - K_ref)) <= H.K_TOL
+    if wl.open_shell:
+        assert np.max(np.abs(Kb - Kb_ref)) <= H.K_TOL
+
+
+@pytest.mark.parametrize("name,make", BIG, ids=[c[0] for c in BIG])
+def test_tensor_core_matches_restatement_302(name, make):
+    wl = make()
+    E_ref, K_ref, Kb_ref, npts = H.restatement(wl)
+    P = H.lib(H.os.path.join(H.ROOT, "lio_b200", "libg2g_b200.so"), True)
+    E, K, Kb = H.run(P, wl, precision=1)
+    print(name, "tc", npts, E, E_ref, abs(E - E_ref), np.max(np.abs(K - K_ref)))
+    assert abs(E - E_ref) <= H.E_TOL, (E, E_ref)
+    assert np.max(np.abs(K - K_ref)) <= H.K_TOL
+    if wl.open_shell:
+        assert np.max(np.abs(Kb - Kb_ref)) <= H.K_TOL
