@@ -55,7 +55,7 @@ constexpr int kNQ = 10;      // rho, grad[3], (xx,yy,zz), (xy,xz,yz)
 
 struct GroupDev {
   int npts, ldp, m, nsimple;
-  int nft, m32, pad1, pad2;  // m32: m rounded up to 32 (tensor-core K extent)
+  int nft, m32, nft32, pad2;  // m32: m rounded up to 32; nft32: tensor-core function tiles
   long long pt_off;    // point arrays
   long long fn_off;    // fn_glob, fn_sh, fn_cp
   long long sf_off;    // sf_glob / sf_type
@@ -319,7 +319,7 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
 // rho * w * (ex + ec) (g2g/cpu/iteration.cpp:106-114, 199-208, 482-492).
 __global__ void k_functional(const int2* __restrict__ tiles, const GroupDev* __restrict__ groups,
                              const double* __restrict__ pw, const double* __restrict__ part_a,
-                             const double* __restrict__ part_b, int lda, int open, int iexch,
+                             const double* __restrict__ part_b, int part_tile, int lda, int open, int iexch,
                              double* __restrict__ fac_a, double* __restrict__ fac_b,
                              double* __restrict__ energy_blocks) {
   __shared__ double sh[32];
@@ -332,7 +332,8 @@ __global__ void k_functional(const int2* __restrict__ tiles, const GroupDev* __r
     const int NQ = lda ? 1 : kNQ;
     double qa[kNQ], qb[kNQ];
     for (int k = 0; k < kNQ; k++) qa[k] = qb[k] = 0.0;
-    for (int f = 0; f < G.nft; f++)
+    const int nparts = (G.m + part_tile - 1) / part_tile;  // partial tiles written by the density stage
+    for (int f = 0; f < nparts; f++)
       for (int k = 0; k < NQ; k++) {
         const long long o = G.part_off + ((long long)f * NQ + k) * G.ldp + p;
         qa[k] += part_a[o];
@@ -494,11 +495,11 @@ struct DeviceEngine::Impl {
   std::vector<GroupDev> hgroups;
   DevBuf<GroupDev> groups;
   DevBuf<double> px, py, pz, pw;
-  DevBuf<int> fn_glob, sf_glob, sf_type, nuc, ncont, fn_sh;
+  DevBuf<int> fn_glob, sf_glob, sf_type, nuc, ncont, fn_sh, fn_atom;
   DevBuf<int8_t> fn_cp;
   // tensor-core form (built on first use per geometry)
   DevBuf<int2> slice_basis_tiles, slice_dens_tiles;
-  DevBuf<int4> tc_tiles;
+
   DevBuf<double> radial;
   DevBuf<int8_t> aslices, dslices_a, dslices_b;
   DevBuf<int16_t> aexp, dexp_a, dexp_b;
@@ -604,7 +605,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
 
   std::vector<GroupDev> gd;
   std::vector<double> hx, hy, hz, hw;
-  std::vector<int> hfn, hsf, hst, hfsh;
+  std::vector<int> hfn, hsf, hst, hfsh, hfat;
   std::vector<int8_t> hfcp;
   std::vector<int2> btiles, ftiles, sbtiles, sdtiles;
   std::vector<int4> dtiles, ktiles, tctiles;
@@ -622,6 +623,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
     G.m32 = ((G.m + 31) / 32) * 32;
     G.nsimple = (int)pg.funcs.size();
     G.nft = (G.m + kTile - 1) / kTile;
+    G.nft32 = (G.m + kTcFuncs - 1) / kTcFuncs;
     G.pt_off = pt_off;
     G.fn_off = fn_off;
     G.sf_off = sf_off;
@@ -656,6 +658,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
       for (int k = 0; k < ncomp; k++) {
         hfn.push_back(f + k);
         hfsh.push_back((int)i);
+        hfat.push_back(sys.nuc[f]);
         const bool normed = type == 2 && (k == 0 || k == 2 || k == 5);
         hfcp.push_back((int8_t)((c0 + k) | (normed ? 16 : 0)));
       }
@@ -668,9 +671,9 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
       for (int jt = it; jt < G.nft; jt++) ktiles.push_back({g, it, jt, 0});
     for (int T = 0; T < G.ldp / kTcPoints; T++) {
       sbtiles.push_back({g, T});
-      for (int ft = 0; ft < G.nft; ft++) tctiles.push_back({g, T, ft, 0});
+      (void)T;
     }
-    for (int ft = 0; ft < G.nft; ft++) sdtiles.push_back({g, ft});
+    for (int ft = 0; ft < G.nft32; ft++) sdtiles.push_back({g, ft});
     pt_off += G.ldp;
     fn_off += G.m;
     sf_off += G.nsimple;
@@ -679,8 +682,8 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
     rad_off += 3LL * G.nsimple * G.ldp;
     sl_off += (long long)kSlices * NA * G.ldp * G.m32;
     aexp_off += (long long)NA * G.ldp;
-    ds_off += (long long)G.nft * kSlices * kTcFuncs * G.m32;
-    dexp_off += (long long)G.nft * kTcFuncs;
+    ds_off += (long long)G.nft32 * kSlices * kTcFuncs * G.m32;
+    dexp_off += (long long)G.nft32 * kTcFuncs;
     npts_total += G.npts;
     gd.push_back(G);
   }
@@ -707,10 +710,11 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
   d->pw.upload(hw);
   d->fn_glob.upload(hfn);
   d->fn_sh.upload(hfsh);
+  d->fn_atom.upload(hfat);
   d->fn_cp.upload(hfcp);
   d->slice_basis_tiles.upload(sbtiles);
   d->slice_dens_tiles.upload(sdtiles);
-  d->tc_tiles.upload(tctiles);
+  (void)tctiles;
   d->sf_glob.upload(hsf);
   d->sf_type.upload(hst);
   d->nuc.upload(hnuc);
@@ -783,9 +787,8 @@ void DeviceEngine::prepare_tensor_core() {
     k_slice_basis<4><<<(unsigned)d->slice_basis_tiles.n, kTcPoints, 0, st>>>(d->slice_basis_tiles.p, d->groups.p,
                                                                             d->basis.p, d->aslices.p, d->aexp.p);
   LIO_CUDA(cudaGetLastError());
-  const int smem = (int)(kTcSmemA + kTcSmemB);
-  LIO_CUDA(cudaFuncSetAttribute(k_density_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  LIO_CUDA(cudaFuncSetAttribute(k_density_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  LIO_CUDA(cudaFuncSetAttribute(k_density_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TcCfg<1>::kSmem));
+  LIO_CUDA(cudaFuncSetAttribute(k_density_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TcCfg<4>::kSmem));
   d->tc_ready = true;
 }
 
@@ -824,15 +827,14 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
       k_slice_density<<<(unsigned)d->slice_dens_tiles.n, kTcFuncs, 0, st>>>(d->slice_dens_tiles.p, d->groups.p,
                                                                           d->fn_glob.p, P, d->M, dsl, dex);
       LIO_CUDA(cudaGetLastError());
-      const size_t smem = kTcSmemA + kTcSmemB;
       if (d->lda)
-        k_density_tc<1><<<(unsigned)d->tc_tiles.n, 128, smem, st>>>(
-            d->tc_tiles.p, d->groups.p, d->aslices.p, d->aexp.p, dsl, dex, d->radial.p, d->px.p, d->py.p, d->pz.p,
-            d->fn_sh.p, d->fn_cp.p, d->sf_glob.p, d->nuc.p, d->ax.p, d->ay.p, d->az.p, d->d_norm, part, d->tc_err.p);
+        k_density_tc<1><<<(unsigned)d->slice_basis_tiles.n, TcCfg<1>::kThreads, TcCfg<1>::kSmem, st>>>(
+            d->slice_basis_tiles.p, d->groups.p, d->aslices.p, d->aexp.p, dsl, dex, d->radial.p, d->px.p, d->py.p,
+            d->pz.p, d->fn_sh.p, d->fn_cp.p, d->fn_atom.p, d->ax.p, d->ay.p, d->az.p, d->d_norm, part, d->tc_err.p);
       else
-        k_density_tc<4><<<(unsigned)d->tc_tiles.n, 128, smem, st>>>(
-            d->tc_tiles.p, d->groups.p, d->aslices.p, d->aexp.p, dsl, dex, d->radial.p, d->px.p, d->py.p, d->pz.p,
-            d->fn_sh.p, d->fn_cp.p, d->sf_glob.p, d->nuc.p, d->ax.p, d->ay.p, d->az.p, d->d_norm, part, d->tc_err.p);
+        k_density_tc<4><<<(unsigned)d->slice_basis_tiles.n, TcCfg<4>::kThreads, TcCfg<4>::kSmem, st>>>(
+            d->slice_basis_tiles.p, d->groups.p, d->aslices.p, d->aexp.p, dsl, dex, d->radial.p, d->px.p, d->py.p,
+            d->pz.p, d->fn_sh.p, d->fn_cp.p, d->fn_atom.p, d->ax.p, d->ay.p, d->az.p, d->d_norm, part, d->tc_err.p);
       LIO_CUDA(cudaGetLastError());
       launches += 2;
     } else {
@@ -845,8 +847,10 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
     }
   }
   d->mark(1);
+  // the tensor-core density writes one partial per point, the FP64 one one per 64-function tile
   k_functional<<<nf, kFuncBlock, 0, st>>>(d->func_tiles.p, d->groups.p, d->pw.p, d->part_a.p,
-                                          d->open ? d->part_b.p : nullptr, d->lda ? 1 : 0, d->open ? 1 : 0,
+                                          d->open ? d->part_b.p : nullptr, tc ? (1 << 30) : kTile, d->lda ? 1 : 0,
+                                          d->open ? 1 : 0,
                                           d->iexch, d->fac_a.p, d->open ? d->fac_b.p : nullptr, d->eblocks.p);
   LIO_CUDA(cudaGetLastError());
   k_sum_blocks<<<1, 1024, 0, st>>>(d->eblocks.p, (int)nf, d->energy.p);
@@ -1003,7 +1007,7 @@ void DeviceEngine::solve_noalloc(const double* rho_a, const double* rho_b, doubl
       LIO_CUDA(cudaGetLastError());
     }
     k_functional<<<(unsigned)nf, kFuncBlock, 0, st>>>(d->func_tiles.p + ft0, d->groups.p, d->pw.p, pa,
-                                                       d->open ? pb : nullptr, d->lda ? 1 : 0, d->open ? 1 : 0,
+                                                       d->open ? pb : nullptr, kTile, d->lda ? 1 : 0, d->open ? 1 : 0,
                                                        d->iexch, fa, d->open ? fb : nullptr, eblk);
     LIO_CUDA(cudaGetLastError());
     k_sum_blocks<<<1, 1024, 0, st>>>(eblk, (int)nf, eparts + nbatch);
