@@ -22,7 +22,7 @@
 constexpr int kSlices = 6;       // Ozaki slices per operand
 constexpr int kTcPoints = 128;   // UMMA M: points per tile
 constexpr int kTcFuncs = 16;     // UMMA N: functions per tile; all kinds x levels stay in TMEM
-constexpr int kTcEpiWarps = 8;   // epilogue warps: kTcEpiWarps / 4 per TMEM lane quadrant
+constexpr int kTcEpiWarps = 16;  // epilogue warps: kTcEpiWarps / 4 per TMEM lane quadrant
 constexpr int kTcEpiCols = kTcFuncs / (kTcEpiWarps / 4);  // columns per epilogue warp
 constexpr int kTcSliceA = 32 * kTcPoints;  // bytes of one A slice per 32-byte K step
 constexpr int kTcSliceB = 32 * kTcFuncs;   // bytes of one B slice per K step
