@@ -65,7 +65,11 @@ struct GroupDev {
   long long sl_off;    // int8 slices of the density A operands (bytes)
   long long aexp_off;  // their per-point exponents (elements): NA x ldp
   long long ds_off;    // int8 slices of the density matrix (bytes, one spin)
-  long long dexp_off;  // their per-function exponents (elements): nft x 64
+  long long dexp_off;  // their per-function exponents (elements): nft32 x kTcFuncs
+  long long fa_off;    // int8 slices of F by function row for the Kohn-Sham contraction (bytes)
+  long long fae_off;   // their per-row exponents (elements): nI x 128
+  long long fb_off;    // int8 slices of f*F by row (bytes, one spin)
+  long long fbe_off;   // their per-row exponents (elements): nJ x 32
 };
 
 template <class T>
@@ -482,6 +486,7 @@ __global__ void k_radial(const int2* __restrict__ tiles, const GroupDev* __restr
 }
 
 #include "density_tc.cuh"
+#include "fock_tc.cuh"
 
 }  // namespace
 
@@ -505,6 +510,12 @@ struct DeviceEngine::Impl {
   DevBuf<int16_t> aexp, dexp_a, dexp_b;
   DevBuf<int> tc_err;
   long long tc_sizes[5] = {0, 0, 0, 0, 0};
+  // tensor-core Kohn-Sham contraction
+  DevBuf<int2> fa_rows, fb_rows;
+  DevBuf<int4> fk_tiles;
+  DevBuf<int8_t> fa_slices, fb_slices_a, fb_slices_b;
+  DevBuf<int16_t> fa_exp, fb_exp_a, fb_exp_b;
+  long long fk_sizes[4] = {0, 0, 0, 0};
   bool tc_ready = false;
   double d_norm = 1.0;
   DevBuf<double> ca, cc, ax, ay, az;
@@ -611,6 +622,9 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
   std::vector<int4> dtiles, ktiles, tctiles;
   long long pt_off = 0, fn_off = 0, sf_off = 0, bas_off = 0, part_off = 0;
   long long rad_off = 0, sl_off = 0, aexp_off = 0, ds_off = 0, dexp_off = 0;
+  long long fa_off = 0, fae_off = 0, fb_off = 0, fbe_off = 0;
+  std::vector<int2> farows, fbrows;
+  std::vector<int4> fktiles;
   long long npts_total = 0;
   const int NA = sys.lda ? 1 : 4;
   const int ngr = part.total_groups();
@@ -634,6 +648,16 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
     G.aexp_off = aexp_off;
     G.ds_off = ds_off;
     G.dexp_off = dexp_off;
+    G.fa_off = fa_off;
+    G.fae_off = fae_off;
+    G.fb_off = fb_off;
+    G.fbe_off = fbe_off;
+    const int nI = (G.m + kFkRows - 1) / kFkRows, nJ = (G.m + kFkCols - 1) / kFkCols;
+    for (int i = 0; i < nI * kFkRows; i++) farows.push_back({g, i});
+    for (int j = 0; j < nJ * kFkCols; j++) fbrows.push_back({g, j});
+    for (int I = 0; I < nI; I++)
+      for (int J = 0; J < nJ; J++)
+        if (J * kFkCols + kFkCols - 1 >= I * kFkRows) fktiles.push_back({g, I, J, 0});
     for (int p = 0; p < G.ldp; p++) {
       if (p < G.npts) {
         const GridPoint& q = pg.points[p];
@@ -684,6 +708,10 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
     aexp_off += (long long)NA * G.ldp;
     ds_off += (long long)G.nft32 * kSlices * kTcFuncs * G.m32;
     dexp_off += (long long)G.nft32 * kTcFuncs;
+    fa_off += (long long)nI * kSlices * kFkRows * G.ldp;
+    fae_off += (long long)nI * kFkRows;
+    fb_off += (long long)nJ * kSlices * kFkCols * G.ldp;
+    fbe_off += (long long)nJ * kFkCols;
     npts_total += G.npts;
     gd.push_back(G);
   }
@@ -693,6 +721,13 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
   d->tc_sizes[3] = ds_off;
   d->tc_sizes[4] = dexp_off;
   d->tc_ready = false;
+  d->fk_sizes[0] = fa_off;
+  d->fk_sizes[1] = fae_off;
+  d->fk_sizes[2] = fb_off;
+  d->fk_sizes[3] = fbe_off;
+  d->fa_rows.upload(farows);
+  d->fb_rows.upload(fbrows);
+  d->fk_tiles.upload(fktiles);
   d->hgroups = gd;
   d->ngroups = ngr;
   d->npoints = npts_total;
@@ -787,6 +822,22 @@ void DeviceEngine::prepare_tensor_core() {
     k_slice_basis<4><<<(unsigned)d->slice_basis_tiles.n, kTcPoints, 0, st>>>(d->slice_basis_tiles.p, d->groups.p,
                                                                             d->basis.p, d->aslices.p, d->aexp.p);
   LIO_CUDA(cudaGetLastError());
+  d->fa_slices.alloc(d->fk_sizes[0]);
+  d->fa_exp.alloc(d->fk_sizes[1]);
+  d->fb_slices_a.alloc(d->fk_sizes[2]);
+  d->fb_exp_a.alloc(d->fk_sizes[3]);
+  if (d->open) {
+    d->fb_slices_b.alloc(d->fk_sizes[2]);
+    d->fb_exp_b.alloc(d->fk_sizes[3]);
+  }
+  {
+    const int nrows = (int)d->fa_rows.n;
+    k_slice_fock<kFkRows><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(d->fa_rows.p, nrows, d->groups.p, d->basis.p,
+                                                                       nullptr, d->fa_slices.p, d->fa_exp.p, 0);
+    LIO_CUDA(cudaGetLastError());
+  }
+  LIO_CUDA(cudaFuncSetAttribute(k_fock_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FkCfg<1>::kSmem));
+  LIO_CUDA(cudaFuncSetAttribute(k_fock_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FkCfg<2>::kSmem));
   LIO_CUDA(cudaFuncSetAttribute(k_density_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TcCfg<1>::kSmem));
   LIO_CUDA(cudaFuncSetAttribute(k_density_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TcCfg<4>::kSmem));
   d->tc_ready = true;
@@ -860,12 +911,30 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
   if (req.compute_rmm) {
     LIO_CUDA(cudaMemsetAsync(d->K_a.p, 0, npacked * sizeof(double), st));
     if (d->open) LIO_CUDA(cudaMemsetAsync(d->K_b.p, 0, npacked * sizeof(double), st));
-    if (d->open)
+    if (tc) {
+      const int nrows = (int)d->fb_rows.n;
+      for (int s = 0; s < (d->open ? 2 : 1); s++) {
+        k_slice_fock<kFkCols><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(
+            d->fb_rows.p, nrows, d->groups.p, d->basis.p, s == 0 ? d->fac_a.p : d->fac_b.p,
+            s == 0 ? d->fb_slices_a.p : d->fb_slices_b.p, s == 0 ? d->fb_exp_a.p : d->fb_exp_b.p, 1);
+        LIO_CUDA(cudaGetLastError());
+        launches++;
+      }
+      if (d->open)
+        k_fock_tc<2><<<(unsigned)d->fk_tiles.n, FkCfg<2>::kThreads, FkCfg<2>::kSmem, st>>>(
+            d->fk_tiles.p, d->groups.p, d->fn_glob.p, d->fa_slices.p, d->fa_exp.p, d->fb_slices_a.p, d->fb_exp_a.p,
+            d->fb_slices_b.p, d->fb_exp_b.p, d->M, d->K_a.p, d->K_b.p, d->tc_err.p);
+      else
+        k_fock_tc<1><<<(unsigned)d->fk_tiles.n, FkCfg<1>::kThreads, FkCfg<1>::kSmem, st>>>(
+            d->fk_tiles.p, d->groups.p, d->fn_glob.p, d->fa_slices.p, d->fa_exp.p, d->fb_slices_a.p, d->fb_exp_a.p,
+            nullptr, nullptr, d->M, d->K_a.p, nullptr, d->tc_err.p);
+    } else if (d->open) {
       k_fock_fp64<2><<<nk, 256, 0, st>>>(d->fock_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, d->fac_a.p,
                                          d->fac_b.p, d->M, d->K_a.p, d->K_b.p);
-    else
+    } else {
       k_fock_fp64<1><<<nk, 256, 0, st>>>(d->fock_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, d->fac_a.p,
                                          nullptr, d->M, d->K_a.p, nullptr);
+    }
     LIO_CUDA(cudaGetLastError());
     launches++;
   }
