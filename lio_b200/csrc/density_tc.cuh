@@ -1,5 +1,5 @@
 // Tensor-core form of the density contraction (included by engine.cu inside its
-// anonymous namespace; uses GroupDev, c_comp_l and the monomial helpers).
+// anonymous namespace; uses GroupDev and packed_index).
 //
 // G^a = A^a . D for the basis kinds a = F (LDA) or F, dF/dx, dF/dy, dF/dz (GGA),
 // with D the group's dense density, computed with int8 tensor-core products
@@ -8,33 +8,61 @@
 //   D_ji   = 2^(f_i) * sum_t d_t[i][j] 128^-(t+1),   |d_t| <= 64  (per function i)
 // and G_pi = 2^(e_p + f_i - 7(S+1)) * sum_l acc_l[p][i] 128^(S-1-l), where the
 // level accumulator acc_l holds every slice pair s + t = l (pairs with
-// s + t >= S are dropped). The level sum is formed exactly in int64 and
-// converted to FP64 once. With S = 6 the dropped terms are ~2^-42 of
+// s + t >= S are dropped). With S = 6 the dropped terms are ~2^-42 of
 // max_j|A_pj| * max_j|D_ji| per term, far inside the 1e-7 / 1e-6 Ha tolerances.
 //
-// The row-dot epilogue needs F, dF and d2F at (p, i) in FP64; instead of
-// re-reading ten cached values per (p, i) it rebuilds them from a per-shell
-// radial cache (t, tg, th) and the point/atom coordinates (no exp), so the
-// kernel's HBM traffic is dominated by the int8 slices.
+// Slice pairs in few, wide MMAs: the S slices of a 32-function D tile are
+// stacked along N ("tall" B operand, row t * 32 + i holds d_t[i]). For A slice s
+// one MMA with N = (S - s) * 32 multiplies a_s by d_0 .. d_(S-1-s) (a prefix of
+// the tall operand) into TMEM columns starting at level s, so product (s, t)
+// lands on level s + t: S MMAs per K step and kind instead of S(S+1)/2 narrow
+// ones (an MMA costs about the same for every N up to 64 on this part).
+//
+// The row-dot epilogue reads F, dF and d2F at (p, i) from the FP64 basis cache.
 #pragma once
 #include "umma.cuh"
 
 constexpr int kSlices = 6;       // Ozaki slices per operand
 constexpr int kTcPoints = 128;   // UMMA M: points per tile
-constexpr int kTcFuncs = 16;     // UMMA N: functions per tile; all kinds x levels stay in TMEM
-constexpr int kTcEpiWarps = 16;  // epilogue warps: kTcEpiWarps / 4 per TMEM lane quadrant
-constexpr int kTcEpiCols = kTcFuncs / (kTcEpiWarps / 4);  // columns per epilogue warp
-constexpr int kTcSliceA = 32 * kTcPoints;  // bytes of one A slice per 32-byte K step
-constexpr int kTcSliceB = 32 * kTcFuncs;   // bytes of one B slice per K step
-template <int NA>
+constexpr int kTcFuncs = 32;     // functions per density tile (output columns per level)
+constexpr int kTcTall = kSlices * kTcFuncs;  // rows of the stacked D operand
+constexpr int kTcEpiWarps = 8;   // two per TMEM lane quadrant
+constexpr int kTcCpw = kTcFuncs / 2;         // columns per epilogue warp
+constexpr int kTcSliceA = 32 * kTcPoints;    // bytes of one A slice per 32-byte K step
+constexpr int kTcStepA = kSlices * kTcSliceA;  // one kind's A slices per K step (contiguous)
+constexpr int kTcStepD = 32 * kTcTall;         // one spin's stacked D slices per K step (contiguous)
+constexpr int kTcMaxFnCap = 512; // functions per group the ring depth leaves table room for
+
+// KP = kinds per unit: all NS x KP x S x 32 level columns of a unit fit in 384
+// TMEM columns. Open shell: one kind per unit (F, x, y, z); closed shell GGA:
+// {F, dF/dx} then {dF/dy, dF/dz}; LDA: {F}.
+template <bool GGA, int NS>
 struct TcCfg {
-  static constexpr int kStageA = NA * kSlices * kTcSliceA;
-  static constexpr int kStage = kStageA + kSlices * kTcSliceB;
-  static constexpr size_t kSmem = 2 * (size_t)kStage;  // double-buffered K steps
-  static constexpr uint32_t kCols = NA * kSlices * kTcFuncs;
-  static constexpr uint32_t kTmem = kCols <= 128 ? 128 : (kCols <= 256 ? 256 : 512);
+  static constexpr int KP = (GGA && NS == 1) ? 2 : 1;
+  static constexpr int NA = GGA ? 4 : 1;  // kinds
+  static constexpr int NP = NA / KP;      // units per function tile
+  static constexpr int NQ = GGA ? 10 : 1;
+  static constexpr int kStageA = KP * kTcStepA;
+  static constexpr int kStage = kStageA + NS * kTcStepD;
+  static constexpr uint32_t kCols = NS * KP * kSlices * kTcFuncs;
+  static constexpr uint32_t kTmem = kCols <= 256 ? 256 : 512;
   static constexpr int kWarps = kTcEpiWarps + 2;  // epilogue warps, producer, MMA issuer
   static constexpr int kThreads = 32 * kWarps;
+  // dynamic shared memory: ring | staged G values | column-group reduction | function table
+  static constexpr size_t kGvWarp = (size_t)NS * KP * kTcCpw * 32 * 8;  // [spin][kind][column][lane] FP64
+  static constexpr size_t kGvBytes = kTcEpiWarps * kGvWarp;
+  static constexpr size_t kRedBytes = (size_t)NS * kTcPoints * NQ * 8;  // [spin][point][NQ] FP64
+  static constexpr size_t kTabEntry = NS * 8;                           // 2^f_i per spin
+  // ring depth: as many stages (up to 4) as fit beside the rest and a full table
+  static constexpr size_t kBudget = 232448 - 1024 - (size_t)kTcMaxFnCap * kTabEntry;
+  static constexpr int kStages =
+      (int)((kBudget - kGvBytes - kRedBytes) / kStage < 4 ? (kBudget - kGvBytes - kRedBytes) / kStage : 4);
+  static_assert(kStages >= 2, "ring too shallow");
+  static constexpr size_t kRing = (size_t)kStages * kStage;
+  static constexpr size_t kGv = kRing;
+  static constexpr size_t kRed = kGv + kGvBytes;
+  static constexpr size_t kTab = kRed + kRedBytes;
+  static size_t smem(int cap) { return kTab + (size_t)cap * kTabEntry; }
 };
 
 // exponent so that |x| * 2^-e <= 1/2 for every |x| <= amax
@@ -47,8 +75,10 @@ __device__ __forceinline__ double pow2(int k) {
 
 // ---------------------------------------------------------------- A slices
 // Per geometry: one thread per (group, point) and kind; reads the FP64 basis
-// cache, writes the int8 slices in the K-major interleaved UMMA layout of each
-// 128-point tile, and the per-point exponents.
+// cache, writes the per-point exponent and the int8 slices. Layout per
+// 128-point tile T, kind a and 32-function K step kk: the S slices one after
+// the other (kTcStepA bytes, one bulk copy), each in the K-major interleaved
+// UMMA layout of a 128-row x 32-byte block.
 template <int NA>
 __global__ void k_slice_basis(const int2* __restrict__ tiles, const GroupDev* __restrict__ groups,
                               const double* __restrict__ basis, int8_t* __restrict__ aslices,
@@ -58,36 +88,39 @@ __global__ void k_slice_basis(const int2* __restrict__ tiles, const GroupDev* __
   const int r = threadIdx.x;
   const int p = t.y * kTcPoints + r;
   const long long kstride = (long long)G.m * G.ldp;
+  const int nks = G.m32 / 32;
   for (int a = 0; a < NA; a++) {
     const double* src = basis + G.bas_off + a * kstride + p;
     double amax = 0.0;
     for (int j = 0; j < G.m; j++) amax = fmax(amax, fabs(src[(long long)j * G.ldp]));
     const int e = slice_exponent(amax);
     aexp[G.aexp_off + (long long)a * G.ldp + p] = (int16_t)e;
-    int8_t* dst = aslices + G.sl_off + ((long long)(t.y * NA + a) * kSlices) * kTcPoints * G.m32;
+    int8_t* dst = aslices + G.sl_off + (long long)(t.y * NA + a) * nks * kTcStepA;
     for (int j = 0; j < G.m32; j++) {
       double x = j < G.m ? ldexp(src[(long long)j * G.ldp], -e) : 0.0;
-      const uint32_t off = lio::umma::kmajor_offset(r, j, kTcPoints);
+      int8_t* blk = dst + (j >> 5) * kTcStepA + lio::umma::kmajor_offset(r, j & 31, kTcPoints);
       for (int s = 0; s < kSlices; s++) {
         x *= 128.0;
         const double d = rint(x);
         x -= d;
-        dst[(long long)s * kTcPoints * G.m32 + off] = (int8_t)d;
+        blk[s * kTcSliceA] = (int8_t)d;
       }
     }
   }
 }
 
 // --------------------------------------------------------------- D slices
-// Per solve and spin: one thread per (group, function i) of a kTcFuncs-function tile;
+// Per solve and spin: one thread per (group, function i) of a 32-function tile;
 // gathers column i of the group's density from the packed matrix (off-diagonal
-// packed values halved), writes its slices and exponent.
+// packed values halved), writes its exponent and its S slices into the stacked
+// operand: per tile and 32-function K step kk a 192-row x 32-byte block
+// (kTcStepD bytes, one bulk copy) whose row t * 32 + i holds d_t[i].
 __global__ void k_slice_density(const int2* __restrict__ tiles, const GroupDev* __restrict__ groups,
                                 const int* __restrict__ fn_glob, const double* __restrict__ P, int M,
                                 int8_t* __restrict__ dslices, int16_t* __restrict__ dexp) {
   const int2 t = tiles[blockIdx.x];
   const GroupDev G = groups[t.x];
-  const int r = threadIdx.x;  // row of the B tile
+  const int r = threadIdx.x;  // function within the tile
   const int i = t.y * kTcFuncs + r;
   const int* fg = fn_glob + G.fn_off;
   double amax = 0.0;
@@ -101,7 +134,8 @@ __global__ void k_slice_density(const int2* __restrict__ tiles, const GroupDev* 
     }
   const int e = slice_exponent(amax);
   dexp[G.dexp_off + i] = (int16_t)e;
-  int8_t* dst = dslices + G.ds_off + ((long long)t.y * kSlices) * kTcFuncs * G.m32;
+  const int nks = G.m32 / 32;
+  int8_t* dst = dslices + G.ds_off + (long long)t.y * nks * kTcStepD;
   for (int j = 0; j < G.m32; j++) {
     double x = 0.0;
     if (i < G.m && j < G.m) {
@@ -110,292 +144,385 @@ __global__ void k_slice_density(const int2* __restrict__ tiles, const GroupDev* 
       if (gi != gj) v *= 0.5;
       x = ldexp(v, -e);
     }
-    const uint32_t off = lio::umma::kmajor_offset(r, j, kTcFuncs);
+    int8_t* blk = dst + (j >> 5) * kTcStepD;
     for (int s = 0; s < kSlices; s++) {
       x *= 128.0;
       const double d = rint(x);
       x -= d;
-      dst[(long long)s * kTcFuncs * G.m32 + off] = (int8_t)d;
+      blk[lio::umma::kmajor_offset(s * kTcFuncs + r, j & 31, kTcTall)] = (int8_t)d;
     }
   }
 }
 
 // ------------------------------------------------------- the fused kernel
-// basis value and derivatives of one Cartesian component x^LX y^LY z^LZ at
-// displacement r from the radial triplet (t, tg, th); the closed forms of
-// k_basis with every exponent a compile-time constant:
-//   F = P t,  dF/da = P_a t - 2 r_a P tg,
-//   d2F/da db = P_ab t - 2 (r_b P_a + r_a P_b + delta_ab P) tg + 4 r_a r_b P th
-template <int L>
-__device__ __forceinline__ double cpow(double x) { return L == 0 ? 1.0 : (L == 1 ? x : x * x); }
-template <int L>
-__device__ __forceinline__ double cdpow(double x) { return L == 0 ? 0.0 : (L == 1 ? 1.0 : 2.0 * x); }
-template <int L>
-__device__ __forceinline__ double cd2pow() { return L == 2 ? 2.0 : 0.0; }
+// K (padded functions) up to which two adjacent levels combine exactly in
+// int32: |acc_l| <= (l + 1) * 64 * 64 * K, so |128 acc_4 + acc_5| < 2^31 for K < 813
+constexpr int kTcNarrowK = 768;
 
-template <int LX, int LY, int LZ, bool HESS>
-__device__ __forceinline__ void rebuild_c(const double r[3], double t, double tg, double th, double sc, double& F,
-                                          double g[3], double h[6]) {
-  const double px = cpow<LX>(r[0]), py = cpow<LY>(r[1]), pz = cpow<LZ>(r[2]);
-  const double dx = cdpow<LX>(r[0]), dy = cdpow<LY>(r[1]), dz = cdpow<LZ>(r[2]);
-  const double P = px * py * pz;
-  const double Pa[3] = {dx * py * pz, px * dy * pz, px * py * dz};
-  const double st = sc * t, sv = sc * (-2.0 * tg), sw = sc * (4.0 * th);
-  F = P * st;
-  g[0] = Pa[0] * st + r[0] * P * sv;
-  g[1] = Pa[1] * st + r[1] * P * sv;
-  g[2] = Pa[2] * st + r[2] * P * sv;
-  if (!HESS) return;
-  const double Pxx = cd2pow<LX>() * py * pz, Pyy = px * cd2pow<LY>() * pz, Pzz = px * py * cd2pow<LZ>();
-  const double Pxy = dx * dy * pz, Pxz = dx * py * dz, Pyz = px * dy * dz;
-  const double wP = sw * P;
-  h[0] = Pxx * st + (2.0 * r[0] * Pa[0] + P) * sv + r[0] * r[0] * wP;
-  h[1] = Pyy * st + (2.0 * r[1] * Pa[1] + P) * sv + r[1] * r[1] * wP;
-  h[2] = Pzz * st + (2.0 * r[2] * Pa[2] + P) * sv + r[2] * r[2] * wP;
-  h[3] = Pxy * st + (r[1] * Pa[0] + r[0] * Pa[1]) * sv + r[0] * r[1] * wP;
-  h[4] = Pxz * st + (r[2] * Pa[0] + r[0] * Pa[2]) * sv + r[0] * r[2] * wP;
-  h[5] = Pyz * st + (r[2] * Pa[1] + r[1] * Pa[2]) * sv + r[1] * r[2] * wP;
-}
-
-// dispatch on the component code (0: s; 1-3: p x,y,z; 4-9: d xx,xy,yy,xz,yz,zz),
-// which is the same for every lane of a warp
-template <bool HESS>
-__device__ __forceinline__ void rebuild_cp(int cp, const double r[3], double t, double tg, double th, double sc,
-                                           double& F, double g[3], double h[6]) {
-  switch (cp) {
-    case 0: rebuild_c<0, 0, 0, HESS>(r, t, tg, th, sc, F, g, h); break;
-    case 1: rebuild_c<1, 0, 0, HESS>(r, t, tg, th, sc, F, g, h); break;
-    case 2: rebuild_c<0, 1, 0, HESS>(r, t, tg, th, sc, F, g, h); break;
-    case 3: rebuild_c<0, 0, 1, HESS>(r, t, tg, th, sc, F, g, h); break;
-    case 4: rebuild_c<2, 0, 0, HESS>(r, t, tg, th, sc, F, g, h); break;
-    case 5: rebuild_c<1, 1, 0, HESS>(r, t, tg, th, sc, F, g, h); break;
-    case 6: rebuild_c<0, 2, 0, HESS>(r, t, tg, th, sc, F, g, h); break;
-    case 7: rebuild_c<1, 0, 1, HESS>(r, t, tg, th, sc, F, g, h); break;
-    case 8: rebuild_c<0, 1, 1, HESS>(r, t, tg, th, sc, F, g, h); break;
-    default: rebuild_c<0, 0, 2, HESS>(r, t, tg, th, sc, F, g, h); break;
-  }
-}
-
-template <int N>
-__device__ __forceinline__ void tmem_ld_cols(uint32_t taddr, int32_t (&v)[N]) {
-  if constexpr (N == 8) {
-    lio::umma::tmem_ld8(taddr, v);
+// sum_l acc_l 128^(S-1-l) of column c in FP64: level pairs in int32 (narrow)
+// or each level converted (wide), then combined with one rounding, 2^-53 of
+// the leading term and far below the dropped slice pairs
+__device__ __forceinline__ double level_sum(const int32_t (&lv)[kSlices][8], int c, bool narrow) {
+  double v0, v1, v2;
+  if (narrow) {
+    v0 = (double)(lv[0][c] * 128 + lv[1][c]);
+    v1 = (double)(lv[2][c] * 128 + lv[3][c]);
+    v2 = (double)(lv[4][c] * 128 + lv[5][c]);
   } else {
-    lio::umma::tmem_ld4(taddr, *reinterpret_cast<int32_t(*)[4]>(v));
+    v0 = fma((double)lv[0][c], 128.0, (double)lv[1][c]);
+    v1 = fma((double)lv[2][c], 128.0, (double)lv[3][c]);
+    v2 = fma((double)lv[4][c], 128.0, (double)lv[5][c]);
+  }
+  return fma(fma(v0, 16384.0, v1), 16384.0, v2);
+}
+// named barrier over the epilogue warps only; returns the OR of `pred` over them
+__device__ __forceinline__ bool epi_sync_or(bool pred) {
+  uint32_t out;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, %2, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(out)
+      : "r"((uint32_t)pred), "n"(kTcEpiWarps * 32)
+      : "memory");
+  return out != 0;
+}
+
+// Row dots of one unit for one epilogue warp: its 16 columns i = cb .. cb+15
+// (G values staged in gv[(sp * KP + kp) * 16 + c][lane], scales 2^f_i in
+// ts[sp][i], zero beyond m) against the FP64 basis values of the point at
+// bas[k * ks + i * ldp], accumulated into q = (rho; grad rho; d2rho xx, yy, zz,
+// xy, xz, yz) per spin:
+//   kind F : rho += F G, grad += 2 dF G, d2 += 2 d2F G
+//   kind x : xx += 2 Fx Gx, xy += 2 Fy Gx, xz += 2 Fz Gx   (Fy Gx = Fx Gy: D is symmetric)
+//   kind y : yy += 2 Fy Gy, yz += 2 Fz Gy
+//   kind z : zz += 2 Fz Gz
+// All loads of a column chunk are issued before any is used, so a warp keeps
+// 16 to 48 loads in flight. Columns at or beyond m read column m-1 (their G
+// and scale are zero).
+template <bool GGA, int NS, int NQ, int KP>
+__device__ __forceinline__ void unit_row_dots(int first, const double* bas, long long ks, int ldp, int cb, int m,
+                                              const double* gv, const double* tsa, const double* tsb, int lane,
+                                              double (&q)[NS][NQ]) {
+  constexpr int C = kTcCpw;
+  auto col = [&](int c) { return (long long)(cb + c < m ? cb + c : m - 1) * ldp; };
+  auto gval = [&](int sp, int kp, int c) {
+    return gv[((sp * KP + kp) * C + c) * 32 + lane] * (sp == 0 ? tsa[cb + c] : tsb[cb + c]);
+  };
+  if (!GGA) {
+    double F[C];
+#pragma unroll
+    for (int c = 0; c < C; c++) F[c] = bas[col(c)];
+#pragma unroll
+    for (int c = 0; c < C; c++)
+#pragma unroll
+      for (int sp = 0; sp < NS; sp++) q[sp][0] += F[c] * gval(sp, 0, c);
+    return;
+  }
+  if (first == 0) {  // F (and x when KP == 2), four columns at a time
+#pragma unroll
+    for (int c0 = 0; c0 < C; c0 += 4) {
+      double v[4][10];
+#pragma unroll
+      for (int c = 0; c < 4; c++)
+#pragma unroll
+        for (int k = 0; k < 10; k++) v[c][k] = bas[k * ks + col(c0 + c)];
+#pragma unroll
+      for (int c = 0; c < 4; c++)
+#pragma unroll
+        for (int sp = 0; sp < NS; sp++) {
+          const double g0 = gval(sp, 0, c0 + c), g2 = 2.0 * g0;
+          q[sp][0] += v[c][0] * g0;
+#pragma unroll
+          for (int k = 1; k < 10; k++) q[sp][k % NQ] += v[c][k] * g2;
+          if (KP == 2) {
+            const double gx2 = 2.0 * gval(sp, 1, c0 + c);
+            q[sp][4 % NQ] += v[c][1] * gx2;
+            q[sp][7 % NQ] += v[c][2] * gx2;
+            q[sp][8 % NQ] += v[c][3] * gx2;
+          }
+        }
+    }
+  } else if (first == 1) {  // x alone (KP == 1)
+    double v[C][3];
+#pragma unroll
+    for (int c = 0; c < C; c++)
+#pragma unroll
+      for (int k = 0; k < 3; k++) v[c][k] = bas[(1 + k) * ks + col(c)];
+#pragma unroll
+    for (int c = 0; c < C; c++)
+#pragma unroll
+      for (int sp = 0; sp < NS; sp++) {
+        const double g2 = 2.0 * gval(sp, 0, c);
+        q[sp][4 % NQ] += v[c][0] * g2;
+        q[sp][7 % NQ] += v[c][1] * g2;
+        q[sp][8 % NQ] += v[c][2] * g2;
+      }
+  } else if (first == 2) {  // y (and z when KP == 2)
+    double v[C][2];
+#pragma unroll
+    for (int c = 0; c < C; c++)
+#pragma unroll
+      for (int k = 0; k < 2; k++) v[c][k] = bas[(2 + k) * ks + col(c)];
+#pragma unroll
+    for (int c = 0; c < C; c++)
+#pragma unroll
+      for (int sp = 0; sp < NS; sp++) {
+        const double g2 = 2.0 * gval(sp, 0, c);
+        q[sp][5 % NQ] += v[c][0] * g2;
+        q[sp][9 % NQ] += v[c][1] * g2;
+        if (KP == 2) q[sp][6 % NQ] += v[c][1] * (2.0 * gval(sp, 1, c));
+      }
+  } else {  // z alone (KP == 1)
+    double v[C];
+#pragma unroll
+    for (int c = 0; c < C; c++) v[c] = bas[3 * ks + col(c)];
+#pragma unroll
+    for (int c = 0; c < C; c++)
+#pragma unroll
+      for (int sp = 0; sp < NS; sp++) q[sp][6 % NQ] += v[c] * (2.0 * gval(sp, 0, c));
   }
 }
 
-// CTA = (group, 128-point tile), warp-specialised:
-//   warps 0..kTcEpiWarps-1  epilogue: TMEM lane quadrant warp % 4 (one lane =
-//                one point), columns kTcEpiCols * (warp / 4) .. of each tile;
-//   next warp    producer: 1-D bulk copies of the A slices (all kinds) and the
-//                D slices of each 32-byte K step into one of two stages;
-//   last warp    MMA issuer: every kind's slice pairs into the NA x S level
-//                accumulators, which stay resident in TMEM for a whole
-//                16-function tile.
-// mbarriers: full[s] (bytes landed), empty[s] (the stage's MMAs are done),
-// tfull (a tile's accumulators are complete), tempty (the epilogue has read
-// them). The epilogue hands TMEM back right after combining the levels, so the
-// next tile's MMAs overlap its FP64 row-dot work. The four column groups of a
-// point are summed through shared memory at the end and written once (one
-// partial per point). Every wait is bounded.
-template <int NA>
-__global__ void __launch_bounds__(TcCfg<NA>::kThreads, 1)
-    k_density_tc(const int2* __restrict__ tiles, const GroupDev* __restrict__ groups,
+// CTA = one per SM, persistent over the 128-point tiles (all groups, largest
+// function count first, tile w handled by CTA w mod gridDim.x); both spins
+// (NS = 2) or one. A unit is (tile, 32-function tile, KP kinds). Warp roles:
+//   warps 0..7  epilogue: TMEM lane quadrant warp % 4 (one lane = one point),
+//               columns 16 * (warp / 4) .. of the function tile;
+//   warp 8      producer: per (unit, 32-function K step) one stage with the
+//               unit's A slices (KP x kTcStepA) and every spin's stacked D
+//               slices (kTcStepD), one bulk copy each, into a four-stage ring;
+//   warp 9      MMA issuer: per stage NS x KP x S MMAs into the unit's
+//               NS x KP x S x 32 level columns in TMEM.
+// The A slices are shared by both spins. The epilogue stages the unit's G
+// values (FP64) in shared memory and hands TMEM back (tempty) before its
+// row-dot work, so the next unit's MMAs overlap it. The ring, unit and tile
+// sequences run on across tiles, so one tile's loads and MMAs overlap the
+// previous tile's epilogue. Every wait is bounded; a timeout sets `fail`,
+// which the other roles poll, and the kernel drains its copies and MMAs
+// before it frees TMEM and reports the error.
+template <bool GGA, int NS>
+__global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
+    k_density_tc(const int2* __restrict__ tiles, int ntiles, const GroupDev* __restrict__ groups,
                  const int8_t* __restrict__ aslices, const int16_t* __restrict__ aexp,
-                 const int8_t* __restrict__ dslices, const int16_t* __restrict__ dexp,
-                 const double* __restrict__ radial, const double* __restrict__ px, const double* __restrict__ py,
-                 const double* __restrict__ pz, const int* __restrict__ fn_sh, const int8_t* __restrict__ fn_cp,
-                 const int* __restrict__ fn_atom, const double* __restrict__ ax, const double* __restrict__ ay,
-                 const double* __restrict__ az, double dnorm, double* __restrict__ partial, int* __restrict__ err) {
-  using Cfg = TcCfg<NA>;
-  constexpr int NQ = NA == 1 ? 1 : kNQ;
-  constexpr int kGroups = kTcEpiWarps / 4;  // column groups per lane quadrant
-  extern __shared__ __align__(1024) uint8_t tc_smem[];
-  __shared__ uint64_t full[2], empty[2], tfull, tempty;
+                 const int8_t* __restrict__ dsl_a, const int16_t* __restrict__ dexp_a,
+                 const int8_t* __restrict__ dsl_b, const int16_t* __restrict__ dexp_b,
+                 const double* __restrict__ basis, int fcap, double* __restrict__ part_a,
+                 double* __restrict__ part_b, int* __restrict__ err) {
+  using Cfg = TcCfg<GGA, NS>;
+  constexpr int KP = Cfg::KP, NP = Cfg::NP, NA = Cfg::NA, NQ = Cfg::NQ, CPW = kTcCpw;
+  constexpr int kStages = Cfg::kStages;
+  extern __shared__ __align__(128) uint8_t tc_smem[];
+  __shared__ uint64_t full[kStages], empty[kStages], tfull, tempty, drain;
   __shared__ uint32_t tmem_base;
-  __shared__ int fail;
-  const int2 t = tiles[blockIdx.x];
-  const GroupDev G = groups[t.x];
-  const int T = t.y;
+  __shared__ int fail, consumed;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int nks = G.m32 / 32;
-  const int nft = (G.m + kTcFuncs - 1) / kTcFuncs;
-  const int total = nft * nks;
   if (warp == 0) lio::umma::tmem_alloc(&tmem_base, Cfg::kTmem);
   if (tid == 0) {
-    lio::umma::mbar_init(&full[0], 1);
-    lio::umma::mbar_init(&full[1], 1);
-    lio::umma::mbar_init(&empty[0], 1);
-    lio::umma::mbar_init(&empty[1], 1);
+    for (int b = 0; b < kStages; b++) {
+      lio::umma::mbar_init(&full[b], 1);
+      lio::umma::mbar_init(&empty[b], 1);
+    }
     lio::umma::mbar_init(&tfull, 1);
     lio::umma::mbar_init(&tempty, kTcEpiWarps);
+    lio::umma::mbar_init(&drain, 1);
     lio::umma::fence_mbar_init();
     fail = 0;
+    consumed = 0;
   }
   lio::umma::fence_before_sync();
   __syncthreads();
   lio::umma::fence_after_sync();
   const uint32_t tbase = tmem_base;
-  double q[NQ];
-#pragma unroll
-  for (int k = 0; k < NQ; k++) q[k] = 0.0;
-  const int quad = warp & 3, colg = warp >> 2;
-  const int row = quad * 32 + lane;
-  const int p = T * kTcPoints + row;
+  volatile int* vfail = &fail;
+  int issued = 0;  // producer: stages issued
 
   if (warp == kTcEpiWarps) {
     // ------------------------------------------------------------ producer
     if (lane == 0) {
-      const int8_t* Abase = aslices + G.sl_off + (long long)T * NA * kSlices * kTcPoints * G.m32;
-      const int8_t* Bbase = dslices + G.ds_off;
-      for (int st = 0; st < total; st++) {
-        const int buf = st & 1, use = st >> 1;
-        if (use > 0 && !lio::umma::mbar_wait(&empty[buf], (use - 1) & 1)) {
-          fail = 1;
-          break;
+      int cnt = 0;
+      for (int w = blockIdx.x; w < ntiles && !*vfail; w += gridDim.x) {
+        const int2 t = tiles[w];
+        const GroupDev& G = groups[t.x];
+        const int nks = G.m32 / 32, nft = (G.m + kTcFuncs - 1) / kTcFuncs;
+        const int8_t* Abase = aslices + G.sl_off + (long long)t.y * NA * nks * kTcStepA;
+        for (int tt = 0; tt < nft * NP && !*vfail; tt++) {
+          const int ft = tt / NP, pass = tt - ft * NP;
+          for (int kk = 0; kk < nks; kk++, cnt++) {
+            const int buf = cnt % kStages, use = cnt / kStages;
+            if (use > 0 && (*vfail || !lio::umma::mbar_wait(&empty[buf], (use - 1) & 1))) {
+              *vfail = 1;
+              break;
+            }
+            uint8_t* stage = tc_smem + buf * Cfg::kStage;
+            lio::umma::mbar_expect_tx(&full[buf], (uint32_t)Cfg::kStage);
+            for (int kp = 0; kp < KP; kp++)
+              lio::umma::bulk_copy_g2s(stage + kp * kTcStepA,
+                                       Abase + ((long long)(pass * KP + kp) * nks + kk) * kTcStepA, kTcStepA,
+                                       &full[buf]);
+            for (int sp = 0; sp < NS; sp++)
+              lio::umma::bulk_copy_g2s(stage + Cfg::kStageA + sp * kTcStepD,
+                                       (sp == 0 ? dsl_a : dsl_b) + G.ds_off + ((long long)ft * nks + kk) * kTcStepD,
+                                       kTcStepD, &full[buf]);
+            issued = cnt + 1;
+          }
         }
-        const int ft = st / nks, kk = st - ft * nks;
-        uint8_t* stage = tc_smem + buf * Cfg::kStage;
-        lio::umma::mbar_expect_tx(&full[buf], (uint32_t)Cfg::kStage);
-        for (int piece = 0; piece < NA * kSlices; piece++)
-          lio::umma::bulk_copy_g2s(stage + piece * kTcSliceA,
-                                   Abase + (long long)piece * kTcPoints * G.m32 + kk * kTcSliceA, kTcSliceA,
-                                   &full[buf]);
-        for (int s = 0; s < kSlices; s++)
-          lio::umma::bulk_copy_g2s(stage + Cfg::kStageA + s * kTcSliceB,
-                                   Bbase + ((long long)ft * kSlices + s) * kTcFuncs * G.m32 + kk * kTcSliceB,
-                                   kTcSliceB, &full[buf]);
       }
     }
   } else if (warp == kTcEpiWarps + 1) {
-    // ------------------------------------------- MMA issuer (all kinds)
+    // ------------------------------------------------------------ MMA issuer
     if (lane == 0) {
-      const uint32_t idesc = lio::umma::idesc_i8(kTcPoints, kTcFuncs);
       const uint32_t smem0 = lio::umma::smem_u32(tc_smem);
-      for (int st = 0; st < total; st++) {
-        const int buf = st & 1, use = st >> 1;
-        const int ft = st / nks, kk = st - ft * nks;
-        if (kk == 0 && ft > 0) {
-          if (!lio::umma::mbar_wait(&tempty, (ft - 1) & 1)) {
-            fail = 1;
-            break;
+      int cnt = 0, ucnt = 0;
+      bool stop = false;
+      for (int w = blockIdx.x; w < ntiles && !stop; w += gridDim.x) {
+        const int2 t = tiles[w];
+        const GroupDev& G = groups[t.x];
+        const int nks = G.m32 / 32, nft = (G.m + kTcFuncs - 1) / kTcFuncs;
+        for (int tt = 0; tt < nft * NP && !stop; tt++, ucnt++) {
+          if (ucnt > 0) {
+            if (*vfail || !lio::umma::mbar_wait(&tempty, (ucnt - 1) & 1)) {
+              stop = true;
+              break;
+            }
+            lio::umma::fence_after_sync();
           }
-          lio::umma::fence_after_sync();
+          for (int kk = 0; kk < nks; kk++, cnt++) {
+            const int buf = cnt % kStages, use = cnt / kStages;
+            if (*vfail || !lio::umma::mbar_wait(&full[buf], use & 1)) {
+              stop = true;
+              break;
+            }
+            consumed = cnt + 1;
+            lio::umma::fence_after_sync();
+            const uint32_t sa = smem0 + buf * Cfg::kStage;
+#pragma unroll
+            for (int sp = 0; sp < NS; sp++) {
+              // stacked D of this spin: K-major, 192 rows (LBO = 16 * 192 bytes between K halves)
+              const uint64_t bd = lio::umma::smem_desc(sa + Cfg::kStageA + sp * kTcStepD, 16u * kTcTall, 128u);
+#pragma unroll
+              for (int kp = 0; kp < KP; kp++)
+#pragma unroll
+                for (int s = 0; s < kSlices; s++)
+                  lio::umma::mma_i8(
+                      tbase + (uint32_t)(((sp * KP + kp) * kSlices + s) * kTcFuncs),
+                      lio::umma::smem_desc(sa + kp * kTcStepA + s * kTcSliceA, 16u * kTcPoints, 128u), bd,
+                      lio::umma::idesc_i8(kTcPoints, (kSlices - s) * kTcFuncs), (kk > 0 || s > 0) ? 1u : 0u);
+            }
+            lio::umma::commit(&empty[buf]);
+            if (kk == nks - 1) lio::umma::commit(&tfull);
+          }
         }
-        if (!lio::umma::mbar_wait(&full[buf], use & 1)) {
-          fail = 1;
-          break;
-        }
-        lio::umma::fence_after_sync();
-        // the descriptor start-address field advances by (byte offset >> 4)
-        const uint64_t ad0 = lio::umma::smem_desc(smem0 + buf * Cfg::kStage, 16u * kTcPoints, 128u);
-        const uint64_t bd0 = lio::umma::smem_desc(smem0 + buf * Cfg::kStage + Cfg::kStageA, 16u * kTcFuncs, 128u);
-        const uint32_t keep = kk > 0 ? 1u : 0u;
-#pragma unroll
-        for (int a = 0; a < NA; a++)
-#pragma unroll
-          for (int l = 0; l < kSlices; l++)
-#pragma unroll
-            for (int s = 0; s <= l; s++)
-              lio::umma::mma_i8(tbase + (uint32_t)((a * kSlices + l) * kTcFuncs),
-                                ad0 + (uint64_t)(((a * kSlices + s) * kTcSliceA) >> 4),
-                                bd0 + (uint64_t)(((l - s) * kTcSliceB) >> 4), idesc, s > 0 ? 1u : keep);
-        lio::umma::commit(&empty[buf]);
-        if (kk == nks - 1) lio::umma::commit(&tfull);
       }
+      if (stop) *vfail = 1;
+      // every MMA issued so far has completed once this arrives
+      lio::umma::commit(&drain);
+      if (!lio::umma::mbar_wait(&drain, 0)) *vfail = 1;
     }
   } else {
     // ------------------------------------------------------------ epilogue
+    const int quad = warp & 3, colg = warp >> 2;
+    const int row = quad * 32 + lane;
+    const int etid = tid;  // 0 .. 255
     const uint32_t lane_base = tbase + ((uint32_t)(quad * 32) << 16);
-    double sp[NA];  // 2^(point exponent - 7(S+1)) per kind
-#pragma unroll
-    for (int a = 0; a < NA; a++) sp[a] = pow2(aexp[G.aexp_off + (long long)a * G.ldp + p] - 7 * (kSlices + 1));
-    const double rp[3] = {px[G.pt_off + p], py[G.pt_off + p], pz[G.pt_off + p]};
-    const double* rad = radial + G.rad_off;
-    const long long rstride = (long long)G.nsimple * G.ldp;
-    for (int ft = 0; ft < nft; ft++) {
-      const int c0 = ft * kTcFuncs + colg * kTcEpiCols;  // first function of this warp's columns
-      if (!lio::umma::mbar_wait(&tfull, ft & 1)) {
-        fail = 1;
-        break;
+    double* gvw = reinterpret_cast<double*>(tc_smem + Cfg::kGv + (size_t)warp * Cfg::kGvWarp);
+    double* red = reinterpret_cast<double*>(tc_smem + Cfg::kRed);
+    double* tsa = reinterpret_cast<double*>(tc_smem + Cfg::kTab);  // 2^f_i, spin a
+    double* tsb = tsa + fcap;                                        // spin b (NS = 2 only)
+    bool lfail = false;
+    int ucnt = 0;
+    for (int w = blockIdx.x; w < ntiles; w += gridDim.x) {
+      const int2 t = tiles[w];
+      const GroupDev& G = groups[t.x];
+      const int m = G.m, ldp = G.ldp;
+      const int nft = (m + kTcFuncs - 1) / kTcFuncs, ntt = nft * NP;
+      const int p = t.y * kTcPoints + row;
+      // per-function scales of this group (the previous tile's readers are past the last barrier)
+      const int mt = nft * kTcFuncs;  // <= fcap: fcap covers the largest padded m
+      for (int i = etid; i < mt; i += kTcEpiWarps * 32) {
+        tsa[i] = i < m ? pow2(dexp_a[G.dexp_off + i]) : 0.0;
+        if (NS == 2) tsb[i] = i < m ? pow2(dexp_b[G.dexp_off + i]) : 0.0;
       }
-      lio::umma::fence_after_sync();
-      double Gv[NA][kTcEpiCols];
+      epi_sync_or(false);
+      double spx[NA];  // 2^(point exponent - 7(S+1)) per kind
 #pragma unroll
-      for (int a = 0; a < NA; a++) {
-        int32_t lv[kSlices][kTcEpiCols];
+      for (int a = 0; a < NA; a++) spx[a] = pow2(aexp[G.aexp_off + (long long)a * ldp + p] - 7 * (kSlices + 1));
+      // FP64 basis values of this point: kind k of function i at bas[k * ks + i * ldp]
+      // (F; dF/dx, dF/dy, dF/dz; d2F xx, yy, zz, xy, xz, yz)
+      const double* bas = basis + G.bas_off + p;
+      const long long ks = (long long)m * ldp;
+      double q[NS][NQ];
 #pragma unroll
-        for (int l = 0; l < kSlices; l++)
-          tmem_ld_cols<kTcEpiCols>(lane_base + (uint32_t)((a * kSlices + l) * kTcFuncs + colg * kTcEpiCols), lv[l]);
-        lio::umma::tmem_wait_ld();
+      for (int sp = 0; sp < NS; sp++)
 #pragma unroll
-        for (int c = 0; c < kTcEpiCols; c++) {
-          // levels pairwise in int32 (|acc| < 2^23, so 128 acc_l + acc_l+1 fits), then exactly in int64
-          long long V = 0;
+        for (int k = 0; k < NQ; k++) q[sp][k] = 0.0;
+      for (int tt = 0; tt < ntt; tt++, ucnt++) {
+        const int ft = tt / NP, pass = tt - ft * NP;
+        const int cb = ft * kTcFuncs + colg * CPW;  // first function of this warp's columns
+        const bool narrow = G.m32 <= kTcNarrowK;
+        bool ok = !lfail && !*vfail && lio::umma::mbar_wait(&tfull, ucnt & 1);
+        ok = __all_sync(0xffffffffu, ok);
+        if (!ok) {
+          lfail = true;
+          *vfail = 1;
+        }
+        lio::umma::fence_after_sync();
+        if (ok) {
 #pragma unroll
-          for (int l = 0; l < kSlices; l += 2) V = V * (1LL << 14) + (long long)(lv[l][c] * 128 + lv[l + 1][c]);
-          Gv[a][c] = (double)V * sp[a];
+          for (int sp = 0; sp < NS; sp++)
+#pragma unroll
+            for (int kp = 0; kp < KP; kp++) {
+              const double sa = spx[pass * KP + kp];
+#pragma unroll
+              for (int c8 = 0; c8 < CPW / 8; c8++) {
+                int32_t lv[kSlices][8];
+#pragma unroll
+                for (int l = 0; l < kSlices; l++)
+                  lio::umma::tmem_ld8(
+                      lane_base + (uint32_t)(((sp * KP + kp) * kSlices + l) * kTcFuncs + colg * CPW + c8 * 8), lv[l]);
+                lio::umma::tmem_wait_ld();
+#pragma unroll
+                for (int c = 0; c < 8; c++)
+                  gvw[((sp * KP + kp) * CPW + c8 * 8 + c) * 32 + lane] = level_sum(lv, c, narrow) * sa;
+              }
+            }
+        }
+        // accumulators read: hand TMEM back to the MMA issuer
+        lio::umma::fence_before_sync();
+        __syncwarp();
+        if (lane == 0 && ok) lio::umma::mbar_arrive(&tempty);
+        unit_row_dots<GGA, NS, NQ, KP>(pass * KP, bas, ks, ldp, cb, m, gvw, tsa, tsb, lane, q);
+        __syncwarp();  // every lane done with this unit's staged values
+      }
+      // tile done: column group 1 hands its sums to column group 0, which writes them
+      if (colg == 1) {
+#pragma unroll
+        for (int sp = 0; sp < NS; sp++)
+#pragma unroll
+          for (int k = 0; k < NQ; k++) red[(sp * kTcPoints + row) * NQ + k] = q[sp][k];
+      }
+      const bool anyfail = epi_sync_or(lfail || *vfail);
+      if (anyfail) break;
+      if (colg == 0) {
+#pragma unroll
+        for (int sp = 0; sp < NS; sp++) {
+          double* dst = (sp == 0 ? part_a : part_b) + G.part_off;
+#pragma unroll
+          for (int k = 0; k < NQ; k++) dst[(long long)k * ldp + p] = q[sp][k] + red[(sp * kTcPoints + row) * NQ + k];
         }
       }
-      // accumulators read: hand TMEM back to the MMA issuer
-      lio::umma::fence_before_sync();
-      __syncwarp();
-      if (lane == 0) lio::umma::mbar_arrive(&tempty);
-#pragma unroll 1
-      for (int c = 0; c < kTcEpiCols; c++) {
-        const int i = c0 + c;
-        if (i >= G.m) break;
-        const int sh = fn_sh[G.fn_off + i];
-        const int code = fn_cp[G.fn_off + i];
-        const double sc = (code & 16) ? dnorm : 1.0;
-        const int atom = fn_atom[G.fn_off + i];
-        const double si = pow2(dexp[G.dexp_off + i]);
-        const double rr[3] = {rp[0] - ax[atom], rp[1] - ay[atom], rp[2] - az[atom]};
-        const long long ro = (long long)sh * G.ldp + p;
-        const double tv = rad[ro], tg = rad[rstride + ro], th = rad[2 * rstride + ro];
-        double F, g[3], h[6];
-        rebuild_cp<(NA > 1)>(code & 15, rr, tv, tg, th, sc, F, g, h);
-        double gg[4];
-#pragma unroll
-        for (int a = 0; a < 4; a++) gg[a] = Gv[a % NA][c] * si;
-        q[0] += F * gg[0];
-        if (NA > 1) {
-          const double g0 = gg[0];
-          q[1 % NQ] += 2.0 * g[0] * g0;
-          q[2 % NQ] += 2.0 * g[1] * g0;
-          q[3 % NQ] += 2.0 * g[2] * g0;
-          q[4 % NQ] += 2.0 * (h[0] * g0 + g[0] * gg[1]);
-          q[5 % NQ] += 2.0 * (h[1] * g0 + g[1] * gg[2]);
-          q[6 % NQ] += 2.0 * (h[2] * g0 + g[2] * gg[3]);
-          q[7 % NQ] += 2.0 * (h[3] * g0 + g[1] * gg[1]);  // xy: gy . Gx (= gx . Gy by symmetry of D)
-          q[8 % NQ] += 2.0 * (h[4] * g0 + g[2] * gg[1]);  // xz: gz . Gx
-          q[9 % NQ] += 2.0 * (h[5] * g0 + g[2] * gg[2]);  // yz: gz . Gy
-        }
-      }
+      epi_sync_or(false);  // the table and the reduction area are free again
     }
   }
-  __syncthreads();  // every role done; all copies and MMAs have completed
-  const bool ok = fail == 0;
-  double* red = reinterpret_cast<double*>(tc_smem);  // [column group 1..][point][NQ]
-  if (ok && warp < kTcEpiWarps && colg > 0) {
-#pragma unroll
-    for (int k = 0; k < NQ; k++) red[((colg - 1) * kTcPoints + row) * NQ + k] = q[k];
-  }
-  __syncthreads();
-  if (ok && warp < kTcEpiWarps && colg == 0) {
-    double* dst = partial + G.part_off;
-#pragma unroll
-    for (int k = 0; k < NQ; k++) {
-      double v = q[k];
-#pragma unroll
-      for (int gi = 1; gi < kGroups; gi++) v += red[((gi - 1) * kTcPoints + row) * NQ + k];
-      dst[(long long)k * G.ldp + p] = v;
-    }
-  } else if (!ok && tid == 0) {
-    atomicExch(err, 1);
+  __syncthreads();  // every role done
+  if (warp == kTcEpiWarps && lane == 0) {
+    // copies issued but never consumed (after a timeout) land before the CTA exits
+    for (int k = consumed; k < issued; k++)
+      if (!lio::umma::mbar_wait(&full[k % kStages], (k / kStages) & 1)) break;
   }
   lio::umma::fence_before_sync();
   __syncthreads();
+  if (tid == 0 && fail) atomicExch(err, 1);
   if (warp == 0) lio::umma::tmem_dealloc(tbase, Cfg::kTmem);
 }

@@ -55,7 +55,7 @@ constexpr int kNQ = 10;      // rho, grad[3], (xx,yy,zz), (xy,xz,yz)
 
 struct GroupDev {
   int npts, ldp, m, nsimple;
-  int nft, m32, nft32, pad2;  // m32: m rounded up to 32; nft32: tensor-core function tiles
+  int nft, m32, nftc, pad2;  // m32: m rounded up to 32; nftc: 32-function tensor-core density tiles
   long long pt_off;    // point arrays
   long long fn_off;    // fn_glob, fn_sh, fn_cp
   long long sf_off;    // sf_glob / sf_type
@@ -65,7 +65,7 @@ struct GroupDev {
   long long sl_off;    // int8 slices of the density A operands (bytes)
   long long aexp_off;  // their per-point exponents (elements): NA x ldp
   long long ds_off;    // int8 slices of the density matrix (bytes, one spin)
-  long long dexp_off;  // their per-function exponents (elements): nft32 x kTcFuncs
+  long long dexp_off;  // their per-function exponents (elements): nftc x 32
   long long fa_off;    // int8 slices of F by function row for the Kohn-Sham contraction (bytes)
   long long fae_off;   // their per-row exponents (elements): nI x 128
   long long fb_off;    // int8 slices of f*F by row (bytes, one spin)
@@ -504,6 +504,8 @@ struct DeviceEngine::Impl {
   DevBuf<int8_t> fn_cp;
   // tensor-core form (built on first use per geometry)
   DevBuf<int2> slice_basis_tiles, slice_dens_tiles;
+  DevBuf<int2> dens_tc_tiles;  // (group, 128-point tile), largest function count first
+  int tc_fcap = 0, nsm = 148;
 
   DevBuf<double> radial;
   DevBuf<int8_t> aslices, dslices_a, dslices_b;
@@ -626,6 +628,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
   std::vector<int2> farows, fbrows;
   std::vector<int4> fktiles;
   long long npts_total = 0;
+  int maxm = 0;
   const int NA = sys.lda ? 1 : 4;
   const int ngr = part.total_groups();
   for (int g = 0; g < ngr; g++) {
@@ -637,7 +640,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
     G.m32 = ((G.m + 31) / 32) * 32;
     G.nsimple = (int)pg.funcs.size();
     G.nft = (G.m + kTile - 1) / kTile;
-    G.nft32 = (G.m + kTcFuncs - 1) / kTcFuncs;
+    G.nftc = (G.m + kTcFuncs - 1) / kTcFuncs;
     G.pt_off = pt_off;
     G.fn_off = fn_off;
     G.sf_off = sf_off;
@@ -693,21 +696,19 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
       for (int ft = 0; ft < G.nft; ft++) dtiles.push_back({g, pt, ft, 0});
     for (int it = 0; it < G.nft; it++)
       for (int jt = it; jt < G.nft; jt++) ktiles.push_back({g, it, jt, 0});
-    for (int T = 0; T < G.ldp / kTcPoints; T++) {
-      sbtiles.push_back({g, T});
-      (void)T;
-    }
-    for (int ft = 0; ft < G.nft32; ft++) sdtiles.push_back({g, ft});
+    for (int T = 0; T < G.ldp / kTcPoints; T++) sbtiles.push_back({g, T});
+    maxm = std::max(maxm, G.m);
+    for (int ft = 0; ft < G.nftc; ft++) sdtiles.push_back({g, ft});
     pt_off += G.ldp;
     fn_off += G.m;
     sf_off += G.nsimple;
     bas_off += (long long)d->nk * G.m * G.ldp;
     part_off += (long long)G.nft * NQ * G.ldp;
     rad_off += 3LL * G.nsimple * G.ldp;
-    sl_off += (long long)kSlices * NA * G.ldp * G.m32;
+    sl_off += (long long)(G.ldp / kTcPoints) * NA * (G.m32 / 32) * kTcStepA;
     aexp_off += (long long)NA * G.ldp;
-    ds_off += (long long)G.nft32 * kSlices * kTcFuncs * G.m32;
-    dexp_off += (long long)G.nft32 * kTcFuncs;
+    ds_off += (long long)G.nftc * (G.m32 / 32) * kTcStepD;
+    dexp_off += (long long)G.nftc * kTcFuncs;
     fa_off += (long long)nI * kSlices * kFkRows * G.ldp;
     fae_off += (long long)nI * kFkRows;
     fb_off += (long long)nJ * kSlices * kFkCols * G.ldp;
@@ -748,6 +749,13 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
   d->fn_atom.upload(hfat);
   d->fn_cp.upload(hfcp);
   d->slice_basis_tiles.upload(sbtiles);
+  {
+    // persistent tensor-core density: heaviest tiles first, dealt round-robin to the CTAs
+    std::vector<int2> order = sbtiles;
+    std::stable_sort(order.begin(), order.end(), [&](const int2& a, const int2& b) { return gd[a.x].m > gd[b.x].m; });
+    d->dens_tc_tiles.upload(order);
+    d->tc_fcap = ((maxm + 31) / 32) * 32;  // per-function table of the tensor-core density
+  }
   d->slice_dens_tiles.upload(sdtiles);
   (void)tctiles;
   d->sf_glob.upload(hsf);
@@ -838,8 +846,27 @@ void DeviceEngine::prepare_tensor_core() {
   }
   LIO_CUDA(cudaFuncSetAttribute(k_fock_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FkCfg<1>::kSmem));
   LIO_CUDA(cudaFuncSetAttribute(k_fock_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FkCfg<2>::kSmem));
-  LIO_CUDA(cudaFuncSetAttribute(k_density_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TcCfg<1>::kSmem));
-  LIO_CUDA(cudaFuncSetAttribute(k_density_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TcCfg<4>::kSmem));
+  {
+    int dev = 0;
+    LIO_CUDA(cudaGetDevice(&dev));
+    LIO_CUDA(cudaDeviceGetAttribute(&d->nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int cap = d->tc_fcap;
+    int optin = 0;
+    LIO_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t need = d->lda ? (d->open ? TcCfg<false, 2>::smem(cap) : TcCfg<false, 1>::smem(cap))
+                               : (d->open ? TcCfg<true, 2>::smem(cap) : TcCfg<true, 1>::smem(cap));
+    if (need + 256 > (size_t)optin)
+      throw std::runtime_error("tensor-core density: a group with " + std::to_string(cap) +
+                               " functions needs more shared memory than a block can have; use precision 0");
+    LIO_CUDA(cudaFuncSetAttribute(k_density_tc<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)TcCfg<false, 1>::smem(cap)));
+    LIO_CUDA(cudaFuncSetAttribute(k_density_tc<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)TcCfg<false, 2>::smem(cap)));
+    LIO_CUDA(cudaFuncSetAttribute(k_density_tc<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)TcCfg<true, 1>::smem(cap)));
+    LIO_CUDA(cudaFuncSetAttribute(k_density_tc<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)TcCfg<true, 2>::smem(cap)));
+  }
   d->tc_ready = true;
 }
 
@@ -869,26 +896,36 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
     prepare_tensor_core();
     d->mark(0);
   }
-  for (int s = 0; s < nspin; s++) {
-    const double* P = s == 0 ? d->P_a.p : d->P_b.p;
-    double* part = s == 0 ? d->part_a.p : d->part_b.p;
-    if (tc) {
+  if (tc) {
+    // D slices of each spin, then one launch for both spins (shared A slices and basis rebuild)
+    for (int s = 0; s < nspin; s++) {
+      const double* P = s == 0 ? d->P_a.p : d->P_b.p;
       int8_t* dsl = s == 0 ? d->dslices_a.p : d->dslices_b.p;
       int16_t* dex = s == 0 ? d->dexp_a.p : d->dexp_b.p;
       k_slice_density<<<(unsigned)d->slice_dens_tiles.n, kTcFuncs, 0, st>>>(d->slice_dens_tiles.p, d->groups.p,
                                                                           d->fn_glob.p, P, d->M, dsl, dex);
       LIO_CUDA(cudaGetLastError());
-      if (d->lda)
-        k_density_tc<1><<<(unsigned)d->slice_basis_tiles.n, TcCfg<1>::kThreads, TcCfg<1>::kSmem, st>>>(
-            d->slice_basis_tiles.p, d->groups.p, d->aslices.p, d->aexp.p, dsl, dex, d->radial.p, d->px.p, d->py.p,
-            d->pz.p, d->fn_sh.p, d->fn_cp.p, d->fn_atom.p, d->ax.p, d->ay.p, d->az.p, d->d_norm, part, d->tc_err.p);
-      else
-        k_density_tc<4><<<(unsigned)d->slice_basis_tiles.n, TcCfg<4>::kThreads, TcCfg<4>::kSmem, st>>>(
-            d->slice_basis_tiles.p, d->groups.p, d->aslices.p, d->aexp.p, dsl, dex, d->radial.p, d->px.p, d->py.p,
-            d->pz.p, d->fn_sh.p, d->fn_cp.p, d->fn_atom.p, d->ax.p, d->ay.p, d->az.p, d->d_norm, part, d->tc_err.p);
-      LIO_CUDA(cudaGetLastError());
-      launches += 2;
+      launches++;
+    }
+    const int ntiles = (int)d->dens_tc_tiles.n;
+    const unsigned nt = (unsigned)std::min(ntiles, d->nsm);
+    const int cap = d->tc_fcap;
+#define LIO_DENSITY_TC(GGA, NS)                                                                                    \
+  k_density_tc<GGA, NS><<<nt, TcCfg<GGA, NS>::kThreads, TcCfg<GGA, NS>::smem(cap), st>>>(                          \
+      d->dens_tc_tiles.p, ntiles, d->groups.p, d->aslices.p, d->aexp.p, d->dslices_a.p, d->dexp_a.p,               \
+      d->dslices_b.p, d->dexp_b.p, d->basis.p, cap, d->part_a.p, d->part_b.p, d->tc_err.p)
+    if (d->lda) {
+      if (d->open) LIO_DENSITY_TC(false, 2); else LIO_DENSITY_TC(false, 1);
     } else {
+      if (d->open) LIO_DENSITY_TC(true, 2); else LIO_DENSITY_TC(true, 1);
+    }
+#undef LIO_DENSITY_TC
+    LIO_CUDA(cudaGetLastError());
+    launches++;
+  } else {
+    for (int s = 0; s < nspin; s++) {
+      const double* P = s == 0 ? d->P_a.p : d->P_b.p;
+      double* part = s == 0 ? d->part_a.p : d->part_b.p;
       if (d->lda)
         k_density_fp64<1><<<nd, 256, 0, st>>>(d->dens_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, P, d->M, part);
       else

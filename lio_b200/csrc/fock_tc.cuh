@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
               const int8_t* __restrict__ bslices_b, const int16_t* __restrict__ bexp_b, int M,
               double* __restrict__ K_a, double* __restrict__ K_b, int* __restrict__ err) {
   using Cfg = FkCfg<NS>;
-  extern __shared__ __align__(1024) uint8_t fk_smem[];
+  extern __shared__ __align__(128) uint8_t fk_smem[];
   __shared__ uint64_t full[kFkStages], empty[kFkStages], done;
   __shared__ uint32_t tmem_base;
   __shared__ int fail;
