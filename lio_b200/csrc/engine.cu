@@ -513,7 +513,7 @@ struct DeviceEngine::Impl {
   DevBuf<int> tc_err;
   long long tc_sizes[5] = {0, 0, 0, 0, 0};
   // tensor-core Kohn-Sham contraction
-  DevBuf<int2> fa_rows, fb_rows;
+  DevBuf<int2> fa_rows, fb_rows, fa_tiles32, fb_tiles32;  // rows, and 32-row pieces, of the Fock slice blocks
   DevBuf<int4> fk_tiles;
   DevBuf<int8_t> fa_slices, fb_slices_a, fb_slices_b;
   DevBuf<int16_t> fa_exp, fb_exp_a, fb_exp_b;
@@ -625,7 +625,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
   long long pt_off = 0, fn_off = 0, sf_off = 0, bas_off = 0, part_off = 0;
   long long rad_off = 0, sl_off = 0, aexp_off = 0, ds_off = 0, dexp_off = 0;
   long long fa_off = 0, fae_off = 0, fb_off = 0, fbe_off = 0;
-  std::vector<int2> farows, fbrows;
+  std::vector<int2> farows, fbrows, fat32, fbt32;
   std::vector<int4> fktiles;
   long long npts_total = 0;
   int maxm = 0;
@@ -658,6 +658,8 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
     const int nI = (G.m + kFkRows - 1) / kFkRows, nJ = (G.m + kFkCols - 1) / kFkCols;
     for (int i = 0; i < nI * kFkRows; i++) farows.push_back({g, i});
     for (int j = 0; j < nJ * kFkCols; j++) fbrows.push_back({g, j});
+    for (int i = 0; i < nI * kFkRows; i += 32) fat32.push_back({g, i});
+    for (int j = 0; j < nJ * kFkCols; j += 32) fbt32.push_back({g, j});
     for (int I = 0; I < nI; I++)
       for (int J = 0; J < nJ; J++)
         if (J * kFkCols + kFkCols - 1 >= I * kFkRows) fktiles.push_back({g, I, J, 0});
@@ -728,6 +730,8 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
   d->fk_sizes[3] = fbe_off;
   d->fa_rows.upload(farows);
   d->fb_rows.upload(fbrows);
+  d->fa_tiles32.upload(fat32);
+  d->fb_tiles32.upload(fbt32);
   d->fk_tiles.upload(fktiles);
   d->hgroups = gd;
   d->ngroups = ngr;
@@ -840,8 +844,11 @@ void DeviceEngine::prepare_tensor_core() {
   }
   {
     const int nrows = (int)d->fa_rows.n;
-    k_slice_fock<kFkRows><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(d->fa_rows.p, nrows, d->groups.p, d->basis.p,
-                                                                       nullptr, d->fa_slices.p, d->fa_exp.p, 0);
+    k_fock_rowexp<1><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(d->fa_rows.p, nrows, d->groups.p, d->basis.p,
+                                                                  nullptr, nullptr, d->fa_exp.p, nullptr, 0);
+    LIO_CUDA(cudaGetLastError());
+    k_fock_slices<kFkRows, false, 1><<<(unsigned)d->fa_tiles32.n, 256, 0, st>>>(
+        d->fa_tiles32.p, d->groups.p, d->basis.p, nullptr, nullptr, d->fa_exp.p, nullptr, d->fa_slices.p, nullptr, 0);
     LIO_CUDA(cudaGetLastError());
   }
   LIO_CUDA(cudaFuncSetAttribute(k_fock_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FkCfg<1>::kSmem));
@@ -949,14 +956,26 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
     LIO_CUDA(cudaMemsetAsync(d->K_a.p, 0, npacked * sizeof(double), st));
     if (d->open) LIO_CUDA(cudaMemsetAsync(d->K_b.p, 0, npacked * sizeof(double), st));
     if (tc) {
+      // f * F slices of both spins: row exponents, then the slices (one pass over F each)
       const int nrows = (int)d->fb_rows.n;
-      for (int s = 0; s < (d->open ? 2 : 1); s++) {
-        k_slice_fock<kFkCols><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(
-            d->fb_rows.p, nrows, d->groups.p, d->basis.p, s == 0 ? d->fac_a.p : d->fac_b.p,
-            s == 0 ? d->fb_slices_a.p : d->fb_slices_b.p, s == 0 ? d->fb_exp_a.p : d->fb_exp_b.p, 1);
+      if (d->open) {
+        k_fock_rowexp<2><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(d->fb_rows.p, nrows, d->groups.p, d->basis.p,
+                                                                      d->fac_a.p, d->fac_b.p, d->fb_exp_a.p,
+                                                                      d->fb_exp_b.p, 1);
         LIO_CUDA(cudaGetLastError());
-        launches++;
+        k_fock_slices<kFkCols, true, 2><<<(unsigned)d->fb_tiles32.n, 256, 0, st>>>(
+            d->fb_tiles32.p, d->groups.p, d->basis.p, d->fac_a.p, d->fac_b.p, d->fb_exp_a.p, d->fb_exp_b.p,
+            d->fb_slices_a.p, d->fb_slices_b.p, 1);
+      } else {
+        k_fock_rowexp<1><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(d->fb_rows.p, nrows, d->groups.p, d->basis.p,
+                                                                      d->fac_a.p, nullptr, d->fb_exp_a.p, nullptr, 1);
+        LIO_CUDA(cudaGetLastError());
+        k_fock_slices<kFkCols, true, 1><<<(unsigned)d->fb_tiles32.n, 256, 0, st>>>(
+            d->fb_tiles32.p, d->groups.p, d->basis.p, d->fac_a.p, nullptr, d->fb_exp_a.p, nullptr, d->fb_slices_a.p,
+            nullptr, 1);
       }
+      LIO_CUDA(cudaGetLastError());
+      launches += 2;
       if (d->open)
         k_fock_tc<2><<<(unsigned)d->fk_tiles.n, FkCfg<2>::kThreads, FkCfg<2>::kSmem, st>>>(
             d->fk_tiles.p, d->groups.p, d->fn_glob.p, d->fa_slices.p, d->fa_exp.p, d->fb_slices_a.p, d->fb_exp_a.p,

@@ -5,68 +5,129 @@
 // as the reduction dimension:
 //   A_ip = F_ip          = 2^(a_i) sum_s a_s[i][p] 128^-(s+1)  (per geometry, per function row)
 //   B_jp = f_p F_jp      = 2^(b_j) sum_t b_t[j][p] 128^-(t+1)  (per solve and spin, per row)
-// with the same int8 slices, level accumulators and exact int64 level sum as
-// the density contraction. A tile is 128 functions (i) x 32 functions (j);
-// both spins share the A slices and keep 2 x S level accumulators in TMEM.
+// with the same int8 slices, level accumulators and level sum as the density
+// contraction. A tile is 128 functions (i) x 32 functions (j); the S slices
+// of a B tile are stacked along N (row t * 32 + j holds b_t[j]), so one MMA per
+// A slice s (N = (S - s) * 32) lands every product (s, t) on level s + t.
+// Both spins share the A slices and keep 2 x S level blocks in TMEM.
 #pragma once
 
 constexpr int kFkRows = 128;  // UMMA M: functions i per tile
-constexpr int kFkCols = 32;   // UMMA N: functions j per tile
+constexpr int kFkCols = 32;   // functions j per tile (output columns per level)
+constexpr int kFkTall = kSlices * kFkCols;  // rows of the stacked B operand
 constexpr int kFkStages = 4;
-constexpr int kFkSliceA = 32 * kFkRows;  // bytes of one A slice per 32-point K step
-constexpr int kFkSliceB = 32 * kFkCols;
+constexpr int kFkSliceA = 32 * kFkRows;       // bytes of one A slice per 32-point K step
+constexpr int kFkStepA = kSlices * kFkSliceA;  // all A slices of a K step (contiguous)
+constexpr int kFkStepB = 32 * kFkTall;         // one spin's stacked B slices of a K step (contiguous)
 template <int NS>
 struct FkCfg {
-  static constexpr int kStageA = kSlices * kFkSliceA;
-  static constexpr int kStage = kStageA + NS * kSlices * kFkSliceB;
+  static constexpr int kStageA = kFkStepA;
+  static constexpr int kStage = kStageA + NS * kFkStepB;
   static constexpr size_t kSmem = (size_t)kFkStages * kStage;
   static constexpr uint32_t kCols = NS * kSlices * kFkCols;
   static constexpr uint32_t kTmem = kCols <= 256 ? 256 : 512;
   static constexpr int kThreads = 32 * 6;  // 4 epilogue warps, producer, MMA issuer
 };
 
-// One warp per (group, row) of a padded slice block: the row's exponent from
-// max_p |v_p| (v = F_rp, times fac_p when fac != nullptr), then its S slices,
-// in the K-major interleaved layout of an R-row block (R = kFkRows for A,
-// kFkCols for B). Rows at or beyond m are written as zeros.
-template <int R>
-__global__ void k_slice_fock(const int2* __restrict__ rows, int nrows, const GroupDev* __restrict__ groups,
-                             const double* __restrict__ basis, const double* __restrict__ fac,
-                             int8_t* __restrict__ slices, int16_t* __restrict__ expo, int use_sl_b) {
+// Slices of the rows of v = F (A operand, per geometry) or v = f_s F (B
+// operand, per solve, both spins at once), in two passes over the FP64 basis.
+//
+// Pass 1, one warp per (group, row): the row's exponent per spin from
+// max_p |v_p|. Rows at or beyond m get exponent 0 (their slices are zeros).
+template <int NS>
+__global__ void k_fock_rowexp(const int2* __restrict__ rows, int nrows, const GroupDev* __restrict__ groups,
+                              const double* __restrict__ basis, const double* __restrict__ fac_a,
+                              const double* __restrict__ fac_b, int16_t* __restrict__ expo_a,
+                              int16_t* __restrict__ expo_b, int use_sl_b) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (warp >= nrows) return;  // whole warps only
   const int2 t = rows[warp];
-  const GroupDev G = groups[t.x];
-  const int i = t.y;
-  const bool valid = i < G.m;
-  const double* Fi = basis + G.bas_off + (long long)(valid ? i : 0) * G.ldp;
-  double amax = 0.0;
-  if (valid)
-    for (int p = lane; p < G.ldp; p += 32) {
-      double v = Fi[p];
-      if (fac) v *= fac[G.pt_off + p];
-      amax = fmax(amax, fabs(v));
+  const GroupDev& G = groups[t.x];
+  const int i = t.y, ldp = G.ldp;
+  double amax[NS];
+#pragma unroll
+  for (int sp = 0; sp < NS; sp++) amax[sp] = 0.0;
+  if (i < G.m) {
+    const double* Fi = basis + G.bas_off + (long long)i * ldp;
+    for (int p = lane; p < ldp; p += 32) {
+      const double v = Fi[p];
+#pragma unroll
+      for (int sp = 0; sp < NS; sp++) {
+        const double* fac = sp == 0 ? fac_a : fac_b;
+        amax[sp] = fmax(amax[sp], fabs(fac ? v * fac[G.pt_off + p] : v));
+      }
     }
-  for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
-  const int e = slice_exponent(amax);
+  }
+  const long long ebase = use_sl_b ? G.fbe_off : G.fae_off;
+#pragma unroll
+  for (int sp = 0; sp < NS; sp++) {
+    double a = amax[sp];
+    for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+    if (lane == 0) (sp == 0 ? expo_a : expo_b)[ebase + i] = (int16_t)slice_exponent(a);
+  }
+}
+
+// Pass 2, a CTA per 32-row piece of a row tile (lane = row), each warp taking
+// 16-point blocks: per spin and slice one 16-byte store. Layout per row tile
+// (R rows) and 32-point K step: A (TALL = false): the S slices one after the
+// other, each an R-row x 32-byte K-major block; B (TALL = true): one
+// (S * R)-row x 32-byte block whose row t * R + r holds slice t of row r.
+template <int R, bool TALL, int NS>
+__global__ void __launch_bounds__(256) k_fock_slices(const int2* __restrict__ rtiles, const GroupDev* __restrict__ groups,
+                                                     const double* __restrict__ basis,
+                                                     const double* __restrict__ fac_a,
+                                                     const double* __restrict__ fac_b,
+                                                     const int16_t* __restrict__ expo_a,
+                                                     const int16_t* __restrict__ expo_b, int8_t* __restrict__ sl_a,
+                                                     int8_t* __restrict__ sl_b, int use_sl_b) {
+  constexpr int kStep = kSlices * 32 * R;  // bytes of one K step of a row tile (either layout)
+  const int2 t = rtiles[blockIdx.x];
+  const GroupDev& G = groups[t.x];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = t.y + lane, ldp = G.ldp, nkp = ldp / 32;
+  const bool valid = i < G.m;
   const long long base = use_sl_b ? G.fb_off : G.fa_off;
   const long long ebase = use_sl_b ? G.fbe_off : G.fae_off;
-  if (lane == 0) expo[ebase + i] = (int16_t)e;
+  double sc[NS];
+#pragma unroll
+  for (int sp = 0; sp < NS; sp++) sc[sp] = pow2(-(int)(sp == 0 ? expo_a : expo_b)[ebase + i]);
   const int tile = i / R, r = i % R;
-  int8_t* dst = slices + base + (long long)tile * kSlices * R * G.ldp;
-  for (int p = lane; p < G.ldp; p += 32) {
-    double x = 0.0;
-    if (valid) {
-      double v = Fi[p];
-      if (fac) v *= fac[G.pt_off + p];
-      x = ldexp(v, -e);
+  const double* Fi = basis + G.bas_off + (long long)(valid ? i : 0) * ldp;
+  for (int b = warp; b < ldp / 16; b += blockDim.x / 32) {
+    const int p0 = b * 16;
+    double F[16];
+#pragma unroll
+    for (int k = 0; k < 16; k += 2) {
+      const double2 v = valid ? *reinterpret_cast<const double2*>(Fi + p0 + k) : make_double2(0.0, 0.0);
+      F[k] = v.x;
+      F[k + 1] = v.y;
     }
-    const uint32_t off = lio::umma::kmajor_offset(r, p, R);
-    for (int s = 0; s < kSlices; s++) {
-      x *= 128.0;
-      const double d = rint(x);
-      x -= d;
-      dst[(long long)s * R * G.ldp + off] = (int8_t)d;
+#pragma unroll
+    for (int sp = 0; sp < NS; sp++) {
+      const double* fac = sp == 0 ? fac_a : fac_b;
+      int8_t* blk = (sp == 0 ? sl_a : sl_b) + base + ((long long)tile * nkp + (p0 >> 5)) * kStep;
+      double x[16];
+#pragma unroll
+      for (int k = 0; k < 16; k++) x[k] = (fac ? F[k] * fac[G.pt_off + p0 + k] : F[k]) * sc[sp];
+#pragma unroll
+      for (int s = 0; s < kSlices; s++) {
+        uint32_t w[4];
+#pragma unroll
+        for (int k4 = 0; k4 < 4; k4++) {
+          uint32_t packed = 0;
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const double y = x[k4 * 4 + k] * 128.0;
+            const double d = rint(y);
+            x[k4 * 4 + k] = y - d;
+            packed |= ((uint32_t)(uint8_t)(int8_t)d) << (8 * k);
+          }
+          w[k4] = packed;
+        }
+        const uint32_t off = TALL ? lio::umma::kmajor_offset(s * R + r, p0 & 31, kSlices * R)
+                                  : s * 32 * R + lio::umma::kmajor_offset(r, p0 & 31, R);
+        *reinterpret_cast<uint4*>(blk + off) = make_uint4(w[0], w[1], w[2], w[3]);
+      }
     }
   }
 }
@@ -109,9 +170,9 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
   const uint32_t tbase = tmem_base;
   if (warp == 4) {
     if (lane == 0) {
-      const int8_t* A = aslices + G.fa_off + (long long)I * kSlices * kFkRows * G.ldp;
-      const int8_t* Ba = bslices_a + G.fb_off + (long long)J * kSlices * kFkCols * G.ldp;
-      const int8_t* Bb = NS == 2 ? bslices_b + G.fb_off + (long long)J * kSlices * kFkCols * G.ldp : nullptr;
+      const int8_t* A = aslices + G.fa_off + (long long)I * nsteps * kFkStepA;
+      const int8_t* Ba = bslices_a + G.fb_off + (long long)J * nsteps * kFkStepB;
+      const int8_t* Bb = NS == 2 ? bslices_b + G.fb_off + (long long)J * nsteps * kFkStepB : nullptr;
       for (int st = 0; st < nsteps; st++) {
         const int buf = st % kFkStages, use = st / kFkStages;
         if (use > 0 && !lio::umma::mbar_wait(&empty[buf], (use - 1) & 1)) {
@@ -120,20 +181,14 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
         }
         uint8_t* stage = fk_smem + buf * Cfg::kStage;
         lio::umma::mbar_expect_tx(&full[buf], (uint32_t)Cfg::kStage);
-        for (int s = 0; s < kSlices; s++)
-          lio::umma::bulk_copy_g2s(stage + s * kFkSliceA, A + (long long)s * kFkRows * G.ldp + st * kFkSliceA,
-                                   kFkSliceA, &full[buf]);
-        for (int sp = 0; sp < NS; sp++) {
-          const int8_t* B = sp == 0 ? Ba : Bb;
-          for (int s = 0; s < kSlices; s++)
-            lio::umma::bulk_copy_g2s(stage + Cfg::kStageA + (sp * kSlices + s) * kFkSliceB,
-                                     B + (long long)s * kFkCols * G.ldp + st * kFkSliceB, kFkSliceB, &full[buf]);
-        }
+        lio::umma::bulk_copy_g2s(stage, A + (long long)st * kFkStepA, kFkStepA, &full[buf]);
+        for (int sp = 0; sp < NS; sp++)
+          lio::umma::bulk_copy_g2s(stage + Cfg::kStageA + sp * kFkStepB, (sp == 0 ? Ba : Bb) + (long long)st * kFkStepB,
+                                   kFkStepB, &full[buf]);
       }
     }
   } else if (warp == 5) {
     if (lane == 0) {
-      const uint32_t idesc = lio::umma::idesc_i8(kFkRows, kFkCols);
       const uint32_t smem0 = lio::umma::smem_u32(fk_smem);
       for (int st = 0; st < nsteps; st++) {
         const int buf = st % kFkStages, use = st / kFkStages;
@@ -142,19 +197,17 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
           break;
         }
         lio::umma::fence_after_sync();
-        const uint64_t ad0 = lio::umma::smem_desc(smem0 + buf * Cfg::kStage, 16u * kFkRows, 128u);
-        const uint64_t bd0 = lio::umma::smem_desc(smem0 + buf * Cfg::kStage + Cfg::kStageA, 16u * kFkCols, 128u);
-        const uint32_t keep = st > 0 ? 1u : 0u;
+        const uint32_t sa = smem0 + buf * Cfg::kStage;
 #pragma unroll
-        for (int sp = 0; sp < NS; sp++)
+        for (int sp = 0; sp < NS; sp++) {
+          // stacked B of this spin: K-major, 192 rows (LBO = 16 * 192 bytes between K halves)
+          const uint64_t bd = lio::umma::smem_desc(sa + Cfg::kStageA + sp * kFkStepB, 16u * kFkTall, 128u);
 #pragma unroll
-          for (int l = 0; l < kSlices; l++)
-#pragma unroll
-            for (int s = 0; s <= l; s++)
-              lio::umma::mma_i8(tbase + (uint32_t)((sp * kSlices + l) * kFkCols),
-                                ad0 + (uint64_t)((s * kFkSliceA) >> 4),
-                                bd0 + (uint64_t)(((sp * kSlices + l - s) * kFkSliceB) >> 4), idesc,
-                                s > 0 ? 1u : keep);
+          for (int s = 0; s < kSlices; s++)
+            lio::umma::mma_i8(tbase + (uint32_t)((sp * kSlices + s) * kFkCols),
+                              lio::umma::smem_desc(sa + s * kFkSliceA, 16u * kFkRows, 128u), bd,
+                              lio::umma::idesc_i8(kFkRows, (kSlices - s) * kFkCols), (st > 0 || s > 0) ? 1u : 0u);
+        }
         lio::umma::commit(&empty[buf]);
       }
       lio::umma::commit(&done);
