@@ -128,6 +128,9 @@ def bind(lib: G2GLibrary, wl: W.Workload):
 def workload(rank: int, name: str = "cfg3") -> W.Workload:
     if name == "cfg2":  # 64-atom closed-shell PBE, 40x302 (small case for profiling)
         return W.config(2)
+    if name == "cfg2-open":  # the same 64 atoms, open-shell PBE (small case of the open-shell kernels)
+        return W.make_workload("cfg2-open: 64 atoms 16C4N4O40H, 40x302, open PBE",
+                               {"C": 16, "N": 4, "O": 4, "H": 40}, 14.0, 2000, 9, True, 302, 40)
     if rank == 0:
         return W.config(3)
     return W.make_workload(f"cfg3-rank{rank}", {"C": 64, "N": 16, "O": 16, "H": 160}, 22.0, 3000 + 17 * rank, 9,
@@ -310,8 +313,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", type=int, default=0, help="0 = FP64 plain, 1 = tensor-core form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="cfg3", choices=["cfg3", "cfg2"],
-                    help="cfg3 = the 256-atom headline workload; cfg2 = the 64-atom case used for ncu captures")
+    ap.add_argument("--workload", default="cfg3", choices=["cfg3", "cfg2", "cfg2-open"],
+                    help="cfg3 = the 256-atom headline workload; cfg2 / cfg2-open = the 64-atom closed- and "
+                         "open-shell cases used for ncu captures")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -18,7 +18,10 @@
 // lands on level s + t: S MMAs per K step and kind instead of S(S+1)/2 narrow
 // ones (an MMA costs about the same for every N up to 64 on this part).
 //
-// The row-dot epilogue reads F, dF and d2F at (p, i) from the FP64 basis cache.
+// The row-dot epilogue needs F, dF and d2F at (p, i) in FP64. They come from a
+// blocked copy of the basis cache (per 128-point tile, 32-function tile and
+// kind one contiguous 32 KB chunk) that a dedicated warp streams into a
+// shared-memory ring with bulk copies, so the epilogue does no global loads.
 #pragma once
 #include "umma.cuh"
 
@@ -31,7 +34,8 @@ constexpr int kTcCpw = kTcFuncs / 2;         // columns per epilogue warp
 constexpr int kTcSliceA = 32 * kTcPoints;    // bytes of one A slice per 32-byte K step
 constexpr int kTcStepA = kSlices * kTcSliceA;  // one kind's A slices per K step (contiguous)
 constexpr int kTcStepD = 32 * kTcTall;         // one spin's stacked D slices per K step (contiguous)
-constexpr int kTcMaxFnCap = 512; // functions per group the ring depth leaves table room for
+constexpr int kTcChunk = kTcFuncs * kTcPoints;  // doubles of one blocked basis chunk (kind, 32 functions)
+constexpr int kTcMaxFnCap = 512; // functions per group the shared memory leaves table room for
 
 // KP = kinds per unit: all NS x KP x S x 32 level columns of a unit fit in 384
 // TMEM columns. Open shell: one kind per unit (F, x, y, z); closed shell GGA:
@@ -39,29 +43,27 @@ constexpr int kTcMaxFnCap = 512; // functions per group the ring depth leaves ta
 template <bool GGA, int NS>
 struct TcCfg {
   static constexpr int KP = (GGA && NS == 1) ? 2 : 1;
-  static constexpr int NA = GGA ? 4 : 1;  // kinds
-  static constexpr int NP = NA / KP;      // units per function tile
+  static constexpr int NA = GGA ? 4 : 1;   // kinds of the contraction
+  static constexpr int NK = GGA ? 10 : 1;  // kinds of the FP64 basis (F; dF; d2F)
+  static constexpr int NP = NA / KP;       // units per function tile
   static constexpr int NQ = GGA ? 10 : 1;
   static constexpr int kStageA = KP * kTcStepA;
   static constexpr int kStage = kStageA + NS * kTcStepD;
   static constexpr uint32_t kCols = NS * KP * kSlices * kTcFuncs;
   static constexpr uint32_t kTmem = kCols <= 256 ? 256 : 512;
-  static constexpr int kWarps = kTcEpiWarps + 2;  // epilogue warps, producer, MMA issuer
+  // epilogue warps, operand producer, MMA issuer, basis producer
+  static constexpr int kWarps = kTcEpiWarps + 3;
   static constexpr int kThreads = 32 * kWarps;
-  // dynamic shared memory: ring | staged G values | column-group reduction | function table
-  static constexpr size_t kGvWarp = (size_t)NS * KP * kTcCpw * 32 * 8;  // [spin][kind][column][lane] FP64
-  static constexpr size_t kGvBytes = kTcEpiWarps * kGvWarp;
-  static constexpr size_t kRedBytes = (size_t)NS * kTcPoints * NQ * 8;  // [spin][point][NQ] FP64
-  static constexpr size_t kTabEntry = NS * 8;                           // 2^f_i per spin
-  // ring depth: as many stages (up to 4) as fit beside the rest and a full table
-  static constexpr size_t kBudget = 232448 - 1024 - (size_t)kTcMaxFnCap * kTabEntry;
-  static constexpr int kStages =
-      (int)((kBudget - kGvBytes - kRedBytes) / kStage < 4 ? (kBudget - kGvBytes - kRedBytes) / kStage : 4);
-  static_assert(kStages >= 2, "ring too shallow");
+  static constexpr int kProd = kTcEpiWarps, kMma = kTcEpiWarps + 1, kBasisProd = kTcEpiWarps + 2;
+  // dynamic shared memory: operand ring | basis ring | column-group reduction | function table
+  static constexpr int kStages = 2;
+  static constexpr int kBStages = 3;
   static constexpr size_t kRing = (size_t)kStages * kStage;
-  static constexpr size_t kGv = kRing;
-  static constexpr size_t kRed = kGv + kGvBytes;
+  static constexpr size_t kBRing = kRing;
+  static constexpr size_t kRed = kBRing + (size_t)kBStages * kTcChunk * 8;
+  static constexpr size_t kRedBytes = (size_t)NS * kTcPoints * NQ * 8;  // [spin][point][NQ] FP64
   static constexpr size_t kTab = kRed + kRedBytes;
+  static constexpr size_t kTabEntry = NS * 8;  // 2^f_i per spin
   static size_t smem(int cap) { return kTab + (size_t)cap * kTabEntry; }
 };
 
@@ -71,6 +73,18 @@ __device__ __forceinline__ int slice_exponent(double amax) { return amax > 0.0 ?
 // exact 2^k as a double (k within the normal range), else ldexp
 __device__ __forceinline__ double pow2(int k) {
   return (k > -1022 && k < 1024) ? __longlong_as_double((long long)(k + 1023) << 52) : ldexp(1.0, k);
+}
+
+// Next base-128 digit of x (|x| <= 1/2): returns rint(128 x) as an integer and
+// leaves the remainder 128 x - rint(128 x) (|.| <= 1/2) in x, all exactly. The
+// rounding is done by the FP64 adder: 128 x + 1.5 * 2^52 rounds to the nearest
+// integer (ties to even, as rint), whose value sits in the low mantissa bits.
+__device__ __forceinline__ int8_t next_digit(double& x) {
+  constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52
+  const double t = fma(x, 128.0, kRound);
+  const double d = t - kRound;
+  x = fma(x, 128.0, -d);
+  return (int8_t)__double2loint(t);
 }
 
 // ---------------------------------------------------------------- A slices
@@ -99,12 +113,7 @@ __global__ void k_slice_basis(const int2* __restrict__ tiles, const GroupDev* __
     for (int j = 0; j < G.m32; j++) {
       double x = j < G.m ? ldexp(src[(long long)j * G.ldp], -e) : 0.0;
       int8_t* blk = dst + (j >> 5) * kTcStepA + lio::umma::kmajor_offset(r, j & 31, kTcPoints);
-      for (int s = 0; s < kSlices; s++) {
-        x *= 128.0;
-        const double d = rint(x);
-        x -= d;
-        blk[s * kTcSliceA] = (int8_t)d;
-      }
+      for (int s = 0; s < kSlices; s++) blk[s * kTcSliceA] = next_digit(x);
     }
   }
 }
@@ -145,12 +154,28 @@ __global__ void k_slice_density(const int2* __restrict__ tiles, const GroupDev* 
       x = ldexp(v, -e);
     }
     int8_t* blk = dst + (j >> 5) * kTcStepD;
-    for (int s = 0; s < kSlices; s++) {
-      x *= 128.0;
-      const double d = rint(x);
-      x -= d;
-      blk[lio::umma::kmajor_offset(s * kTcFuncs + r, j & 31, kTcTall)] = (int8_t)d;
-    }
+    for (int s = 0; s < kSlices; s++) blk[lio::umma::kmajor_offset(s * kTcFuncs + r, j & 31, kTcTall)] = next_digit(x);
+  }
+}
+
+// ------------------------------------------------- blocked FP64 basis
+// Per geometry: the basis cache rearranged for the density epilogue: per group,
+// 128-point tile T, 32-function tile ft and kind k one contiguous chunk
+// [function i - 32 ft][point p - 128 T] (kTcChunk doubles) at
+// bb_off + ((T * nftc + ft) * NK + k) * kTcChunk; functions at or beyond m
+// are zeros. One CTA (128 threads = points) per (tile, ft * NK + k).
+__global__ void k_basis_block(const int2* __restrict__ tiles, const GroupDev* __restrict__ groups, int NK,
+                              const double* __restrict__ basis, double* __restrict__ bblk) {
+  const int2 t = tiles[blockIdx.x];
+  const GroupDev& G = groups[t.x];
+  const int ft = blockIdx.y / NK, k = blockIdx.y - ft * NK;
+  if (ft >= G.nftc) return;
+  const int p = t.y * kTcPoints + threadIdx.x;
+  const double* src = basis + G.bas_off + (long long)k * G.m * G.ldp + p;
+  double* dst = bblk + G.bb_off + ((long long)(t.y * G.nftc + ft) * NK + k) * kTcChunk + threadIdx.x;
+  for (int c = 0; c < kTcFuncs; c++) {
+    const int i = ft * kTcFuncs + c;
+    dst[c * kTcPoints] = i < G.m ? src[(long long)i * G.ldp] : 0.0;
   }
 }
 
@@ -162,7 +187,8 @@ constexpr int kTcNarrowK = 768;
 // sum_l acc_l 128^(S-1-l) of column c in FP64: level pairs in int32 (narrow)
 // or each level converted (wide), then combined with one rounding, 2^-53 of
 // the leading term and far below the dropped slice pairs
-__device__ __forceinline__ double level_sum(const int32_t (&lv)[kSlices][8], int c, bool narrow) {
+template <int W>
+__device__ __forceinline__ double level_sum(const int32_t (&lv)[kSlices][W], int c, bool narrow) {
   double v0, v1, v2;
   if (narrow) {
     v0 = (double)(lv[0][c] * 128 + lv[1][c]);
@@ -175,6 +201,7 @@ __device__ __forceinline__ double level_sum(const int32_t (&lv)[kSlices][8], int
   }
   return fma(fma(v0, 16384.0, v1), 16384.0, v2);
 }
+
 // named barrier over the epilogue warps only; returns the OR of `pred` over them
 __device__ __forceinline__ bool epi_sync_or(bool pred) {
   uint32_t out;
@@ -189,134 +216,93 @@ __device__ __forceinline__ bool epi_sync_or(bool pred) {
   return out != 0;
 }
 
-// Row dots of one unit for one epilogue warp: its 16 columns i = cb .. cb+15
-// (G values staged in gv[(sp * KP + kp) * 16 + c][lane], scales 2^f_i in
-// ts[sp][i], zero beyond m) against the FP64 basis values of the point at
-// bas[k * ks + i * ldp], accumulated into q = (rho; grad rho; d2rho xx, yy, zz,
-// xy, xz, yz) per spin:
-//   kind F : rho += F G, grad += 2 dF G, d2 += 2 d2F G
-//   kind x : xx += 2 Fx Gx, xy += 2 Fy Gx, xz += 2 Fz Gx   (Fy Gx = Fx Gy: D is symmetric)
-//   kind y : yy += 2 Fy Gy, yz += 2 Fz Gy
-//   kind z : zz += 2 Fz Gz
-// All loads of a column chunk are issued before any is used, so a warp keeps
-// 16 to 48 loads in flight. Columns at or beyond m read column m-1 (their G
-// and scale are zero).
+// FP64 basis kinds whose chunks a unit with first contraction kind `first`
+// consumes, in order: F unit: all NK; x: dF/dx..dF/dz; y: dF/dy, dF/dz; z: dF/dz.
+__host__ __device__ __forceinline__ int unit_klo(int first) { return first == 0 ? 0 : first; }
+__host__ __device__ __forceinline__ int unit_khi(int first, int NK) { return first == 0 ? NK - 1 : 3; }
+
+// Adds the row dots of basis-kind chunk k, d[sp][kp] = sum_i v_ki G^(kp)_i over
+// this warp's columns, to the point's q = (rho; grad rho; d2rho xx, yy, zz, xy,
+// xz, yz) per spin:
+//   unit F : k = F: rho += d;  k = dF_a: grad_a += 2 d;  k = d2F_ab: d2_ab += 2 d
+//            with KP = 2 also G^x: xx += 2 d(Fx), xy += 2 d(Fy), xz += 2 d(Fz)
+//   unit x : xx += 2 d(Fx), xy += 2 d(Fy), xz += 2 d(Fz)   (Fy Gx = Fx Gy: D is symmetric)
+//   unit y : yy += 2 d(Fy), yz += 2 d(Fz)   (with KP = 2 also zz += 2 d(Fz) of G^z)
+//   unit z : zz += 2 d(Fz)
 template <bool GGA, int NS, int NQ, int KP>
-__device__ __forceinline__ void unit_row_dots(int first, const double* bas, long long ks, int ldp, int cb, int m,
-                                              const double* gv, const double* tsa, const double* tsb, int lane,
-                                              double (&q)[NS][NQ]) {
-  constexpr int C = kTcCpw;
-  auto col = [&](int c) { return (long long)(cb + c < m ? cb + c : m - 1) * ldp; };
-  auto gval = [&](int sp, int kp, int c) {
-    return gv[((sp * KP + kp) * C + c) * 32 + lane] * (sp == 0 ? tsa[cb + c] : tsb[cb + c]);
-  };
-  if (!GGA) {
-    double F[C];
+__device__ __forceinline__ void apply_chunk(int first, int k, const double (&d)[NS][KP], double (&q)[NS][NQ]) {
 #pragma unroll
-    for (int c = 0; c < C; c++) F[c] = bas[col(c)];
-#pragma unroll
-    for (int c = 0; c < C; c++)
-#pragma unroll
-      for (int sp = 0; sp < NS; sp++) q[sp][0] += F[c] * gval(sp, 0, c);
-    return;
-  }
-  if (first == 0) {  // F (and x when KP == 2), four columns at a time
-#pragma unroll
-    for (int c0 = 0; c0 < C; c0 += 4) {
-      double v[4][10];
-#pragma unroll
-      for (int c = 0; c < 4; c++)
-#pragma unroll
-        for (int k = 0; k < 10; k++) v[c][k] = bas[k * ks + col(c0 + c)];
-#pragma unroll
-      for (int c = 0; c < 4; c++)
-#pragma unroll
-        for (int sp = 0; sp < NS; sp++) {
-          const double g0 = gval(sp, 0, c0 + c), g2 = 2.0 * g0;
-          q[sp][0] += v[c][0] * g0;
-#pragma unroll
-          for (int k = 1; k < 10; k++) q[sp][k % NQ] += v[c][k] * g2;
-          if (KP == 2) {
-            const double gx2 = 2.0 * gval(sp, 1, c0 + c);
-            q[sp][4 % NQ] += v[c][1] * gx2;
-            q[sp][7 % NQ] += v[c][2] * gx2;
-            q[sp][8 % NQ] += v[c][3] * gx2;
-          }
-        }
+  for (int sp = 0; sp < NS; sp++) {
+    if (!GGA) {
+      q[sp][0] += d[sp][0];
+      continue;
     }
-  } else if (first == 1) {  // x alone (KP == 1)
-    double v[C][3];
-#pragma unroll
-    for (int c = 0; c < C; c++)
-#pragma unroll
-      for (int k = 0; k < 3; k++) v[c][k] = bas[(1 + k) * ks + col(c)];
-#pragma unroll
-    for (int c = 0; c < C; c++)
-#pragma unroll
-      for (int sp = 0; sp < NS; sp++) {
-        const double g2 = 2.0 * gval(sp, 0, c);
-        q[sp][4 % NQ] += v[c][0] * g2;
-        q[sp][7 % NQ] += v[c][1] * g2;
-        q[sp][8 % NQ] += v[c][2] * g2;
+    const double d0 = 2.0 * d[sp][0], d1 = 2.0 * d[sp][KP - 1];
+    if (first == 0) {
+      // kinds F, dF/dx, dF/dy, dF/dz, d2F xx .. yz map onto q[0 .. 9] in order
+      switch (k) {
+        case 0: q[sp][0] += d[sp][0]; break;
+        case 1: q[sp][1 % NQ] += d0; if (KP == 2) q[sp][4 % NQ] += d1; break;
+        case 2: q[sp][2 % NQ] += d0; if (KP == 2) q[sp][7 % NQ] += d1; break;
+        case 3: q[sp][3 % NQ] += d0; if (KP == 2) q[sp][8 % NQ] += d1; break;
+        case 4: q[sp][4 % NQ] += d0; break;
+        case 5: q[sp][5 % NQ] += d0; break;
+        case 6: q[sp][6 % NQ] += d0; break;
+        case 7: q[sp][7 % NQ] += d0; break;
+        case 8: q[sp][8 % NQ] += d0; break;
+        default: q[sp][9 % NQ] += d0; break;
       }
-  } else if (first == 2) {  // y (and z when KP == 2)
-    double v[C][2];
-#pragma unroll
-    for (int c = 0; c < C; c++)
-#pragma unroll
-      for (int k = 0; k < 2; k++) v[c][k] = bas[(2 + k) * ks + col(c)];
-#pragma unroll
-    for (int c = 0; c < C; c++)
-#pragma unroll
-      for (int sp = 0; sp < NS; sp++) {
-        const double g2 = 2.0 * gval(sp, 0, c);
-        q[sp][5 % NQ] += v[c][0] * g2;
-        q[sp][9 % NQ] += v[c][1] * g2;
-        if (KP == 2) q[sp][6 % NQ] += v[c][1] * (2.0 * gval(sp, 1, c));
+    } else if (first == 1) {
+      if (k == 1) q[sp][4 % NQ] += d0;
+      else if (k == 2) q[sp][7 % NQ] += d0;
+      else q[sp][8 % NQ] += d0;
+    } else if (first == 2) {
+      if (k == 2) {
+        q[sp][5 % NQ] += d0;
+      } else {
+        q[sp][9 % NQ] += d0;
+        if (KP == 2) q[sp][6 % NQ] += d1;
       }
-  } else {  // z alone (KP == 1)
-    double v[C];
-#pragma unroll
-    for (int c = 0; c < C; c++) v[c] = bas[3 * ks + col(c)];
-#pragma unroll
-    for (int c = 0; c < C; c++)
-#pragma unroll
-      for (int sp = 0; sp < NS; sp++) q[sp][6 % NQ] += v[c] * (2.0 * gval(sp, 0, c));
+    } else {
+      q[sp][6 % NQ] += d0;
+    }
   }
 }
 
 // CTA = one per SM, persistent over the 128-point tiles (all groups, largest
 // function count first, tile w handled by CTA w mod gridDim.x); both spins
-// (NS = 2) or one. A unit is (tile, 32-function tile, KP kinds). Warp roles:
+// (NS = 2) or one. A unit is (tile, 32-function tile, KP contraction kinds).
+// Warp roles:
 //   warps 0..7  epilogue: TMEM lane quadrant warp % 4 (one lane = one point),
 //               columns 16 * (warp / 4) .. of the function tile;
-//   warp 8      producer: per (unit, 32-function K step) one stage with the
-//               unit's A slices (KP x kTcStepA) and every spin's stacked D
-//               slices (kTcStepD), one bulk copy each, into a four-stage ring;
+//   warp 8      operand producer: per (unit, 32-function K step) one stage with
+//               the unit's A slices (KP x kTcStepA) and every spin's stacked D
+//               slices (kTcStepD), one bulk copy each;
 //   warp 9      MMA issuer: per stage NS x KP x S MMAs into the unit's
-//               NS x KP x S x 32 level columns in TMEM.
-// The A slices are shared by both spins. The epilogue stages the unit's G
-// values (FP64) in shared memory and hands TMEM back (tempty) before its
-// row-dot work, so the next unit's MMAs overlap it. The ring, unit and tile
-// sequences run on across tiles, so one tile's loads and MMAs overlap the
-// previous tile's epilogue. Every wait is bounded; a timeout sets `fail`,
-// which the other roles poll, and the kernel drains its copies and MMAs
-// before it frees TMEM and reports the error.
+//               NS x KP x S x 32 level columns in TMEM;
+//   warp 10     basis producer: per unit the FP64 basis chunks its row dots
+//               need (unit_klo .. unit_khi), one 32 KB bulk copy each, into a
+//               three-slot ring.
+// The epilogue reads the unit's levels (tfull), forms G in FP64 in registers,
+// hands TMEM back (tempty) so the next unit's MMAs overlap its row dots, and
+// consumes the basis chunks from shared memory. Every wait is bounded; a
+// timeout sets `fail`, which the other roles poll, and the kernel drains its
+// copies and MMAs before it frees TMEM and reports the error.
 template <bool GGA, int NS>
 __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
     k_density_tc(const int2* __restrict__ tiles, int ntiles, const GroupDev* __restrict__ groups,
                  const int8_t* __restrict__ aslices, const int16_t* __restrict__ aexp,
                  const int8_t* __restrict__ dsl_a, const int16_t* __restrict__ dexp_a,
                  const int8_t* __restrict__ dsl_b, const int16_t* __restrict__ dexp_b,
-                 const double* __restrict__ basis, int fcap, double* __restrict__ part_a,
+                 const double* __restrict__ bblk, int fcap, double* __restrict__ part_a,
                  double* __restrict__ part_b, int* __restrict__ err) {
   using Cfg = TcCfg<GGA, NS>;
-  constexpr int KP = Cfg::KP, NP = Cfg::NP, NA = Cfg::NA, NQ = Cfg::NQ, CPW = kTcCpw;
-  constexpr int kStages = Cfg::kStages;
+  constexpr int KP = Cfg::KP, NP = Cfg::NP, NA = Cfg::NA, NK = Cfg::NK, NQ = Cfg::NQ, CPW = kTcCpw;
+  constexpr int kStages = Cfg::kStages, kBStages = Cfg::kBStages;
   extern __shared__ __align__(128) uint8_t tc_smem[];
-  __shared__ uint64_t full[kStages], empty[kStages], tfull, tempty, drain;
+  __shared__ uint64_t full[kStages], empty[kStages], bfull[kBStages], bempty[kBStages], tfull, tempty, drain;
   __shared__ uint32_t tmem_base;
-  __shared__ int fail, consumed;
+  __shared__ int fail, consumed, bconsumed;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (warp == 0) lio::umma::tmem_alloc(&tmem_base, Cfg::kTmem);
   if (tid == 0) {
@@ -324,28 +310,33 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
       lio::umma::mbar_init(&full[b], 1);
       lio::umma::mbar_init(&empty[b], 1);
     }
+    for (int b = 0; b < kBStages; b++) {
+      lio::umma::mbar_init(&bfull[b], 1);
+      lio::umma::mbar_init(&bempty[b], kTcEpiWarps);
+    }
     lio::umma::mbar_init(&tfull, 1);
     lio::umma::mbar_init(&tempty, kTcEpiWarps);
     lio::umma::mbar_init(&drain, 1);
     lio::umma::fence_mbar_init();
     fail = 0;
     consumed = 0;
+    bconsumed = 0;
   }
   lio::umma::fence_before_sync();
   __syncthreads();
   lio::umma::fence_after_sync();
   const uint32_t tbase = tmem_base;
   volatile int* vfail = &fail;
-  int issued = 0;  // producer: stages issued
+  int issued = 0;  // producers: stages / chunks issued
 
-  if (warp == kTcEpiWarps) {
-    // ------------------------------------------------------------ producer
+  if (warp == Cfg::kProd) {
+    // ------------------------------------------------------------ operand producer
     if (lane == 0) {
       int cnt = 0;
       for (int w = blockIdx.x; w < ntiles && !*vfail; w += gridDim.x) {
         const int2 t = tiles[w];
         const GroupDev& G = groups[t.x];
-        const int nks = G.m32 / 32, nft = (G.m + kTcFuncs - 1) / kTcFuncs;
+        const int nks = G.m32 / 32, nft = G.nftc;
         const int8_t* Abase = aslices + G.sl_off + (long long)t.y * NA * nks * kTcStepA;
         for (int tt = 0; tt < nft * NP && !*vfail; tt++) {
           const int ft = tt / NP, pass = tt - ft * NP;
@@ -370,7 +361,32 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
         }
       }
     }
-  } else if (warp == kTcEpiWarps + 1) {
+  } else if (warp == Cfg::kBasisProd) {
+    // ------------------------------------------------------------ basis producer
+    if (lane == 0) {
+      int cnt = 0;
+      for (int w = blockIdx.x; w < ntiles && !*vfail; w += gridDim.x) {
+        const int2 t = tiles[w];
+        const GroupDev& G = groups[t.x];
+        const int nft = G.nftc;
+        for (int tt = 0; tt < nft * NP && !*vfail; tt++) {
+          const int ft = tt / NP, first = (tt - ft * NP) * KP;
+          const double* src = bblk + G.bb_off + (long long)(t.y * nft + ft) * NK * kTcChunk;
+          for (int k = unit_klo(first); k <= unit_khi(first, NK); k++, cnt++) {
+            const int buf = cnt % kBStages, use = cnt / kBStages;
+            if (use > 0 && (*vfail || !lio::umma::mbar_wait(&bempty[buf], (use - 1) & 1))) {
+              *vfail = 1;
+              break;
+            }
+            lio::umma::mbar_expect_tx(&bfull[buf], (uint32_t)(kTcChunk * 8));
+            lio::umma::bulk_copy_g2s(tc_smem + Cfg::kBRing + (size_t)buf * kTcChunk * 8,
+                                     src + (long long)k * kTcChunk, kTcChunk * 8, &bfull[buf]);
+            issued = cnt + 1;
+          }
+        }
+      }
+    }
+  } else if (warp == Cfg::kMma) {
     // ------------------------------------------------------------ MMA issuer
     if (lane == 0) {
       const uint32_t smem0 = lio::umma::smem_u32(tc_smem);
@@ -379,7 +395,7 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
       for (int w = blockIdx.x; w < ntiles && !stop; w += gridDim.x) {
         const int2 t = tiles[w];
         const GroupDev& G = groups[t.x];
-        const int nks = G.m32 / 32, nft = (G.m + kTcFuncs - 1) / kTcFuncs;
+        const int nks = G.m32 / 32, nft = G.nftc;
         for (int tt = 0; tt < nft * NP && !stop; tt++, ucnt++) {
           if (ucnt > 0) {
             if (*vfail || !lio::umma::mbar_wait(&tempty, (ucnt - 1) & 1)) {
@@ -426,17 +442,16 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
     const int row = quad * 32 + lane;
     const int etid = tid;  // 0 .. 255
     const uint32_t lane_base = tbase + ((uint32_t)(quad * 32) << 16);
-    double* gvw = reinterpret_cast<double*>(tc_smem + Cfg::kGv + (size_t)warp * Cfg::kGvWarp);
+    const double* bring = reinterpret_cast<const double*>(tc_smem + Cfg::kBRing);
     double* red = reinterpret_cast<double*>(tc_smem + Cfg::kRed);
     double* tsa = reinterpret_cast<double*>(tc_smem + Cfg::kTab);  // 2^f_i, spin a
     double* tsb = tsa + fcap;                                        // spin b (NS = 2 only)
     bool lfail = false;
-    int ucnt = 0;
+    int ucnt = 0, bcnt = 0;
     for (int w = blockIdx.x; w < ntiles; w += gridDim.x) {
       const int2 t = tiles[w];
       const GroupDev& G = groups[t.x];
-      const int m = G.m, ldp = G.ldp;
-      const int nft = (m + kTcFuncs - 1) / kTcFuncs, ntt = nft * NP;
+      const int m = G.m, ldp = G.ldp, nft = G.nftc, ntt = nft * NP;
       const int p = t.y * kTcPoints + row;
       // per-function scales of this group (the previous tile's readers are past the last barrier)
       const int mt = nft * kTcFuncs;  // <= fcap: fcap covers the largest padded m
@@ -448,52 +463,83 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
       double spx[NA];  // 2^(point exponent - 7(S+1)) per kind
 #pragma unroll
       for (int a = 0; a < NA; a++) spx[a] = pow2(aexp[G.aexp_off + (long long)a * ldp + p] - 7 * (kSlices + 1));
-      // FP64 basis values of this point: kind k of function i at bas[k * ks + i * ldp]
-      // (F; dF/dx, dF/dy, dF/dz; d2F xx, yy, zz, xy, xz, yz)
-      const double* bas = basis + G.bas_off + p;
-      const long long ks = (long long)m * ldp;
       double q[NS][NQ];
 #pragma unroll
       for (int sp = 0; sp < NS; sp++)
 #pragma unroll
         for (int k = 0; k < NQ; k++) q[sp][k] = 0.0;
+      const bool narrow = G.m32 <= kTcNarrowK;
       for (int tt = 0; tt < ntt; tt++, ucnt++) {
-        const int ft = tt / NP, pass = tt - ft * NP;
+        const int ft = tt / NP, pass = tt - ft * NP, first = pass * KP;
         const int cb = ft * kTcFuncs + colg * CPW;  // first function of this warp's columns
-        const bool narrow = G.m32 <= kTcNarrowK;
+        // ---- the unit's accumulators -> G (FP64, scaled by 2^(e_p + f_i - 7(S+1))) in registers
         bool ok = !lfail && !*vfail && lio::umma::mbar_wait(&tfull, ucnt & 1);
         ok = __all_sync(0xffffffffu, ok);
-        if (!ok) {
-          lfail = true;
-          *vfail = 1;
-        }
         lio::umma::fence_after_sync();
+        double g[CPW][NS][KP];
         if (ok) {
 #pragma unroll
           for (int sp = 0; sp < NS; sp++)
 #pragma unroll
-            for (int kp = 0; kp < KP; kp++) {
-              const double sa = spx[pass * KP + kp];
+            for (int kp = 0; kp < KP; kp++)
 #pragma unroll
-              for (int c8 = 0; c8 < CPW / 8; c8++) {
+              for (int h = 0; h < CPW / 8; h++) {
                 int32_t lv[kSlices][8];
 #pragma unroll
                 for (int l = 0; l < kSlices; l++)
                   lio::umma::tmem_ld8(
-                      lane_base + (uint32_t)(((sp * KP + kp) * kSlices + l) * kTcFuncs + colg * CPW + c8 * 8), lv[l]);
+                      lane_base + (uint32_t)(((sp * KP + kp) * kSlices + l) * kTcFuncs + colg * CPW + h * 8), lv[l]);
                 lio::umma::tmem_wait_ld();
+                const double sa = spx[first + kp];
 #pragma unroll
                 for (int c = 0; c < 8; c++)
-                  gvw[((sp * KP + kp) * CPW + c8 * 8 + c) * 32 + lane] = level_sum(lv, c, narrow) * sa;
+                  g[h * 8 + c][sp][kp] =
+                      level_sum(lv, c, narrow) * sa * (sp == 0 ? tsa[cb + h * 8 + c] : tsb[cb + h * 8 + c]);
               }
-            }
+        } else {
+          lfail = true;
+          *vfail = 1;
         }
         // accumulators read: hand TMEM back to the MMA issuer
         lio::umma::fence_before_sync();
         __syncwarp();
         if (lane == 0 && ok) lio::umma::mbar_arrive(&tempty);
-        unit_row_dots<GGA, NS, NQ, KP>(pass * KP, bas, ks, ldp, cb, m, gvw, tsa, tsb, lane, q);
-        __syncwarp();  // every lane done with this unit's staged values
+        // ---- row dots against the unit's basis chunks
+        const int klo = unit_klo(first), khi = unit_khi(first, NK);
+        for (int k = klo; k <= khi; k++, bcnt++) {
+          const int buf = bcnt % kBStages, use = bcnt / kBStages;
+          bool okb = !lfail && !*vfail && lio::umma::mbar_wait(&bfull[buf], use & 1);
+          okb = __all_sync(0xffffffffu, okb);
+          if (!okb) {
+            lfail = true;
+            *vfail = 1;
+          } else {
+            const double* ch = bring + (size_t)buf * kTcChunk + (colg * CPW) * kTcPoints + row;
+            double d4[4][NS][KP];
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+#pragma unroll
+              for (int sp = 0; sp < NS; sp++)
+#pragma unroll
+                for (int kp = 0; kp < KP; kp++) d4[c][sp][kp] = ch[c * kTcPoints] * g[c][sp][kp];
+#pragma unroll
+            for (int c = 4; c < CPW; c++) {
+              const double v = ch[c * kTcPoints];
+#pragma unroll
+              for (int sp = 0; sp < NS; sp++)
+#pragma unroll
+                for (int kp = 0; kp < KP; kp++) d4[c & 3][sp][kp] = fma(v, g[c][sp][kp], d4[c & 3][sp][kp]);
+            }
+            double d[NS][KP];
+#pragma unroll
+            for (int sp = 0; sp < NS; sp++)
+#pragma unroll
+              for (int kp = 0; kp < KP; kp++) d[sp][kp] = (d4[0][sp][kp] + d4[1][sp][kp]) + (d4[2][sp][kp] + d4[3][sp][kp]);
+            apply_chunk<GGA, NS, NQ, KP>(first, k, d, q);
+          }
+          __syncwarp();
+          if (lane == 0 && okb) lio::umma::mbar_arrive(&bempty[buf]);
+        }
       }
       // tile done: column group 1 hands its sums to column group 0, which writes them
       if (colg == 1) {
@@ -514,12 +560,15 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
       }
       epi_sync_or(false);  // the table and the reduction area are free again
     }
+    if (etid == 0) bconsumed = bcnt;
   }
   __syncthreads();  // every role done
-  if (warp == kTcEpiWarps && lane == 0) {
+  if ((warp == Cfg::kProd || warp == Cfg::kBasisProd) && lane == 0) {
     // copies issued but never consumed (after a timeout) land before the CTA exits
-    for (int k = consumed; k < issued; k++)
-      if (!lio::umma::mbar_wait(&full[k % kStages], (k / kStages) & 1)) break;
+    const bool basis = warp == Cfg::kBasisProd;
+    const int nb = basis ? kBStages : kStages;
+    for (int k = basis ? bconsumed : consumed; k < issued; k++)
+      if (!lio::umma::mbar_wait(basis ? &bfull[k % nb] : &full[k % nb], (k / nb) & 1)) break;
   }
   lio::umma::fence_before_sync();
   __syncthreads();

@@ -61,7 +61,7 @@ struct GroupDev {
   long long sf_off;    // sf_glob / sf_type
   long long bas_off;   // basis cache (elements)
   long long part_off;  // partial densities (elements, one spin)
-  long long rad_off;   // radial cache (elements): 3 x nsimple x ldp
+  long long bb_off;    // blocked FP64 basis of the tensor-core density (elements)
   long long sl_off;    // int8 slices of the density A operands (bytes)
   long long aexp_off;  // their per-point exponents (elements): NA x ldp
   long long ds_off;    // int8 slices of the density matrix (bytes, one spin)
@@ -448,43 +448,6 @@ __global__ void __launch_bounds__(256) k_fock_fp64(const int4* __restrict__ tile
   }
 }
 
-// radial parts (t, tg, th) of every simple function at every point (per
-// geometry), the input of the tensor-core epilogue's basis rebuild
-__global__ void k_radial(const int2* __restrict__ tiles, const GroupDev* __restrict__ groups,
-                         const double* __restrict__ px, const double* __restrict__ py, const double* __restrict__ pz,
-                         const int* __restrict__ sf_glob, const int* __restrict__ nuc, const int* __restrict__ ncont,
-                         const double* __restrict__ ca, const double* __restrict__ cc, const double* __restrict__ ax,
-                         const double* __restrict__ ay, const double* __restrict__ az, double* __restrict__ radial) {
-  const int2 t = tiles[blockIdx.x];
-  const GroupDev G = groups[t.x];
-  const int p = t.y * kBasisBlock + threadIdx.x;
-  if (p >= G.ldp) return;
-  const bool valid = p < G.npts;
-  const double x = px[G.pt_off + p], y = py[G.pt_off + p], z = pz[G.pt_off + p];
-  const long long rs = (long long)G.nsimple * G.ldp;
-  double* out = radial + G.rad_off;
-  for (int sf = 0; sf < G.nsimple; sf++) {
-    const int gf = sf_glob[G.sf_off + sf];
-    const int atom = nuc[gf];
-    const double dx = x - ax[atom], dy = y - ay[atom], dz = z - az[atom];
-    const double dist = dx * dx + dy * dy + dz * dz;
-    double tt = 0.0, tg = 0.0, th = 0.0;
-    for (int k = 0; k < ncont[gf]; k++) {
-      const double a = ca[gf * 13 + k], c = cc[gf * 13 + k];
-      const double expo = a * dist;
-      if (expo > 70.0) continue;
-      const double t0 = exp(-expo) * c;
-      tt += t0;
-      tg += t0 * a;
-      th += t0 * (a * a);
-    }
-    const long long o = (long long)sf * G.ldp + p;
-    out[o] = valid ? tt : 0.0;
-    out[rs + o] = valid ? tg : 0.0;
-    out[2 * rs + o] = valid ? th : 0.0;
-  }
-}
-
 #include "density_tc.cuh"
 #include "fock_tc.cuh"
 
@@ -507,7 +470,8 @@ struct DeviceEngine::Impl {
   DevBuf<int2> dens_tc_tiles;  // (group, 128-point tile), largest function count first
   int tc_fcap = 0, nsm = 148;
 
-  DevBuf<double> radial;
+  DevBuf<double> bblk;  // blocked FP64 basis (tensor-core density epilogue)
+  int max_nftc = 0;
   DevBuf<int8_t> aslices, dslices_a, dslices_b;
   DevBuf<int16_t> aexp, dexp_a, dexp_b;
   DevBuf<int> tc_err;
@@ -613,6 +577,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
   d->open = sys.open;
   d->iexch = sys.iexch;
   d->nk = sys.lda ? 1 : 10;
+  d->max_nftc = 0;
   d->d_norm = sys.d_norm;
   const int NQ = sys.lda ? 1 : kNQ;
 
@@ -623,7 +588,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
   std::vector<int2> btiles, ftiles, sbtiles, sdtiles;
   std::vector<int4> dtiles, ktiles, tctiles;
   long long pt_off = 0, fn_off = 0, sf_off = 0, bas_off = 0, part_off = 0;
-  long long rad_off = 0, sl_off = 0, aexp_off = 0, ds_off = 0, dexp_off = 0;
+  long long bb_off = 0, sl_off = 0, aexp_off = 0, ds_off = 0, dexp_off = 0;
   long long fa_off = 0, fae_off = 0, fb_off = 0, fbe_off = 0;
   std::vector<int2> farows, fbrows, fat32, fbt32;
   std::vector<int4> fktiles;
@@ -646,7 +611,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
     G.sf_off = sf_off;
     G.bas_off = bas_off;
     G.part_off = part_off;
-    G.rad_off = rad_off;
+    G.bb_off = bb_off;
     G.sl_off = sl_off;
     G.aexp_off = aexp_off;
     G.ds_off = ds_off;
@@ -706,7 +671,8 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
     sf_off += G.nsimple;
     bas_off += (long long)d->nk * G.m * G.ldp;
     part_off += (long long)G.nft * NQ * G.ldp;
-    rad_off += 3LL * G.nsimple * G.ldp;
+    bb_off += (long long)(G.ldp / kTcPoints) * G.nftc * d->nk * kTcChunk;
+    d->max_nftc = std::max(d->max_nftc, G.nftc);
     sl_off += (long long)(G.ldp / kTcPoints) * NA * (G.m32 / 32) * kTcStepA;
     aexp_off += (long long)NA * G.ldp;
     ds_off += (long long)G.nftc * (G.m32 / 32) * kTcStepD;
@@ -718,7 +684,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
     npts_total += G.npts;
     gd.push_back(G);
   }
-  d->tc_sizes[0] = rad_off;
+  d->tc_sizes[0] = bb_off;
   d->tc_sizes[1] = sl_off;
   d->tc_sizes[2] = aexp_off;
   d->tc_sizes[3] = ds_off;
@@ -807,12 +773,13 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
   LIO_CUDA(cudaStreamSynchronize(d->stream));
 }
 
-// Builds the tensor-core operands of the current geometry: radial cache and
-// int8 slices of the density A operands (F, and for GGA its gradient).
+// Builds the tensor-core operands of the current geometry: the blocked FP64
+// basis and the int8 slices of the density A operands (F, and for GGA its
+// gradient) and of the Kohn-Sham A operand (F).
 void DeviceEngine::prepare_tensor_core() {
   Impl* d = impl_.get();
   cudaStream_t st = d->stream;
-  d->radial.alloc(d->tc_sizes[0]);
+  d->bblk.alloc(d->tc_sizes[0]);
   d->aslices.alloc(d->tc_sizes[1]);
   d->aexp.alloc(d->tc_sizes[2]);
   d->dslices_a.alloc(d->tc_sizes[3]);
@@ -823,10 +790,11 @@ void DeviceEngine::prepare_tensor_core() {
   }
   d->tc_err.alloc(1);
   LIO_CUDA(cudaMemsetAsync(d->tc_err.p, 0, sizeof(int), st));
-  k_radial<<<(unsigned)d->basis_tiles.n, kBasisBlock, 0, st>>>(d->basis_tiles.p, d->groups.p, d->px.p, d->py.p,
-                                                               d->pz.p, d->sf_glob.p, d->nuc.p, d->ncont.p, d->ca.p,
-                                                               d->cc.p, d->ax.p, d->ay.p, d->az.p, d->radial.p);
-  LIO_CUDA(cudaGetLastError());
+  {
+    const dim3 grid((unsigned)d->slice_basis_tiles.n, (unsigned)(d->max_nftc * d->nk));
+    k_basis_block<<<grid, kTcPoints, 0, st>>>(d->slice_basis_tiles.p, d->groups.p, d->nk, d->basis.p, d->bblk.p);
+    LIO_CUDA(cudaGetLastError());
+  }
   if (d->lda)
     k_slice_basis<1><<<(unsigned)d->slice_basis_tiles.n, kTcPoints, 0, st>>>(d->slice_basis_tiles.p, d->groups.p,
                                                                             d->basis.p, d->aslices.p, d->aexp.p);
@@ -920,7 +888,7 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
 #define LIO_DENSITY_TC(GGA, NS)                                                                                    \
   k_density_tc<GGA, NS><<<nt, TcCfg<GGA, NS>::kThreads, TcCfg<GGA, NS>::smem(cap), st>>>(                          \
       d->dens_tc_tiles.p, ntiles, d->groups.p, d->aslices.p, d->aexp.p, d->dslices_a.p, d->dexp_a.p,               \
-      d->dslices_b.p, d->dexp_b.p, d->basis.p, cap, d->part_a.p, d->part_b.p, d->tc_err.p)
+      d->dslices_b.p, d->dexp_b.p, d->bblk.p, cap, d->part_a.p, d->part_b.p, d->tc_err.p)
     if (d->lda) {
       if (d->open) LIO_DENSITY_TC(false, 2); else LIO_DENSITY_TC(false, 1);
     } else {

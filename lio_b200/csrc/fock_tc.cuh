@@ -116,12 +116,7 @@ __global__ void __launch_bounds__(256) k_fock_slices(const int2* __restrict__ rt
         for (int k4 = 0; k4 < 4; k4++) {
           uint32_t packed = 0;
 #pragma unroll
-          for (int k = 0; k < 4; k++) {
-            const double y = x[k4 * 4 + k] * 128.0;
-            const double d = rint(y);
-            x[k4 * 4 + k] = y - d;
-            packed |= ((uint32_t)(uint8_t)(int8_t)d) << (8 * k);
-          }
+          for (int k = 0; k < 4; k++) packed |= ((uint32_t)(uint8_t)next_digit(x[k4 * 4 + k])) << (8 * k);
           w[k4] = packed;
         }
         const uint32_t off = TALL ? lio::umma::kmajor_offset(s * R + r, p0 & 31, kSlices * R)
