@@ -172,6 +172,43 @@ def reference_arm(args, rank, world):
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+STAGES = ("density_operands", "density", "functional", "ks_operands", "ks")
+
+
+def stage_times(L, steps: int):
+    """Per-stage device ms of the current precision (events between stages; a separate pass)."""
+    import torch
+
+    L.g2g_profile_(C.byref(C.c_uint(1)))
+    for _ in range(steps):
+        L.g2g_solve_resident_()
+    torch.cuda.synchronize()
+    stage = (C.c_double * 5)()
+    nsol = C.c_int(0)
+    L.g2g_stage_times_(stage, C.byref(nsol))
+    L.g2g_profile_(C.byref(C.c_uint(0)))
+    return [stage[i] / max(1, nsol.value) for i in range(5)]
+
+
+def measured_traffic(workload: str, tc: bool):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary
+    (profiles/density_launch_traffic.md: 'workload | kernel | bytes' rows), or None."""
+    p = os.path.join(ROOT, "profiles", "density_launch_traffic.md")
+    if not os.path.exists(p):
+        return None
+    want = "k_density_tc" if tc else "k_density_fp64"
+    key = workload.split(":")[0]
+    with open(p) as f:
+        for ln in f:
+            parts = [x.strip() for x in ln.strip().strip("|").split("|")]
+            if len(parts) >= 3 and parts[0] == key and parts[1] == want:
+                try:
+                    return float(parts[2])
+                except ValueError:
+                    return None
+    return None
+
+
 def cpu_baseline(wl: W.Workload):
     """Reference CPU g2g path on the same molecule (194-point grid), one warm-up and one timed build."""
     if not os.path.exists(REF_LIB):
@@ -259,47 +296,62 @@ def ours(args, rank, world):
         total_pts = float(npts)
 
     # per-stage times (separate profiled pass: events between stages)
-    L.g2g_profile_(C.byref(C.c_uint(1)))
-    for _ in range(args.steps):
-        L.g2g_solve_resident_()
-    torch.cuda.synchronize()
-    stage = (C.c_double * 3)()
-    nsol = C.c_int(0)
-    L.g2g_stage_times_(stage, C.byref(nsol))
-    L.g2g_profile_(C.byref(C.c_uint(0)))
-    stage_ms = [stage[i] / max(1, nsol.value) for i in range(3)]
+    stage_ms = stage_times(L, args.steps)
+
+    # the plain FP64 form on the same molecule and device, for the speed-up
+    fp64 = None
+    if args.precision == 1 and not args.no_fp64:
+        lib.set_precision(0)
+        for _ in range(args.warmup):
+            L.g2g_solve_resident_()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            L.g2g_solve_resident_()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        fp64_ms = e0.elapsed_time(e1) / args.steps
+        fp64_stage = stage_times(L, args.steps)
+        fp64 = {"value": total_pts / (fp64_ms * 1e-3), "ms_per_step": fp64_ms,
+                "stage_ms": dict(zip(STAGES, fp64_stage))}
+        lib.set_precision(args.precision)
 
     if rank != 0:
         return None
     hbm, bf16, src = load_peaks()
-    # dominant kernel: the density contraction (stage 0), nspin launches per build
+    # dominant kernel: the density contraction (stage 1), one launch per build
     pm = st["pm"]
-    pm2 = st["pm2"]
     nk = 10 if wl.iexch > 3 else 1
     na = 4 if wl.iexch > 3 else 1
-    dens_flops = 2.0 * na * pm2 * nspin
-    dens_bytes = (nk * pm * 8.0 + 10 * 8.0 * npts) * nspin
-    t_dens = stage_ms[0] * 1e-3
+    nq = 10 if wl.iexch > 3 else 1
+    tc = args.precision == 1
+    # algorithmic bytes of one launch: the FP64 basis values (nk per point and
+    # function), the int8 slices of the basis (na kinds x 6 slices) in the
+    # tensor-core form, and the per-point density quantities written per spin
+    dens_bytes = pm * (nk * 8.0 + (na * 6.0 if tc else 0.0)) + nq * 8.0 * npts * nspin
+    t_dens = stage_ms[1] * 1e-3
+    traffic = measured_traffic(wl.name, tc)
     result = {
         "metric": METRIC, "value": total_pts / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if args.precision == 0 else "i8-split/f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f64" if not tc else "i8-split/f64", "data": "synthetic",
         "config": {"workload": wl.name,
                    "points": npts, "groups": st["groups"], "M": wl.basis.M,
-                   "precision": "fp64" if args.precision == 0 else "tensor",
+                   "precision": "fp64" if not tc else "tensor (int8 Ozaki slices, exact int32, FP64 outside)",
                    "l2": "inputs larger than L2 (resident basis cache of %.1f GB)" % (nk * pm * 8 / 1e9),
                    "grid_build_s": round(grid_s, 3), "E_xc": E},
         "e2e": {"value": total_pts / (e2e_ms * 1e-3), "unit": UNIT,
                 "h2d_bytes_per_step": npacked * 8 * nspin, "d2h_bytes_per_step": npacked * 8 * nspin + 8},
         "gpu_launches": int(launches) * args.steps,
-        "stage_ms": {"density": stage_ms[0], "functional": stage_ms[1], "fock": stage_ms[2]},
+        "stage_ms": dict(zip(STAGES, stage_ms)),
         "roofline": {"bound": "hbm", "achieved": dens_bytes / t_dens / 1e9, "peak": hbm,
-                     "unit": "GB/s", "frac": dens_bytes / t_dens / 1e9 / hbm, "traffic": None,
-                     "kernel": "k_density (GGA, %d launches per build)" % nspin,
-                     "peak_source": src,
-                     "fp64_tflops": dens_flops / t_dens / 1e12},
+                     "unit": "GB/s", "frac": dens_bytes / t_dens / 1e9 / hbm,
+                     "traffic": traffic, "kernel": "k_density_tc" if tc else "k_density_fp64",
+                     "peak_source": src},
         "clocks": clk.summary(),
     }
+    if fp64 is not None:
+        result["fp64_plain"] = fp64
     if world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(wl)
     return result
@@ -311,8 +363,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", type=int, default=0, help="0 = FP64 plain, 1 = tensor-core form")
+    ap.add_argument("--precision", type=int, default=1, help="1 = tensor-core form (default), 0 = FP64 plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 form's comparison timing")
     ap.add_argument("--workload", default="cfg3", choices=["cfg3", "cfg2", "cfg2-open"],
                     help="cfg3 = the 256-atom headline workload; cfg2 / cfg2-open = the 64-atom closed- and "
                          "open-shell cases used for ncu captures")

@@ -138,9 +138,11 @@ int g2g_solve_resident_(void);
 
 /* Per-stage device timing with CUDA events recorded between the stages of
  * every solve. g2g_profile_(on) resets the sums; g2g_stage_times_ writes the
- * accumulated ms of stage 0 = density contraction(s), 1 = point functional and
- * energy sum, 2 = Kohn-Sham contraction, and the number of solves timed.
- * Returns the number of stages. */
+ * accumulated ms of five stages into ms[0..4]: 0 = density operand preparation
+ * (the int8 slices of the density matrices; empty in the FP64 form), 1 = density
+ * contraction, 2 = point functional and energy sum, 3 = Kohn-Sham operand
+ * preparation (slices of f*F; empty in the FP64 form), 4 = Kohn-Sham
+ * contraction, and the number of solves timed. Returns the number of stages. */
 void g2g_profile_(const unsigned int* on);
 int g2g_stage_times_(double* ms, int* solves);
 

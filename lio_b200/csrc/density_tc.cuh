@@ -216,6 +216,15 @@ __device__ __forceinline__ bool epi_sync_or(bool pred) {
   return out != 0;
 }
 
+// Whether a later unit of the same function tile reads chunk k again (the dF/dy,
+// dF/dz chunks after the F or x unit, dF/dx after F when x is a unit of its own):
+// those are kept in L2, last uses are evicted first.
+__device__ __forceinline__ bool chunk_reused(int first, int k, int KP) {
+  if (k < 1 || k > 3) return false;
+  const int next = first + KP;  // first kind of the next unit
+  return next <= 3 && k >= next;
+}
+
 // FP64 basis kinds whose chunks a unit with first contraction kind `first`
 // consumes, in order: F unit: all NK; x: dF/dx..dF/dz; y: dF/dy, dF/dz; z: dF/dz.
 __host__ __device__ __forceinline__ int unit_klo(int first) { return first == 0 ? 0 : first; }
@@ -332,6 +341,7 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
   if (warp == Cfg::kProd) {
     // ------------------------------------------------------------ operand producer
     if (lane == 0) {
+      const uint64_t keep = lio::umma::l2_evict_last(), drop = lio::umma::l2_evict_first();
       int cnt = 0;
       for (int w = blockIdx.x; w < ntiles && !*vfail; w += gridDim.x) {
         const int2 t = tiles[w];
@@ -348,14 +358,17 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
             }
             uint8_t* stage = tc_smem + buf * Cfg::kStage;
             lio::umma::mbar_expect_tx(&full[buf], (uint32_t)Cfg::kStage);
+            // A is read again by the tile's next function tile; D by every tile of the group
+            const uint64_t pa = ft + 1 < nft ? keep : drop;
             for (int kp = 0; kp < KP; kp++)
-              lio::umma::bulk_copy_g2s(stage + kp * kTcStepA,
-                                       Abase + ((long long)(pass * KP + kp) * nks + kk) * kTcStepA, kTcStepA,
-                                       &full[buf]);
+              lio::umma::bulk_copy_g2s_hint(stage + kp * kTcStepA,
+                                            Abase + ((long long)(pass * KP + kp) * nks + kk) * kTcStepA, kTcStepA,
+                                            &full[buf], pa);
             for (int sp = 0; sp < NS; sp++)
-              lio::umma::bulk_copy_g2s(stage + Cfg::kStageA + sp * kTcStepD,
-                                       (sp == 0 ? dsl_a : dsl_b) + G.ds_off + ((long long)ft * nks + kk) * kTcStepD,
-                                       kTcStepD, &full[buf]);
+              lio::umma::bulk_copy_g2s_hint(
+                  stage + Cfg::kStageA + sp * kTcStepD,
+                  (sp == 0 ? dsl_a : dsl_b) + G.ds_off + ((long long)ft * nks + kk) * kTcStepD, kTcStepD, &full[buf],
+                  keep);
             issued = cnt + 1;
           }
         }
@@ -364,6 +377,7 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
   } else if (warp == Cfg::kBasisProd) {
     // ------------------------------------------------------------ basis producer
     if (lane == 0) {
+      const uint64_t keep = lio::umma::l2_evict_last(), drop = lio::umma::l2_evict_first();
       int cnt = 0;
       for (int w = blockIdx.x; w < ntiles && !*vfail; w += gridDim.x) {
         const int2 t = tiles[w];
@@ -379,8 +393,9 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
               break;
             }
             lio::umma::mbar_expect_tx(&bfull[buf], (uint32_t)(kTcChunk * 8));
-            lio::umma::bulk_copy_g2s(tc_smem + Cfg::kBRing + (size_t)buf * kTcChunk * 8,
-                                     src + (long long)k * kTcChunk, kTcChunk * 8, &bfull[buf]);
+            lio::umma::bulk_copy_g2s_hint(tc_smem + Cfg::kBRing + (size_t)buf * kTcChunk * 8,
+                                          src + (long long)k * kTcChunk, kTcChunk * 8, &bfull[buf],
+                                          chunk_reused(first, k, KP) ? keep : drop);
             issued = cnt + 1;
           }
         }

@@ -495,14 +495,15 @@ struct DeviceEngine::Impl {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int launches = 0;
   bool profiling = false;
-  cudaEvent_t sev[4] = {nullptr, nullptr, nullptr, nullptr};
-  double stage_ms[3] = {0, 0, 0};
+  static constexpr int kNumStages = 5;
+  cudaEvent_t sev[kNumStages + 1] = {};
+  double stage_ms[kNumStages] = {};
   int profiled = 0;
   bool pending = false;
   void collect() {
     if (!pending) return;
-    LIO_CUDA(cudaEventSynchronize(sev[3]));
-    for (int i = 0; i < 3; i++) {
+    LIO_CUDA(cudaEventSynchronize(sev[kNumStages]));
+    for (int i = 0; i < kNumStages; i++) {
       float ms = 0.f;
       LIO_CUDA(cudaEventElapsedTime(&ms, sev[i], sev[i + 1]));
       stage_ms[i] += ms;
@@ -563,9 +564,9 @@ void DeviceEngine::set_profiling(bool on) {
 }
 int DeviceEngine::stage_times(double* ms, int max_stages, int* solves) const {
   impl_->collect();
-  for (int i = 0; i < 3 && i < max_stages; i++) ms[i] = impl_->stage_ms[i];
+  for (int i = 0; i < Impl::kNumStages && i < max_stages; i++) ms[i] = impl_->stage_ms[i];
   if (solves) *solves = impl_->profiled;
-  return 3;
+  return Impl::kNumStages;
 }
 long long DeviceEngine::groups() const { return impl_->ngroups; }
 
@@ -882,6 +883,7 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
       LIO_CUDA(cudaGetLastError());
       launches++;
     }
+    d->mark(1);
     const int ntiles = (int)d->dens_tc_tiles.n;
     const unsigned nt = (unsigned)std::min(ntiles, d->nsm);
     const int cap = d->tc_fcap;
@@ -898,6 +900,7 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
     LIO_CUDA(cudaGetLastError());
     launches++;
   } else {
+    d->mark(1);  // no operand preparation in the FP64 form
     for (int s = 0; s < nspin; s++) {
       const double* P = s == 0 ? d->P_a.p : d->P_b.p;
       double* part = s == 0 ? d->part_a.p : d->part_b.p;
@@ -909,7 +912,7 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
       launches++;
     }
   }
-  d->mark(1);
+  d->mark(2);
   // the tensor-core density writes one partial per point, the FP64 one one per 64-function tile
   k_functional<<<nf, kFuncBlock, 0, st>>>(d->func_tiles.p, d->groups.p, d->pw.p, d->part_a.p,
                                           d->open ? d->part_b.p : nullptr, tc ? (1 << 30) : kTile, d->lda ? 1 : 0,
@@ -919,7 +922,7 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
   k_sum_blocks<<<1, 1024, 0, st>>>(d->eblocks.p, (int)nf, d->energy.p);
   LIO_CUDA(cudaGetLastError());
   launches += 2;
-  d->mark(2);
+  d->mark(3);
   if (req.compute_rmm) {
     LIO_CUDA(cudaMemsetAsync(d->K_a.p, 0, npacked * sizeof(double), st));
     if (d->open) LIO_CUDA(cudaMemsetAsync(d->K_b.p, 0, npacked * sizeof(double), st));
@@ -944,6 +947,7 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
       }
       LIO_CUDA(cudaGetLastError());
       launches += 2;
+      d->mark(4);
       if (d->open)
         k_fock_tc<2><<<(unsigned)d->fk_tiles.n, FkCfg<2>::kThreads, FkCfg<2>::kSmem, st>>>(
             d->fk_tiles.p, d->groups.p, d->fn_glob.p, d->fa_slices.p, d->fa_exp.p, d->fb_slices_a.p, d->fb_exp_a.p,
@@ -953,17 +957,20 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
             d->fk_tiles.p, d->groups.p, d->fn_glob.p, d->fa_slices.p, d->fa_exp.p, d->fb_slices_a.p, d->fb_exp_a.p,
             nullptr, nullptr, d->M, d->K_a.p, nullptr, d->tc_err.p);
     } else if (d->open) {
+      d->mark(4);  // no operand preparation in the FP64 form
       k_fock_fp64<2><<<nk, 256, 0, st>>>(d->fock_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, d->fac_a.p,
                                          d->fac_b.p, d->M, d->K_a.p, d->K_b.p);
     } else {
+      d->mark(4);
       k_fock_fp64<1><<<nk, 256, 0, st>>>(d->fock_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, d->fac_a.p,
                                          nullptr, d->M, d->K_a.p, nullptr);
     }
     LIO_CUDA(cudaGetLastError());
     launches++;
   }
+  if (!req.compute_rmm) d->mark(4);
   d->launches = launches;
-  d->mark(3);
+  d->mark(5);
   d->pending = d->profiling;
   if (req.resident) {
     LIO_CUDA(cudaEventRecord(d->ev1, st));

@@ -355,7 +355,7 @@ int g2g_stage_times_(double* ms, int* solves) {
   guarded("g2g_stage_times_", [&] {
     State& s = st();
     if (!s.engine) throw std::runtime_error("no device engine");
-    n = s.engine->stage_times(ms, 3, solves);
+    n = s.engine->stage_times(ms, 5, solves);
   });
   return n;
 }

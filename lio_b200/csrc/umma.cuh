@@ -167,6 +167,16 @@ __device__ __forceinline__ double ld_hint(const double* a, uint64_t policy) {
   return v;
 }
 
+// bulk_copy_g2s with an L2 eviction-priority policy for the source lines
+__device__ __forceinline__ void bulk_copy_g2s_hint(void* smem_dst, const void* gmem_src, uint32_t size, uint64_t* mbar,
+                                                   uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+          smem_u32(smem_dst)),
+      "l"(gmem_src), "r"(size), "r"(smem_u32(mbar)), "l"(policy)
+      : "memory");
+}
+
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 }  // namespace umma
