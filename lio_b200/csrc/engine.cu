@@ -321,54 +321,79 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
 // One thread per point: reduce the function-tile partials, evaluate the
 // functional, write factor = w * v_xc, and a per-block energy sum of
 // rho * w * (ex + ec) (g2g/cpu/iteration.cpp:106-114, 199-208, 482-492).
-__global__ void k_functional(const int2* __restrict__ tiles, const GroupDev* __restrict__ groups,
-                             const double* __restrict__ pw, const double* __restrict__ part_a,
-                             const double* __restrict__ part_b, int part_tile, int lda, int open, int iexch,
-                             double* __restrict__ fac_a, double* __restrict__ fac_b,
-                             double* __restrict__ energy_blocks) {
+// MODE: 0 closed LDA, 1 closed GGA (PBE), 2 open GGA (PBE), 3 open LDA (the
+// reference CPU path has no branch for it, g2g/cpu/iteration.cpp:362-363:
+// energy and potential stay zero). Compile-time so the per-point sums live in
+// registers.
+template <int MODE>
+__global__ void __launch_bounds__(kFuncBlock) k_functional(const int2* __restrict__ tiles,
+                                                           const GroupDev* __restrict__ groups,
+                                                           const double* __restrict__ pw,
+                                                           const double* __restrict__ part_a,
+                                                           const double* __restrict__ part_b, int part_tile,
+                                                           int iexch, double* __restrict__ fac_a,
+                                                           double* __restrict__ fac_b,
+                                                           double* __restrict__ energy_blocks) {
+  constexpr bool kLda = MODE == 0 || MODE == 3, kOpen = MODE >= 2;
+  constexpr int NQ = kLda ? 1 : kNQ;
   __shared__ double sh[32];
   const int2 t = tiles[blockIdx.x];
-  const GroupDev G = groups[t.x];
+  const GroupDev& G = groups[t.x];
   const int p = t.y * kFuncBlock + threadIdx.x;
+  const int ldp = G.ldp;
   double e = 0.0;
-  if (p < G.ldp) {
+  if (p < ldp) {
     const double w = pw[G.pt_off + p];
-    const int NQ = lda ? 1 : kNQ;
     double qa[kNQ], qb[kNQ];
+#pragma unroll
     for (int k = 0; k < kNQ; k++) qa[k] = qb[k] = 0.0;
     const int nparts = (G.m + part_tile - 1) / part_tile;  // partial tiles written by the density stage
     for (int f = 0; f < nparts; f++)
+#pragma unroll
       for (int k = 0; k < NQ; k++) {
-        const long long o = G.part_off + ((long long)f * NQ + k) * G.ldp + p;
+        const long long o = G.part_off + ((long long)f * NQ + k) * ldp + p;
         qa[k] += part_a[o];
-        if (open) qb[k] += part_b[o];
+        if (kOpen) qb[k] += part_b[o];
       }
     double va = 0.0, vb = 0.0;
     if (p < G.npts) {
-      if (open) {
-        if (!lda) {
-          const xc::GgaOpenOut o = xc::pbe_open(qa[0], qb[0], qa + 1, qb + 1, qa + 4, qb + 4, qa + 7, qb + 7);
-          e = ((qa[0] + qb[0]) * w) * (o.ex + o.ec);
-          va = w * o.va;
-          vb = w * o.vb;
-        }
-        // open-shell LDA: the reference CPU path has no branch for it
-        // (g2g/cpu/iteration.cpp:362-363); energy and potential stay zero.
-      } else if (lda) {
+      if (MODE == 2) {
+        const xc::GgaOpenOut o = xc::pbe_open(qa[0], qb[0], qa + 1, qb + 1, qa + 4, qb + 4, qa + 7, qb + 7);
+        e = ((qa[0] + qb[0]) * w) * (o.ex + o.ec);
+        va = w * o.va;
+        vb = w * o.vb;
+      } else if (MODE == 0) {
         const xc::LdaOut o = xc::lda_closed(qa[0], iexch);
         e = (qa[0] * w) * (o.ex + o.ec);
         va = w * o.v;
-      } else {
+      } else if (MODE == 1) {
         const xc::GgaOut o = xc::pbe_closed(qa[0], qa + 1, qa + 4, qa + 7);
         e = (qa[0] * w) * (o.ex + o.ec);
         va = w * o.v;
       }
     }
     fac_a[G.pt_off + p] = va;
-    if (open) fac_b[G.pt_off + p] = vb;
+    if (kOpen) fac_b[G.pt_off + p] = vb;
   }
   const double s = block_sum(e, sh);
   if (threadIdx.x == 0) energy_blocks[blockIdx.x] = s;
+}
+
+void launch_functional(bool lda, bool open, unsigned nblocks, cudaStream_t st, const int2* tiles,
+                       const GroupDev* groups, const double* pw, const double* part_a, const double* part_b,
+                       int part_tile, int iexch, double* fac_a, double* fac_b, double* eblocks) {
+  if (!open && lda)
+    k_functional<0><<<nblocks, kFuncBlock, 0, st>>>(tiles, groups, pw, part_a, part_b, part_tile, iexch, fac_a, fac_b,
+                                                    eblocks);
+  else if (!open)
+    k_functional<1><<<nblocks, kFuncBlock, 0, st>>>(tiles, groups, pw, part_a, part_b, part_tile, iexch, fac_a, fac_b,
+                                                    eblocks);
+  else if (!lda)
+    k_functional<2><<<nblocks, kFuncBlock, 0, st>>>(tiles, groups, pw, part_a, part_b, part_tile, iexch, fac_a, fac_b,
+                                                    eblocks);
+  else
+    k_functional<3><<<nblocks, kFuncBlock, 0, st>>>(tiles, groups, pw, part_a, part_b, part_tile, iexch, fac_a, fac_b,
+                                                    eblocks);
 }
 
 __global__ void k_sum_blocks(const double* __restrict__ in, int n, double* __restrict__ out) {
@@ -914,10 +939,9 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
   }
   d->mark(2);
   // the tensor-core density writes one partial per point, the FP64 one one per 64-function tile
-  k_functional<<<nf, kFuncBlock, 0, st>>>(d->func_tiles.p, d->groups.p, d->pw.p, d->part_a.p,
-                                          d->open ? d->part_b.p : nullptr, tc ? (1 << 30) : kTile, d->lda ? 1 : 0,
-                                          d->open ? 1 : 0,
-                                          d->iexch, d->fac_a.p, d->open ? d->fac_b.p : nullptr, d->eblocks.p);
+  launch_functional(d->lda, d->open, nf, st, d->func_tiles.p, d->groups.p, d->pw.p, d->part_a.p,
+                    d->open ? d->part_b.p : nullptr, tc ? (1 << 30) : kTile, d->iexch, d->fac_a.p,
+                    d->open ? d->fac_b.p : nullptr, d->eblocks.p);
   LIO_CUDA(cudaGetLastError());
   k_sum_blocks<<<1, 1024, 0, st>>>(d->eblocks.p, (int)nf, d->energy.p);
   LIO_CUDA(cudaGetLastError());
@@ -1106,9 +1130,8 @@ void DeviceEngine::solve_noalloc(const double* rho_a, const double* rho_b, doubl
                                                           P, d->M, s == 0 ? pa : pb);
       LIO_CUDA(cudaGetLastError());
     }
-    k_functional<<<(unsigned)nf, kFuncBlock, 0, st>>>(d->func_tiles.p + ft0, d->groups.p, d->pw.p, pa,
-                                                       d->open ? pb : nullptr, kTile, d->lda ? 1 : 0, d->open ? 1 : 0,
-                                                       d->iexch, fa, d->open ? fb : nullptr, eblk);
+    launch_functional(d->lda, d->open, (unsigned)nf, st, d->func_tiles.p + ft0, d->groups.p, d->pw.p, pa,
+                      d->open ? pb : nullptr, kTile, d->iexch, fa, d->open ? fb : nullptr, eblk);
     LIO_CUDA(cudaGetLastError());
     k_sum_blocks<<<1, 1024, 0, st>>>(eblk, (int)nf, eparts + nbatch);
     LIO_CUDA(cudaGetLastError());
