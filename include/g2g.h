@@ -136,6 +136,12 @@ void g2g_set_stream_(void* cuda_stream);
  * number of kernel launches it enqueued. */
 int g2g_solve_resident_(void);
 
+/* No counterpart in the reference: replay each solve's kernels from a CUDA
+ * graph captured on the first solve after a new grid or precision (on by
+ * default; 0 launches the kernels one by one). Profiled solves always launch
+ * them one by one. */
+void g2g_set_graphs_(const unsigned int* on);
+
 /* Per-stage device timing with CUDA events recorded between the stages of
  * every solve. g2g_profile_(on) resets the sums; g2g_stage_times_ writes the
  * accumulated ms of five stages into ms[0..4]: 0 = density operand preparation

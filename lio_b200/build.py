@@ -23,11 +23,12 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
-HOST_SRCS = ["partition.cpp", "g2g_abi.cpp"]
+HOST_SRCS = ["partition.cpp", "g2g_abi.cpp", "serve.cpp"]
 CUDA_SRCS = ["engine.cu", "tc_selftest.cu"]
 HEADERS = ["system.h", "partition.h", "engine.h", "xc_functionals.cuh", "umma.cuh", "density_tc.cuh", "fock_tc.cuh"]
 
 CXXFLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-fopenmp", "-fvisibility=hidden",
+            "-I" + os.path.join(CUDA_HOME, "include"),
             "-Wall", "-Wextra", "-Wno-unused-parameter"]
 NVCCFLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
              "-Xcompiler", "-fPIC,-fvisibility=hidden", "--expt-relaxed-constexpr", "-Xptxas", "-v"]
@@ -54,7 +55,8 @@ def _run(cmd: list[str], log: list[str]) -> None:
 
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
-    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(HERE, "..", "include", "g2g.h")]
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(HERE, "..", "include", h)
+                                                       for h in ("g2g.h", "lio_serve.h")]
     objs, log = [], []
     for s in HOST_SRCS:
         src, obj = os.path.join(CSRC, s), os.path.join(OBJ, s + ".o")

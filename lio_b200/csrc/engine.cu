@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -72,6 +73,9 @@ struct GroupDev {
   long long fbe_off;   // their per-row exponents (elements): nJ x 32
 };
 
+// device bytes held by every DevBuf of the process (footprint accounting)
+std::atomic<long long> g_devbuf_bytes{0};
+
 template <class T>
 struct DevBuf {
   T* p = nullptr;
@@ -81,13 +85,17 @@ struct DevBuf {
     if (count == 0) count = 1;
     LIO_CUDA(cudaMalloc(&p, count * sizeof(T)));
     n = count;
+    g_devbuf_bytes += (long long)(n * sizeof(T));
   }
   void upload(const std::vector<T>& v) {
     alloc(v.size());
     if (!v.empty()) LIO_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
   }
   void free() {
-    if (p) cudaFree(p);
+    if (p) {
+      cudaFree(p);
+      g_devbuf_bytes -= (long long)(n * sizeof(T));
+    }
     p = nullptr;
     n = 0;
   }
@@ -514,7 +522,25 @@ struct DeviceEngine::Impl {
   DevBuf<int2> basis_tiles, func_tiles;
   DevBuf<int4> dens_tiles, fock_tiles;
   DevBuf<double> P_a, P_b, K_a, K_b, part_a, part_b, fac_a, fac_b, eblocks, energy;
-  std::vector<double> hK;
+  double* hK = nullptr;  // pinned: Kohn-Sham result of the last solve (nspin x npacked)
+  double* hE = nullptr;  // pinned: its energy
+  int* hErr = nullptr;   // pinned: the tensor-core error flag
+  bool enqueued = false;
+  bool use_graphs = true;
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_key = -1, graph_launches = 0;
+  void drop_graph() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    graph_exec = nullptr;
+    graph_key = -1;
+  }
+  void free_pinned() {
+    if (hK) cudaFreeHost(hK);
+    if (hE) cudaFreeHost(hE);
+    if (hErr) cudaFreeHost(hErr);
+    hK = hE = nullptr;
+    hErr = nullptr;
+  }
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -548,6 +574,8 @@ struct DeviceEngine::Impl {
     for (auto& e : sev) LIO_CUDA(cudaEventCreate(&e));
   }
   ~Impl() {
+    drop_graph();
+    free_pinned();
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     for (auto& e : sev)
@@ -786,7 +814,12 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
   }
   d->eblocks.alloc(ftiles.size());
   d->energy.alloc(1);
-  d->hK.resize(npacked);
+  d->drop_graph();
+  d->free_pinned();
+  LIO_CUDA(cudaMallocHost(&d->hK, npacked * (sys.open ? 2 : 1) * sizeof(double)));
+  LIO_CUDA(cudaMallocHost(&d->hE, sizeof(double)));
+  LIO_CUDA(cudaMallocHost(&d->hErr, sizeof(int)));
+  *d->hErr = 0;
 
   // basis values, computed once per geometry and kept resident
   d->basis.alloc(bas_off);
@@ -871,32 +904,19 @@ void DeviceEngine::prepare_tensor_core() {
   d->tc_ready = true;
 }
 
-SolveResult DeviceEngine::solve(const SolveRequest& req) {
+// The device work of one solve, from the densities in d->P_a / d->P_b to E_xc in
+// d->energy and the Kohn-Sham contributions in d->K_a / d->K_b; captured once
+// into a CUDA graph when graphs are on. Returns the number of kernel launches.
+int DeviceEngine::run_kernels(bool compute_rmm) {
   Impl* d = impl_.get();
-  SolveResult res;
   const size_t npacked = (size_t)d->M * (d->M + 1) / 2;
-  if (d->ngroups == 0) return res;
   cudaStream_t st = d->stream;
   int launches = 0;
-  LIO_CUDA(cudaEventRecord(d->ev0, st));
-  if (req.resident) {
-    // density already on the device
-  } else if (d->open) {
-    LIO_CUDA(cudaMemcpyAsync(d->P_a.p, req.rho_a, npacked * sizeof(double), cudaMemcpyHostToDevice, st));
-    LIO_CUDA(cudaMemcpyAsync(d->P_b.p, req.rho_b, npacked * sizeof(double), cudaMemcpyHostToDevice, st));
-  } else {
-    LIO_CUDA(cudaMemcpyAsync(d->P_a.p, req.rho, npacked * sizeof(double), cudaMemcpyHostToDevice, st));
-  }
   const unsigned nd = (unsigned)d->dens_tiles.n, nf = (unsigned)d->func_tiles.n,
                  nk = (unsigned)d->fock_tiles.n;
-  d->collect();
   d->mark(0);
   const int nspin = d->open ? 2 : 1;
   const bool tc = precision_ == Precision::TensorCore;
-  if (tc && !d->tc_ready) {
-    prepare_tensor_core();
-    d->mark(0);
-  }
   if (tc) {
     // D slices of each spin, then one launch for both spins (shared A slices and basis rebuild)
     for (int s = 0; s < nspin; s++) {
@@ -947,7 +967,7 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
   LIO_CUDA(cudaGetLastError());
   launches += 2;
   d->mark(3);
-  if (req.compute_rmm) {
+  if (compute_rmm) {
     LIO_CUDA(cudaMemsetAsync(d->K_a.p, 0, npacked * sizeof(double), st));
     if (d->open) LIO_CUDA(cudaMemsetAsync(d->K_b.p, 0, npacked * sizeof(double), st));
     if (tc) {
@@ -992,37 +1012,144 @@ SolveResult DeviceEngine::solve(const SolveRequest& req) {
     LIO_CUDA(cudaGetLastError());
     launches++;
   }
-  if (!req.compute_rmm) d->mark(4);
-  d->launches = launches;
+  if (!compute_rmm) d->mark(4);
   d->mark(5);
-  d->pending = d->profiling;
+  return launches;
+}
+
+void DeviceEngine::set_graphs(bool on) {
+  impl_->use_graphs = on;
+  impl_->drop_graph();
+}
+void DeviceEngine::set_graphs_dirty() { impl_->drop_graph(); }
+
+void DeviceEngine::prepare() {
+  if (precision_ == Precision::TensorCore && !impl_->tc_ready) {
+    prepare_tensor_core();
+    impl_->drop_graph();
+    LIO_CUDA(cudaStreamSynchronize(impl_->stream));
+  }
+}
+
+long long DeviceEngine::process_device_bytes() { return g_devbuf_bytes.load(); }
+
+size_t DeviceEngine::estimate_device_bytes(const System& sys, const Partition& part, Precision prec) {
+  const int nk = sys.lda ? 1 : 10, na = sys.lda ? 1 : 4, nq = sys.lda ? 1 : kNQ, nspin = sys.open ? 2 : 1;
+  const size_t npacked = (size_t)sys.M * (sys.M + 1) / 2;
+  double b = (double)npacked * 8 * 2 * nspin;  // densities and Kohn-Sham accumulators
+  for (int g = 0; g < part.total_groups(); g++) {
+    const PointGroup& pg = part.group(g);
+    const double ldp = (double)(((long long)pg.points.size() + kPointPad - 1) / kPointPad * kPointPad);
+    const int m = pg.total_functions(), m32 = (m + 31) / 32 * 32;
+    const int nft = (m + kTile - 1) / kTile, nftc = (m + kTcFuncs - 1) / kTcFuncs;
+    const int nI = (m + kFkRows - 1) / kFkRows, nJ = (m + kFkCols - 1) / kFkCols;
+    b += ldp * (nk * (double)m * 8 + 6 * 8 + nspin * (nq * (double)nft * 8 + 8));  // basis, points, partials, factors
+    if (prec == Precision::TensorCore)
+      b += ldp * ((double)nftc * kTcFuncs * nk * 8 + (double)na * m32 * kSlices + na * 2 +
+                  (double)nI * kFkRows * kSlices + (double)nspin * nJ * kFkCols * kSlices) +
+           (double)nspin * nftc * m32 * kTcTall;
+  }
+  return (size_t)(b * 1.05) + (16u << 20);
+}
+
+void DeviceEngine::enqueue(const SolveRequest& req) {
+  Impl* d = impl_.get();
+  const size_t npacked = (size_t)d->M * (d->M + 1) / 2;
+  d->enqueued = false;
+  if (d->ngroups == 0) return;
+  cudaStream_t st = d->stream;
+  const bool tc = precision_ == Precision::TensorCore;
+  if (tc && !d->tc_ready) {
+    prepare_tensor_core();
+    d->drop_graph();
+  }
+  d->collect();
+  LIO_CUDA(cudaEventRecord(d->ev0, st));
   if (req.resident) {
-    LIO_CUDA(cudaEventRecord(d->ev1, st));
-    return res;
+    // density already on the device
+  } else if (d->open) {
+    LIO_CUDA(cudaMemcpyAsync(d->P_a.p, req.rho_a, npacked * sizeof(double), cudaMemcpyHostToDevice, st));
+    LIO_CUDA(cudaMemcpyAsync(d->P_b.p, req.rho_b, npacked * sizeof(double), cudaMemcpyHostToDevice, st));
+  } else {
+    LIO_CUDA(cudaMemcpyAsync(d->P_a.p, req.rho, npacked * sizeof(double), cudaMemcpyHostToDevice, st));
   }
-  double e = 0.0;
-  LIO_CUDA(cudaMemcpyAsync(&e, d->energy.p, sizeof(double), cudaMemcpyDeviceToHost, st));
-  LIO_CUDA(cudaEventRecord(d->ev1, st));
-  if (req.compute_rmm) {
-    for (int s = 0; s < nspin; s++) {
-      LIO_CUDA(cudaMemcpyAsync(d->hK.data(), s == 0 ? d->K_a.p : d->K_b.p, npacked * sizeof(double),
-                               cudaMemcpyDeviceToHost, st));
-      LIO_CUDA(cudaStreamSynchronize(st));
-      double* dst = s == 0 ? req.fock : req.fock_b;
-      for (size_t i = 0; i < npacked; i++) dst[i] += d->hK[i];
+  // graph replay when on (not while profiling: the stage events are recorded eagerly)
+  const int key = (tc ? 2 : 0) | (req.compute_rmm ? 1 : 0);
+  if (d->use_graphs && !d->profiling) {
+    if (!d->graph_exec || d->graph_key != key) {
+      d->drop_graph();
+      cudaGraph_t g = nullptr;
+      LIO_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      int n = 0;
+      try {
+        n = run_kernels(req.compute_rmm);
+      } catch (...) {
+        cudaStreamEndCapture(st, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      LIO_CUDA(cudaStreamEndCapture(st, &g));
+      LIO_CUDA(cudaGraphInstantiate(&d->graph_exec, g, 0));
+      LIO_CUDA(cudaGraphDestroy(g));
+      d->graph_key = key;
+      d->graph_launches = n;
     }
+    LIO_CUDA(cudaGraphLaunch(d->graph_exec, st));
+    d->launches = d->graph_launches;
+  } else {
+    d->launches = run_kernels(req.compute_rmm);
+    d->pending = d->profiling;
   }
-  LIO_CUDA(cudaStreamSynchronize(st));
-  if (tc) {
-    int flag = 0;
-    LIO_CUDA(cudaMemcpy(&flag, d->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost));
-    if (flag) throw std::runtime_error("tensor-core density: an MMA completion wait timed out");
+  if (!req.resident) {
+    const int nspin = d->open ? 2 : 1;
+    LIO_CUDA(cudaMemcpyAsync(d->hE, d->energy.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (tc) LIO_CUDA(cudaMemcpyAsync(d->hErr, d->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (req.compute_rmm)
+      for (int s = 0; s < nspin; s++)
+        LIO_CUDA(cudaMemcpyAsync(d->hK + s * npacked, s == 0 ? d->K_a.p : d->K_b.p, npacked * sizeof(double),
+                                 cudaMemcpyDeviceToHost, st));
+  }
+  LIO_CUDA(cudaEventRecord(d->ev1, st));
+  d->enqueued = true;
+}
+
+bool DeviceEngine::ready() const {
+  Impl* d = impl_.get();
+  if (!d->enqueued) return true;
+  const cudaError_t e = cudaEventQuery(d->ev1);
+  if (e == cudaErrorNotReady) return false;
+  LIO_CUDA(e);
+  return true;
+}
+
+SolveResult DeviceEngine::finish(const SolveRequest& req) {
+  Impl* d = impl_.get();
+  SolveResult res;
+  if (!d->enqueued) return res;
+  d->enqueued = false;
+  if (req.resident) return res;
+  const size_t npacked = (size_t)d->M * (d->M + 1) / 2;
+  LIO_CUDA(cudaEventSynchronize(d->ev1));
+  if (precision_ == Precision::TensorCore && *d->hErr)
+    throw std::runtime_error("tensor-core density: an MMA completion wait timed out");
+  if (req.compute_rmm) {
+    const int nspin = d->open ? 2 : 1;
+    for (int s = 0; s < nspin; s++) {
+      double* dst = s == 0 ? req.fock : req.fock_b;
+      const double* src = d->hK + s * npacked;
+      for (size_t i = 0; i < npacked; i++) dst[i] += src[i];
+    }
   }
   float ms = 0.f;
   LIO_CUDA(cudaEventElapsedTime(&ms, d->ev0, d->ev1));
-  res.energy = e;
+  res.energy = *d->hE;
   res.device_ms = ms;
   return res;
+}
+
+SolveResult DeviceEngine::solve(const SolveRequest& req) {
+  enqueue(req);
+  return finish(req);
 }
 
 // ======================================================= no-allocation variant

@@ -46,15 +46,29 @@ class DeviceEngine {
   // Uploads basis parameters, points and function lists; evaluates and caches
   // the basis values of every group that fits the cache budget.
   void upload(const System& sys, const Partition& part);
+  // One XC build: enqueue() puts all of its device work on the engine's stream
+  // (density upload unless resident, the kernels, result download into pinned
+  // buffers) and returns; ready() polls it; finish() waits for it and delivers
+  // the outputs (Kohn-Sham += into req.fock / fock_b, E_xc). solve() = both.
+  // One solve in flight per engine.
+  void enqueue(const SolveRequest& req);
+  bool ready() const;
+  SolveResult finish(const SolveRequest& req);
   SolveResult solve(const SolveRequest& req);
-  void set_precision(Precision p) { precision_ = p; }
+  // Replay the kernels of a solve from a CUDA graph captured on first use
+  // (re-captured after a new geometry or precision).
+  void set_graphs(bool on);
+  void set_precision(Precision p) {
+    if (p != precision_) set_graphs_dirty();
+    precision_ = p;
+  }
   // Stream for all device work (nullptr: the engine's own stream).
   void set_stream(void* cuda_stream);
   // Kernel launches of one solve (for launch accounting).
   int launches_per_solve() const;
   // Per-stage device timing (CUDA events between the stages of every solve):
-  // stage 0 = density contraction(s), 1 = point functional + energy sum,
-  // 2 = Kohn-Sham contraction. Accumulated over solves until reset.
+  // five stages (density operands, density contraction, functional and energy,
+  // Kohn-Sham operands, Kohn-Sham contraction), accumulated over solves until reset.
   void set_profiling(bool on);
   int stage_times(double* ms, int max_stages, int* solves) const;
   Precision precision() const { return precision_; }
@@ -72,6 +86,12 @@ class DeviceEngine {
 
   // true when a CUDA device can be used from this process
   static bool available();
+  // builds the tensor-core operands now (otherwise the first tensor-core solve does)
+  void prepare();
+  // device bytes held by all engines of the process, and an estimate of one
+  // molecule's footprint before it is uploaded
+  static long long process_device_bytes();
+  static size_t estimate_device_bytes(const System& sys, const Partition& part, Precision prec);
 
   // statistics of the uploaded partition
   long long points() const;
@@ -79,6 +99,8 @@ class DeviceEngine {
 
  private:
   void prepare_tensor_core();
+  int run_kernels(bool compute_rmm);
+  void set_graphs_dirty();
   struct Impl;
   std::unique_ptr<Impl> impl_;
   Precision precision_ = Precision::FP64;

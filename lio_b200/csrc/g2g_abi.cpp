@@ -55,6 +55,7 @@ struct State {
   double last_solve_ms = 0.0, last_grid_ms = 0.0;
   bool device_ready = false;
   void* stream = nullptr;
+  bool graphs = true;
 };
 
 State& st() {
@@ -149,6 +150,7 @@ void build_grid(unsigned grid_type) {
   }
   if (!s.engine) s.engine.reset(new lio::DeviceEngine());
   s.engine->set_stream(s.stream);
+  s.engine->set_graphs(s.graphs);
   s.engine->set_precision(s.precision);
   s.engine->upload(s.sys, s.part);
   s.device_ready = true;
@@ -341,6 +343,14 @@ int g2g_solve_resident_(void) {
     n = s.engine->launches_per_solve();
   });
   return n;
+}
+
+void g2g_set_graphs_(const unsigned* on) {
+  guarded("g2g_set_graphs_", [&] {
+    State& s = st();
+    s.graphs = *on != 0;
+    if (s.engine) s.engine->set_graphs(s.graphs);
+  });
 }
 
 void g2g_profile_(const unsigned* on) {
