@@ -357,6 +357,122 @@ def ours(args, rank, world):
     return result
 
 
+def batch_mode(args):
+    """Many-molecule batch: every build of the batch submitted at once to the
+    XC service (continuous batching over per-molecule streams); value = grid
+    points / wall second from first submission to last result (host arrays in
+    and out, so this is also the end-to-end figure)."""
+    from lio_b200 import serve as S
+
+    wls = S.batch_molecules(args.batch)
+    srv = S.XCServer(precision=args.service_precision, max_inflight=args.inflight)
+    t0 = time.perf_counter()
+    mids = [srv.add(wl) for wl in wls]
+    grid_s = time.perf_counter() - t0
+    dens = {m: S.densities(srv.mols[m][0]) for m in mids}
+    pts = sum(srv.info(m)["points"] for m in mids)
+    for _ in range(max(1, args.warmup)):
+        res = S.run_all(srv, mids, dens)
+    srv.reset_stats()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        res = S.run_all(srv, mids, dens)
+    dt = (time.perf_counter() - t0) / args.steps
+    st = srv.stats()
+    forms = [srv.form(m) for m in mids]
+    srv.close()
+    tuned = {"fp64_ms_sum": sum(f[1] for f in forms), "tensor_ms_sum": sum(f[2] for f in forms)}
+    forms = [f[0] for f in forms]
+    # the same builds in the plain FP64 form: per-molecule differences and its throughput
+    ref = S.XCServer(precision=0, max_inflight=args.inflight)
+    rmids = [ref.add(wl) for wl in wls]
+    S.run_all(ref, rmids, {r: dens[m] for r, m in zip(rmids, mids)})
+    t0 = time.perf_counter()
+    res0 = S.run_all(ref, rmids, {r: dens[m] for r, m in zip(rmids, mids)})
+    dt0 = time.perf_counter() - t0
+    ref.close()
+    de = max(abs(res[m][0] - res0[r][0]) for m, r in zip(mids, rmids))
+    dk = max(float(np.max(np.abs(res[m][1] - res0[r][1]))) for m, r in zip(mids, rmids))
+    nlda = sum(1 for wl in wls if wl.iexch <= 3)
+    return {"metric": METRIC, "value": pts / dt, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "i8-split/f64" if args.service_precision else "f64", "data": "synthetic",
+            "mode": "batch",
+            "config": {"workload": f"cfg4: {len(wls)} clusters, 3-40 atoms log-uniform (H:C:N:O 10:4:1:1), "
+                                   f"30x194 grids, closed shell, {nlda} LDA-VWN / {len(wls) - nlda} PBE",
+                       "points": pts, "grid_build_s": round(grid_s, 2), "max_inflight": args.inflight,
+                       "peak_inflight": st["peak_inflight"], "evictions": st["evictions"],
+                       "forms": {"tensor": sum(1 for f in forms if f == 1), "fp64": sum(1 for f in forms if f == 0)},
+                       "autotune_device_ms_per_build": tuned,
+                       "service_precision": args.service_precision},
+            "e2e": {"value": pts / dt, "unit": UNIT, "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
+            "fp64_plain": {"value": pts / dt0, "ms_per_step": dt0 * 1e3},
+            "max_abs_dE_vs_fp64": de, "max_abs_dK_vs_fp64": dk}
+
+
+def serve_mode(args):
+    """Served stream: Poisson arrivals of XC builds for resident molecules at a
+    sweep of rates (fractions of the measured closed-loop capacity); p50/p99
+    latency per rate, for the tensor-core and the FP64 form."""
+    from lio_b200 import serve as S
+
+    wls = S.served_molecules(args.molecules, max_atoms=args.max_atoms)
+    out = {"metric": METRIC, "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "data": "synthetic", "mode": "serve",
+           "config": {"workload": f"cfg5: {len(wls)} resident clusters, 4-{args.max_atoms} atoms log-uniform, "
+                                  "40x302 grids, closed-shell PBE, P = P0 + 1e-3 S per request",
+                      "duration_s_per_rate": args.duration, "max_inflight": args.inflight}}
+    rates = None
+    for prec in (args.service_precision, 0):
+        srv = S.XCServer(precision=prec, max_inflight=args.inflight)
+        mids = [srv.add(wl) for wl in wls]
+        dens = {m: S.densities(srv.mols[m][0]) for m in mids}
+        S.run_all(srv, mids, dens)  # residency and graphs
+        srv.reset_stats()
+        t0 = time.perf_counter()
+        for _ in range(2):
+            S.run_all(srv, mids, dens)
+        cap = 2 * len(mids) / (time.perf_counter() - t0)  # builds per second, closed loop
+        if rates is None:  # offered loads: fractions of the tensor-core form's capacity, for both forms
+            rates = [f * cap for f in (0.25, 0.5, 0.75, 0.9)]
+        sweep = []
+        for rate in rates:
+            srv.reset_stats()
+            lat, sample = S.serve_poisson(srv, mids, rate, args.duration, seed=int(rate) % 1000)
+            st = srv.stats()
+            row = {"rate_hz": round(rate, 2), "requests": len(lat), "p50_ms": st["p50_ms"],
+                   "p99_ms": st["p99_ms"], "points_per_s": st["points"] / max(st["wall_s"], 1e-9),
+                   "peak_inflight": st["peak_inflight"], "evictions": st["evictions"]}
+            if prec == args.service_precision and sample:
+                row["spot_checks"] = len(sample)
+                row["spot_max_abs_dE_vs_fp64"], row["spot_max_abs_dK_vs_fp64"] = spot_check(wls, mids, sample)
+            sweep.append(row)
+        forms = [srv.form(m)[0] for m in mids]
+        srv.close()
+        out["tensor" if prec else "fp64_plain"] = {
+            "capacity_builds_per_s": cap, "sweep": sweep,
+            "forms": {"tensor": sum(1 for f in forms if f == 1), "fp64": sum(1 for f in forms if f == 0)}}
+    top = out["tensor"]["sweep"][-1]
+    out.update(value=top["points_per_s"], p50_ms=top["p50_ms"], p99_ms=top["p99_ms"],
+               dtype="i8-split/f64" if args.service_precision else "f64")
+    return out
+
+
+def spot_check(wls, mids, sample):
+    """FP64 single-molecule C ABI on the sampled requests' molecules and densities."""
+    from tests import helpers as H
+
+    L = G2GLibrary()
+    de = dk = 0.0
+    for mid, rho, e, ka in sample:
+        wl = wls[mids.index(mid)]
+        wl2 = W.Workload(**{**wl.__dict__, "rho": rho})
+        E0, K0, _ = H.run(L, wl2, precision=0)
+        de = max(de, abs(e - E0))
+        dk = max(dk, float(np.max(np.abs(ka - K0))))
+    return de, dk
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -366,6 +482,16 @@ def main():
     ap.add_argument("--precision", type=int, default=1, help="1 = tensor-core form (default), 0 = FP64 plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 form's comparison timing")
+    ap.add_argument("--mode", default="single", choices=["single", "batch", "serve"],
+                    help="single = the headline 256-atom build; batch = the 512-molecule batch; "
+                         "serve = Poisson-arrival serving of 64 resident molecules")
+    ap.add_argument("--batch", type=int, default=512, help="molecules in the batch mode")
+    ap.add_argument("--molecules", type=int, default=64, help="resident molecules in the serve mode")
+    ap.add_argument("--max-atoms", type=int, default=200, help="largest molecule in the serve mode")
+    ap.add_argument("--duration", type=float, default=4.0, help="seconds per arrival rate in the serve mode")
+    ap.add_argument("--inflight", type=int, default=32, help="builds on the GPU at once (batch / serve)")
+    ap.add_argument("--service-precision", type=int, default=2,
+                    help="form of the batch / serve modes: 0 FP64, 1 tensor core, 2 autotuned per molecule")
     ap.add_argument("--workload", default="cfg3", choices=["cfg3", "cfg2", "cfg2-open"],
                     help="cfg3 = the 256-atom headline workload; cfg2 / cfg2-open = the 64-atom closed- and "
                          "open-shell cases used for ncu captures")
@@ -376,6 +502,10 @@ def main():
         res = reference_arm(args, rank, world)
         if res is not None:
             print(json.dumps(res), flush=True)
+        return
+    if args.mode != "single":
+        if rank == 0:
+            print(json.dumps(batch_mode(args) if args.mode == "batch" else serve_mode(args)), flush=True)
         return
     if world > 1:
         import datetime

@@ -105,7 +105,10 @@ void g2g_set_angular_grid_(const unsigned int* grid_type, const unsigned int* np
                            const double* e, const double* wang);
 
 /* Arithmetic of the two contractions (density and Kohn-Sham update):
- * 0 = FP64 on the CUDA cores (the plain form), 1 = tensor-core form. */
+ * 0 = FP64 on the CUDA cores (the plain form), 1 = tensor-core form,
+ * 2 = autotuned: after each grid upload one build of each form is timed and
+ * the faster kept (both meet the accuracy bar; small molecules, whose
+ * function tiles are mostly padding, often run faster in FP64). */
 void g2g_set_precision_(const unsigned int* mode);
 
 /* Partition statistics of the current grid: out[0] = groups, out[1] = cubes,

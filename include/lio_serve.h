@@ -58,8 +58,10 @@ typedef struct lio_molecule {
 } lio_molecule;
 
 /* A server on `device`. hbm_budget_bytes = 0 takes 90% of the free device
- * memory. precision: 0 FP64 form, 1 tensor-core form. max_inflight: requests
- * on the GPU at once (0 = 16). */
+ * memory. precision: 0 FP64 form, 1 tensor-core form, 2 autotuned per molecule
+ * (one build of each form timed at the molecule's first upload; the form with
+ * the smaller time x device-bytes product is kept, so residency is not spent on
+ * little speed). max_inflight: requests on the GPU at once (0 = 16). */
 lio_server* lio_srv_create(int device, unsigned long long hbm_budget_bytes, int precision, int max_inflight);
 void lio_srv_destroy(lio_server* srv);
 const char* lio_srv_last_error(lio_server* srv);
@@ -72,6 +74,10 @@ int lio_srv_add_molecule(lio_server* srv, const lio_molecule* mol);
  * until it has been resident once, measured after). */
 int lio_srv_molecule_info(lio_server* srv, int mol, long long* points, unsigned long long* footprint_bytes,
                           int* resident);
+
+/* The form a molecule runs in (0 FP64, 1 tensor core, -1 not yet uploaded)
+ * and, when autotuned, the measured ms per build of each form. */
+int lio_srv_molecule_form(lio_server* srv, int mol, int* form, double* fp64_ms, double* tc_ms);
 
 /* Submits one XC build. Closed shell: rho_a = the packed total density
  * (doubled off-diagonal elements, as rho_vec of g2g_parameter_init_), rho_b

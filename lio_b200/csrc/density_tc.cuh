@@ -88,30 +88,32 @@ __device__ __forceinline__ int8_t next_digit(double& x) {
 }
 
 // ---------------------------------------------------------------- A slices
-// Per geometry: one thread per (group, point) and kind; reads the FP64 basis
-// cache, writes the per-point exponent and the int8 slices. Layout per
-// 128-point tile T, kind a and 32-function K step kk: the S slices one after
-// the other (kTcStepA bytes, one bulk copy), each in the K-major interleaved
-// UMMA layout of a 128-row x 32-byte block.
+// Per geometry: one thread per (group, point) and kind; reads the blocked FP64
+// basis (NK kinds per block), writes the per-point exponent and the int8
+// slices. Layout per 128-point tile T, kind a and 32-function K step kk: the S
+// slices one after the other (kTcStepA bytes, one bulk copy), each in the
+// K-major interleaved UMMA layout of a 128-row x 32-byte block.
 template <int NA>
 __global__ void k_slice_basis(const int2* __restrict__ tiles, const GroupDev* __restrict__ groups,
-                              const double* __restrict__ basis, int8_t* __restrict__ aslices,
+                              const double* __restrict__ bblk, int NK, int8_t* __restrict__ aslices,
                               int16_t* __restrict__ aexp) {
   const int2 t = tiles[blockIdx.x];
   const GroupDev G = groups[t.x];
   const int r = threadIdx.x;
   const int p = t.y * kTcPoints + r;
-  const long long kstride = (long long)G.m * G.ldp;
   const int nks = G.m32 / 32;
+  // value (kind a, function j) of this point
+  auto val = [&](int a, int j) {
+    return bblk[G.bb_off + ((long long)(t.y * G.nftc + (j >> 5)) * NK + a) * kTcChunk + (j & 31) * kTcPoints + r];
+  };
   for (int a = 0; a < NA; a++) {
-    const double* src = basis + G.bas_off + a * kstride + p;
     double amax = 0.0;
-    for (int j = 0; j < G.m; j++) amax = fmax(amax, fabs(src[(long long)j * G.ldp]));
+    for (int j = 0; j < G.m; j++) amax = fmax(amax, fabs(val(a, j)));
     const int e = slice_exponent(amax);
     aexp[G.aexp_off + (long long)a * G.ldp + p] = (int16_t)e;
     int8_t* dst = aslices + G.sl_off + (long long)(t.y * NA + a) * nks * kTcStepA;
     for (int j = 0; j < G.m32; j++) {
-      double x = j < G.m ? ldexp(src[(long long)j * G.ldp], -e) : 0.0;
+      double x = j < G.m ? ldexp(val(a, j), -e) : 0.0;
       int8_t* blk = dst + (j >> 5) * kTcStepA + lio::umma::kmajor_offset(r, j & 31, kTcPoints);
       for (int s = 0; s < kSlices; s++) blk[s * kTcSliceA] = next_digit(x);
     }
@@ -155,27 +157,6 @@ __global__ void k_slice_density(const int2* __restrict__ tiles, const GroupDev* 
     }
     int8_t* blk = dst + (j >> 5) * kTcStepD;
     for (int s = 0; s < kSlices; s++) blk[lio::umma::kmajor_offset(s * kTcFuncs + r, j & 31, kTcTall)] = next_digit(x);
-  }
-}
-
-// ------------------------------------------------- blocked FP64 basis
-// Per geometry: the basis cache rearranged for the density epilogue: per group,
-// 128-point tile T, 32-function tile ft and kind k one contiguous chunk
-// [function i - 32 ft][point p - 128 T] (kTcChunk doubles) at
-// bb_off + ((T * nftc + ft) * NK + k) * kTcChunk; functions at or beyond m
-// are zeros. One CTA (128 threads = points) per (tile, ft * NK + k).
-__global__ void k_basis_block(const int2* __restrict__ tiles, const GroupDev* __restrict__ groups, int NK,
-                              const double* __restrict__ basis, double* __restrict__ bblk) {
-  const int2 t = tiles[blockIdx.x];
-  const GroupDev& G = groups[t.x];
-  const int ft = blockIdx.y / NK, k = blockIdx.y - ft * NK;
-  if (ft >= G.nftc) return;
-  const int p = t.y * kTcPoints + threadIdx.x;
-  const double* src = basis + G.bas_off + (long long)k * G.m * G.ldp + p;
-  double* dst = bblk + G.bb_off + ((long long)(t.y * G.nftc + ft) * NK + k) * kTcChunk + threadIdx.x;
-  for (int c = 0; c < kTcFuncs; c++) {
-    const int i = ft * kTcFuncs + c;
-    dst[c * kTcPoints] = i < G.m ? src[(long long)i * G.ldp] : 0.0;
   }
 }
 

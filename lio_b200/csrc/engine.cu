@@ -49,6 +49,7 @@ namespace {
 
 constexpr int kTile = 64;    // points / functions per GEMM tile
 constexpr int kPointPad = 128;  // points per group padded to a multiple of this
+constexpr int kTcChunkElems = 32 * 128;  // doubles of one (kind, 32-function, 128-point) block of the blocked basis
 constexpr int kKStep = 16;   // reduction step of the FP64 GEMMs
 constexpr int kBasisBlock = 128;
 constexpr int kFuncBlock = 128;
@@ -132,15 +133,22 @@ __global__ void k_basis(const int2* __restrict__ tiles, const GroupDev* __restri
                         const int* __restrict__ ncont, const double* __restrict__ ca,
                         const double* __restrict__ cc, const double* __restrict__ ax,
                         const double* __restrict__ ay, const double* __restrict__ az, double dnorm,
-                        int gga, double* __restrict__ basis) {
+                        int gga, double* __restrict__ basis, int nkb) {
   const int2 t = tiles[blockIdx.x];
   const GroupDev G = groups[t.x];
   const int p = t.y * kBasisBlock + threadIdx.x;
   if (p >= G.ldp) return;
   const bool valid = p < G.npts;
   const double x = px[G.pt_off + p], y = py[G.pt_off + p], z = pz[G.pt_off + p];
-  double* out = basis + G.bas_off;
-  const long long kstride = (long long)G.m * G.ldp;
+  // function-major cache (nkb = 0): value (kind, i, p) at bas_off + kind * m * ldp + i * ldp + p;
+  // blocked copy of the tensor-core density (nkb kinds): per (128-point tile, 32-function
+  // tile) the kinds one after the other, each [i mod 32][p mod 128]
+  double* out = basis + (nkb ? G.bb_off : G.bas_off);
+  const long long kstride = nkb ? (long long)kTcChunkElems : (long long)G.m * G.ldp;
+  auto at = [&](int i) {
+    return nkb ? ((long long)((p >> 7) * G.nftc + (i >> 5)) * nkb * kTcChunkElems + (i & 31) * 128 + (p & 127))
+               : (long long)i * G.ldp + p;
+  };
   int ii = 0;
   for (int sf = 0; sf < G.nsimple; sf++) {
     const int gf = sf_glob[G.sf_off + sf];
@@ -165,7 +173,7 @@ __global__ void k_basis(const int2* __restrict__ tiles, const GroupDev* __restri
       const int* l = c_comp_l[c0 + q];
       const double scale = (type == 2 && (q == 0 || q == 2 || q == 5)) ? dnorm : 1.0;
       const double P = ipow(r[0], l[0]) * ipow(r[1], l[1]) * ipow(r[2], l[2]);
-      const long long o = (long long)ii * G.ldp + p;
+      const long long o = at(ii);
       out[o] = valid ? scale * P * tt : 0.0;
       if (!gga) continue;
       double Pa[3];
@@ -534,6 +542,30 @@ struct DeviceEngine::Impl {
     graph_exec = nullptr;
     graph_key = -1;
   }
+  double tuned_fp64_ms = 0.0, tuned_tc_ms = 0.0;
+  long long basis_elems = 0, bblk_elems = 0;
+  double basis_norm = 1.0;
+  bool basis_valid = false;
+  // the function-major cache of the FP64 form, or (blocked) the tensor-core
+  // form's blocked copy; the padded functions of a blocked tile stay zero
+  void compute_basis(bool blocked = false) {
+    DevBuf<double>& dst = blocked ? bblk : basis;
+    if (blocked) {
+      bblk.alloc(bblk_elems);
+      LIO_CUDA(cudaMemsetAsync(bblk.p, 0, bblk_elems * sizeof(double), stream));
+    } else {
+      basis.alloc(basis_elems);
+    }
+    if (basis_tiles.n > 0 && ngroups > 0) {
+      k_basis<<<(unsigned)basis_tiles.n, kBasisBlock, 0, stream>>>(basis_tiles.p, groups.p, px.p, py.p, pz.p,
+                                                                    sf_glob.p, sf_type.p, nuc.p, ncont.p, ca.p, cc.p,
+                                                                    ax.p, ay.p, az.p, basis_norm, lda ? 0 : 1, dst.p,
+                                                                    blocked ? nk : 0);
+      LIO_CUDA(cudaGetLastError());
+    }
+    LIO_CUDA(cudaStreamSynchronize(stream));
+    if (!blocked) basis_valid = true;
+  }
   void free_pinned() {
     if (hK) cudaFreeHost(hK);
     if (hE) cudaFreeHost(hE);
@@ -599,6 +631,7 @@ DeviceEngine::~DeviceEngine() = default;
 void DeviceEngine::release() {
   Impl* d = impl_.get();
   d->basis.free();
+  d->basis_valid = false;
   d->part_a.free();
   d->part_b.free();
   d->ngroups = d->npoints = 0;
@@ -739,6 +772,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
     gd.push_back(G);
   }
   d->tc_sizes[0] = bb_off;
+  d->bblk_elems = bb_off;
   d->tc_sizes[1] = sl_off;
   d->tc_sizes[2] = aexp_off;
   d->tc_sizes[3] = ds_off;
@@ -798,11 +832,13 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
 
   const size_t npacked = (size_t)sys.M * (sys.M + 1) / 2;
   d->P_a.alloc(npacked);
+  LIO_CUDA(cudaMemset(d->P_a.p, 0, npacked * sizeof(double)));
   d->K_a.alloc(npacked);
   d->part_a.alloc(part_off);
   d->fac_a.alloc(pt_off);
   if (sys.open) {
     d->P_b.alloc(npacked);
+    LIO_CUDA(cudaMemset(d->P_b.p, 0, npacked * sizeof(double)));
     d->K_b.alloc(npacked);
     d->part_b.alloc(part_off);
     d->fac_b.alloc(pt_off);
@@ -821,15 +857,14 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
   LIO_CUDA(cudaMallocHost(&d->hErr, sizeof(int)));
   *d->hErr = 0;
 
-  // basis values, computed once per geometry and kept resident
-  d->basis.alloc(bas_off);
-  if (!btiles.empty()) {
-    k_basis<<<(unsigned)btiles.size(), kBasisBlock, 0, d->stream>>>(
-        d->basis_tiles.p, d->groups.p, d->px.p, d->py.p, d->pz.p, d->sf_glob.p, d->sf_type.p, d->nuc.p,
-        d->ncont.p, d->ca.p, d->cc.p, d->ax.p, d->ay.p, d->az.p, sys.d_norm, sys.lda ? 0 : 1, d->basis.p);
-    LIO_CUDA(cudaGetLastError());
-  }
-  LIO_CUDA(cudaStreamSynchronize(d->stream));
+  // basis values, computed once per geometry and kept resident (the tensor-core
+  // form drops them once its operands are built, and recomputes them if the
+  // FP64 form is asked for again)
+  d->basis_elems = bas_off;
+  d->basis_norm = sys.d_norm;
+  d->basis.free();
+  d->basis_valid = false;
+  if (precision_ == Precision::FP64) d->compute_basis();
 }
 
 // Builds the tensor-core operands of the current geometry: the blocked FP64
@@ -838,7 +873,11 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
 void DeviceEngine::prepare_tensor_core() {
   Impl* d = impl_.get();
   cudaStream_t st = d->stream;
-  d->bblk.alloc(d->tc_sizes[0]);
+  // the FP64 form's function-major cache is not needed (and not kept): every
+  // tensor-core operand is built from the blocked copy, computed directly
+  d->basis.free();
+  d->basis_valid = false;
+  d->compute_basis(true);
   d->aslices.alloc(d->tc_sizes[1]);
   d->aexp.alloc(d->tc_sizes[2]);
   d->dslices_a.alloc(d->tc_sizes[3]);
@@ -849,17 +888,12 @@ void DeviceEngine::prepare_tensor_core() {
   }
   d->tc_err.alloc(1);
   LIO_CUDA(cudaMemsetAsync(d->tc_err.p, 0, sizeof(int), st));
-  {
-    const dim3 grid((unsigned)d->slice_basis_tiles.n, (unsigned)(d->max_nftc * d->nk));
-    k_basis_block<<<grid, kTcPoints, 0, st>>>(d->slice_basis_tiles.p, d->groups.p, d->nk, d->basis.p, d->bblk.p);
-    LIO_CUDA(cudaGetLastError());
-  }
   if (d->lda)
     k_slice_basis<1><<<(unsigned)d->slice_basis_tiles.n, kTcPoints, 0, st>>>(d->slice_basis_tiles.p, d->groups.p,
-                                                                            d->basis.p, d->aslices.p, d->aexp.p);
+                                                                            d->bblk.p, 1, d->aslices.p, d->aexp.p);
   else
     k_slice_basis<4><<<(unsigned)d->slice_basis_tiles.n, kTcPoints, 0, st>>>(d->slice_basis_tiles.p, d->groups.p,
-                                                                            d->basis.p, d->aslices.p, d->aexp.p);
+                                                                            d->bblk.p, 10, d->aslices.p, d->aexp.p);
   LIO_CUDA(cudaGetLastError());
   d->fa_slices.alloc(d->fk_sizes[0]);
   d->fa_exp.alloc(d->fk_sizes[1]);
@@ -871,11 +905,12 @@ void DeviceEngine::prepare_tensor_core() {
   }
   {
     const int nrows = (int)d->fa_rows.n;
-    k_fock_rowexp<1><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(d->fa_rows.p, nrows, d->groups.p, d->basis.p,
-                                                                  nullptr, nullptr, d->fa_exp.p, nullptr, 0);
+    k_fock_rowexp<1><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(d->fa_rows.p, nrows, d->groups.p, d->bblk.p,
+                                                                  nullptr, nullptr, d->fa_exp.p, nullptr, 0, d->nk);
     LIO_CUDA(cudaGetLastError());
     k_fock_slices<kFkRows, false, 1><<<(unsigned)d->fa_tiles32.n, 256, 0, st>>>(
-        d->fa_tiles32.p, d->groups.p, d->basis.p, nullptr, nullptr, d->fa_exp.p, nullptr, d->fa_slices.p, nullptr, 0);
+        d->fa_tiles32.p, d->groups.p, d->bblk.p, nullptr, nullptr, d->fa_exp.p, nullptr, d->fa_slices.p, nullptr, 0,
+        d->nk);
     LIO_CUDA(cudaGetLastError());
   }
   LIO_CUDA(cudaFuncSetAttribute(k_fock_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FkCfg<1>::kSmem));
@@ -974,20 +1009,21 @@ int DeviceEngine::run_kernels(bool compute_rmm) {
       // f * F slices of both spins: row exponents, then the slices (one pass over F each)
       const int nrows = (int)d->fb_rows.n;
       if (d->open) {
-        k_fock_rowexp<2><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(d->fb_rows.p, nrows, d->groups.p, d->basis.p,
+        k_fock_rowexp<2><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(d->fb_rows.p, nrows, d->groups.p, d->bblk.p,
                                                                       d->fac_a.p, d->fac_b.p, d->fb_exp_a.p,
-                                                                      d->fb_exp_b.p, 1);
+                                                                      d->fb_exp_b.p, 1, d->nk);
         LIO_CUDA(cudaGetLastError());
         k_fock_slices<kFkCols, true, 2><<<(unsigned)d->fb_tiles32.n, 256, 0, st>>>(
-            d->fb_tiles32.p, d->groups.p, d->basis.p, d->fac_a.p, d->fac_b.p, d->fb_exp_a.p, d->fb_exp_b.p,
-            d->fb_slices_a.p, d->fb_slices_b.p, 1);
+            d->fb_tiles32.p, d->groups.p, d->bblk.p, d->fac_a.p, d->fac_b.p, d->fb_exp_a.p, d->fb_exp_b.p,
+            d->fb_slices_a.p, d->fb_slices_b.p, 1, d->nk);
       } else {
-        k_fock_rowexp<1><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(d->fb_rows.p, nrows, d->groups.p, d->basis.p,
-                                                                      d->fac_a.p, nullptr, d->fb_exp_a.p, nullptr, 1);
+        k_fock_rowexp<1><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(d->fb_rows.p, nrows, d->groups.p, d->bblk.p,
+                                                                      d->fac_a.p, nullptr, d->fb_exp_a.p, nullptr, 1,
+                                                                      d->nk);
         LIO_CUDA(cudaGetLastError());
         k_fock_slices<kFkCols, true, 1><<<(unsigned)d->fb_tiles32.n, 256, 0, st>>>(
-            d->fb_tiles32.p, d->groups.p, d->basis.p, d->fac_a.p, nullptr, d->fb_exp_a.p, nullptr, d->fb_slices_a.p,
-            nullptr, 1);
+            d->fb_tiles32.p, d->groups.p, d->bblk.p, d->fac_a.p, nullptr, d->fb_exp_a.p, nullptr, d->fb_slices_a.p,
+            nullptr, 1, d->nk);
       }
       LIO_CUDA(cudaGetLastError());
       launches += 2;
@@ -1033,6 +1069,65 @@ void DeviceEngine::prepare() {
 
 long long DeviceEngine::process_device_bytes() { return g_devbuf_bytes.load(); }
 
+void DeviceEngine::drop_tensor_core() {
+  Impl* d = impl_.get();
+  for (auto* b : {&d->aslices, &d->dslices_a, &d->dslices_b, &d->fa_slices, &d->fb_slices_a, &d->fb_slices_b})
+    b->free();
+  for (auto* b : {&d->aexp, &d->dexp_a, &d->dexp_b, &d->fa_exp, &d->fb_exp_a, &d->fb_exp_b}) b->free();
+  d->bblk.free();
+  d->tc_ready = false;
+  d->drop_graph();
+}
+
+// The autotuner: one resident build of each form after a warm-up (the density
+// contents do not change the work of either), the faster one kept and the
+// other's buffers released. Memory-aware (for many resident molecules): the
+// tensor-core form is kept only when its time x device-bytes product is the
+// smaller, so a form that buys little time with much more HBM (small groups,
+// whose 32-function tiles are mostly padding) does not crowd other molecules out.
+Precision DeviceEngine::autotune(bool memory_aware) {
+  Impl* d = impl_.get();
+  if (d->ngroups == 0) return precision_;
+  auto time_form = [&](Precision p) {
+    set_precision(p);
+    SolveRequest req;
+    req.resident = true;
+    solve(req);  // builds the form's operands and captures its graph
+    LIO_CUDA(cudaStreamSynchronize(d->stream));
+    cudaEvent_t a, b;
+    LIO_CUDA(cudaEventCreate(&a));
+    LIO_CUDA(cudaEventCreate(&b));
+    LIO_CUDA(cudaEventRecord(a, d->stream));
+    for (int k = 0; k < 2; k++) solve(req);
+    LIO_CUDA(cudaEventRecord(b, d->stream));
+    LIO_CUDA(cudaEventSynchronize(b));
+    float ms = 0.f;
+    LIO_CUDA(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ms;
+  };
+  const long long b0 = g_devbuf_bytes.load();
+  const float t64 = time_form(Precision::FP64);
+  const long long b64 = g_devbuf_bytes.load() - b0;
+  const float ttc = time_form(Precision::TensorCore);  // its operands replace the FP64 cache
+  const long long btc = g_devbuf_bytes.load() - b0;
+  d->tuned_fp64_ms = t64 / 2;
+  d->tuned_tc_ms = ttc / 2;
+  const bool tc_wins = memory_aware ? (double)ttc * (double)(btc + 1) < (double)t64 * (double)(b64 + 1) : ttc < t64;
+  if (!tc_wins) {
+    drop_tensor_core();
+    set_precision(Precision::FP64);
+    if (!d->basis_valid) d->compute_basis();
+  }
+  return precision_;
+}
+
+void DeviceEngine::tuned_times(double* fp64_ms, double* tc_ms) const {
+  *fp64_ms = impl_->tuned_fp64_ms;
+  *tc_ms = impl_->tuned_tc_ms;
+}
+
 size_t DeviceEngine::estimate_device_bytes(const System& sys, const Partition& part, Precision prec) {
   const int nk = sys.lda ? 1 : 10, na = sys.lda ? 1 : 4, nq = sys.lda ? 1 : kNQ, nspin = sys.open ? 2 : 1;
   const size_t npacked = (size_t)sys.M * (sys.M + 1) / 2;
@@ -1043,7 +1138,8 @@ size_t DeviceEngine::estimate_device_bytes(const System& sys, const Partition& p
     const int m = pg.total_functions(), m32 = (m + 31) / 32 * 32;
     const int nft = (m + kTile - 1) / kTile, nftc = (m + kTcFuncs - 1) / kTcFuncs;
     const int nI = (m + kFkRows - 1) / kFkRows, nJ = (m + kFkCols - 1) / kFkCols;
-    b += ldp * (nk * (double)m * 8 + 6 * 8 + nspin * (nq * (double)nft * 8 + 8));  // basis, points, partials, factors
+    b += ldp * (6 * 8 + nspin * (nq * (double)nft * 8 + 8));  // points, partials, factors
+    if (prec == Precision::FP64) b += ldp * nk * (double)m * 8;  // function-major basis cache
     if (prec == Precision::TensorCore)
       b += ldp * ((double)nftc * kTcFuncs * nk * 8 + (double)na * m32 * kSlices + na * 2 +
                   (double)nI * kFkRows * kSlices + (double)nspin * nJ * kFkCols * kSlices) +
@@ -1061,6 +1157,10 @@ void DeviceEngine::enqueue(const SolveRequest& req) {
   const bool tc = precision_ == Precision::TensorCore;
   if (tc && !d->tc_ready) {
     prepare_tensor_core();
+    d->drop_graph();
+  }
+  if (!tc && !d->basis_valid) {
+    d->compute_basis();
     d->drop_graph();
   }
   d->collect();
@@ -1196,6 +1296,7 @@ void DeviceEngine::solve_noalloc(const double* rho_a, const double* rho_b, doubl
   if (d->ngroups == 0) throw std::runtime_error("no grid uploaded");
   if (!rho_a || !fock_a || !energy || (d->open && (!rho_b || !fock_b)))
     throw std::runtime_error("null device pointer");
+  if (!d->basis_valid) d->compute_basis();  // allocates: only after a tensor-core solve dropped the cache
   double* scratch = noalloc_scratch_address();
   cudaStream_t st = cuda_stream ? (cudaStream_t)cuda_stream : d->stream;
   const int nspin = d->open ? 2 : 1;

@@ -88,6 +88,13 @@ class DeviceEngine {
   static bool available();
   // builds the tensor-core operands now (otherwise the first tensor-core solve does)
   void prepare();
+  // Times one build of this molecule in each form, keeps the faster (both meet
+  // the accuracy bar; memory_aware: the smaller time x device-bytes product)
+  // and releases the other's device buffers; returns it.
+  Precision autotune(bool memory_aware = false);
+  void tuned_times(double* fp64_ms, double* tc_ms) const;
+  // releases the tensor-core operands (rebuilt by the next tensor-core solve)
+  void drop_tensor_core();
   // device bytes held by all engines of the process, and an estimate of one
   // molecule's footprint before it is uploaded
   static long long process_device_bytes();

@@ -32,13 +32,22 @@ struct FkCfg {
 // Slices of the rows of v = F (A operand, per geometry) or v = f_s F (B
 // operand, per solve, both spins at once), in two passes over the FP64 basis.
 //
+// F(i, p) of a group and the values after it up to the end of its 128-point
+// tile: from the function-major basis cache (nkb = 0) or from the blocked copy
+// of the tensor-core density (nkb = its number of kinds; kind 0 is F)
+__device__ __forceinline__ const double* f_row(const GroupDev& G, const double* basis, int i, int p, int nkb) {
+  if (nkb == 0) return basis + G.bas_off + (long long)i * G.ldp + p;
+  return basis + G.bb_off + (long long)((p >> 7) * G.nftc + (i >> 5)) * nkb * kTcChunk + (i & 31) * kTcPoints +
+         (p & 127);
+}
+
 // Pass 1, one warp per (group, row): the row's exponent per spin from
 // max_p |v_p|. Rows at or beyond m get exponent 0 (their slices are zeros).
 template <int NS>
 __global__ void k_fock_rowexp(const int2* __restrict__ rows, int nrows, const GroupDev* __restrict__ groups,
                               const double* __restrict__ basis, const double* __restrict__ fac_a,
                               const double* __restrict__ fac_b, int16_t* __restrict__ expo_a,
-                              int16_t* __restrict__ expo_b, int use_sl_b) {
+                              int16_t* __restrict__ expo_b, int use_sl_b, int nkb) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (warp >= nrows) return;  // whole warps only
   const int2 t = rows[warp];
@@ -48,9 +57,8 @@ __global__ void k_fock_rowexp(const int2* __restrict__ rows, int nrows, const Gr
 #pragma unroll
   for (int sp = 0; sp < NS; sp++) amax[sp] = 0.0;
   if (i < G.m) {
-    const double* Fi = basis + G.bas_off + (long long)i * ldp;
     for (int p = lane; p < ldp; p += 32) {
-      const double v = Fi[p];
+      const double v = *f_row(G, basis, i, p, nkb);
 #pragma unroll
       for (int sp = 0; sp < NS; sp++) {
         const double* fac = sp == 0 ? fac_a : fac_b;
@@ -79,7 +87,7 @@ __global__ void __launch_bounds__(256) k_fock_slices(const int2* __restrict__ rt
                                                      const double* __restrict__ fac_b,
                                                      const int16_t* __restrict__ expo_a,
                                                      const int16_t* __restrict__ expo_b, int8_t* __restrict__ sl_a,
-                                                     int8_t* __restrict__ sl_b, int use_sl_b) {
+                                                     int8_t* __restrict__ sl_b, int use_sl_b, int nkb) {
   constexpr int kStep = kSlices * 32 * R;  // bytes of one K step of a row tile (either layout)
   const int2 t = rtiles[blockIdx.x];
   const GroupDev& G = groups[t.x];
@@ -92,13 +100,13 @@ __global__ void __launch_bounds__(256) k_fock_slices(const int2* __restrict__ rt
 #pragma unroll
   for (int sp = 0; sp < NS; sp++) sc[sp] = pow2(-(int)(sp == 0 ? expo_a : expo_b)[ebase + i]);
   const int tile = i / R, r = i % R;
-  const double* Fi = basis + G.bas_off + (long long)(valid ? i : 0) * ldp;
   for (int b = warp; b < ldp / 16; b += blockDim.x / 32) {
     const int p0 = b * 16;
+    const double* Fi = f_row(G, basis, valid ? i : 0, p0, nkb);  // 16 values within one 128-point tile
     double F[16];
 #pragma unroll
     for (int k = 0; k < 16; k += 2) {
-      const double2 v = valid ? *reinterpret_cast<const double2*>(Fi + p0 + k) : make_double2(0.0, 0.0);
+      const double2 v = valid ? *reinterpret_cast<const double2*>(Fi + k) : make_double2(0.0, 0.0);
       F[k] = v.x;
       F[k + 1] = v.y;
     }

@@ -56,6 +56,7 @@ struct State {
   bool device_ready = false;
   void* stream = nullptr;
   bool graphs = true;
+  bool auto_precision = false;
 };
 
 State& st() {
@@ -153,6 +154,7 @@ void build_grid(unsigned grid_type) {
   s.engine->set_graphs(s.graphs);
   s.engine->set_precision(s.precision);
   s.engine->upload(s.sys, s.part);
+  if (s.auto_precision) s.precision = s.engine->autotune();
   s.device_ready = true;
   s.last_grid_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -405,7 +407,13 @@ int g2g_last_error_(char* msg, const unsigned* len) {
 }
 
 void g2g_set_precision_(const unsigned* mode) {
-  st().precision = *mode == 1 ? lio::Precision::TensorCore : lio::Precision::FP64;
+  guarded("g2g_set_precision_", [&] {
+    State& s = st();
+    if (*mode > 2) throw std::runtime_error("precision mode must be 0 (FP64), 1 (tensor core) or 2 (autotuned)");
+    s.auto_precision = *mode == 2;
+    if (!s.auto_precision) s.precision = *mode == 1 ? lio::Precision::TensorCore : lio::Precision::FP64;
+    if (s.auto_precision && s.engine && s.device_ready) s.precision = s.engine->autotune();
+  });
 }
 
 void g2g_partition_stats_(long long* out) {

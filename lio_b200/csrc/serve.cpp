@@ -75,6 +75,8 @@ struct Molecule {
   std::unique_ptr<lio::DeviceEngine> engine;  // null while not resident
   unsigned long long footprint = 0;           // device bytes while resident
   bool measured = false;
+  int form = -1;  // the form it runs in (0 FP64, 1 tensor core) once resident
+  double tuned_ms[2] = {0.0, 0.0};
   bool busy = false;
   unsigned long long last_use = 0;
   long long points = 0;
@@ -98,6 +100,7 @@ struct Request {
 struct lio_server {
   int device = 0;
   lio::Precision precision = lio::Precision::TensorCore;
+  bool autotune = false;  // per molecule: the faster form, timed at its first upload
   int max_inflight = 16;
   unsigned long long budget = 0, used = 0;
   std::mutex mu;
@@ -125,8 +128,14 @@ struct lio_server {
 
 bool lio_server::admit(Molecule& m, std::string& why) {
   if (m.engine) return true;
+  // before the first upload: the estimate of its form (autotuned: the larger of
+  // the two, held one after the other while both are timed)
   const unsigned long long need =
-      m.measured ? m.footprint : (unsigned long long)lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, precision);
+      m.measured ? m.footprint
+      : autotune ? (unsigned long long)std::max(
+                       lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, lio::Precision::FP64),
+                       lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, lio::Precision::TensorCore))
+                 : (unsigned long long)lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, precision);
   std::vector<unsigned long long> fp, lu;
   std::vector<int> busy;
   for (auto& x : mols) {
@@ -147,10 +156,21 @@ bool lio_server::admit(Molecule& m, std::string& why) {
   }
   const long long before = lio::DeviceEngine::process_device_bytes();
   std::unique_ptr<lio::DeviceEngine> e(new lio::DeviceEngine());
-  e->set_precision(precision);
   e->set_graphs(true);
-  e->upload(m.sys, m.part);
-  e->prepare();
+  if (autotune && m.form >= 0) {  // decided at an earlier upload
+    e->set_precision(m.form ? lio::Precision::TensorCore : lio::Precision::FP64);
+    e->upload(m.sys, m.part);
+    e->prepare();
+  } else if (autotune) {
+    e->upload(m.sys, m.part);
+    m.form = e->autotune(true) == lio::Precision::TensorCore ? 1 : 0;
+    e->tuned_times(&m.tuned_ms[0], &m.tuned_ms[1]);
+  } else {
+    e->set_precision(precision);
+    e->upload(m.sys, m.part);
+    e->prepare();
+    m.form = precision == lio::Precision::TensorCore ? 1 : 0;
+  }
   const long long after = lio::DeviceEngine::process_device_bytes();
   m.footprint = (unsigned long long)std::max<long long>(after - before, 1);
   m.measured = true;
@@ -334,7 +354,8 @@ lio_server* lio_srv_create(int device, unsigned long long hbm_budget_bytes, int 
     }
     std::unique_ptr<lio_server> s(new lio_server());
     s->device = device;
-    s->precision = precision ? lio::Precision::TensorCore : lio::Precision::FP64;
+    s->precision = precision == 1 ? lio::Precision::TensorCore : lio::Precision::FP64;
+    s->autotune = precision == 2;
     s->max_inflight = max_inflight > 0 ? max_inflight : 16;
     size_t fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return nullptr;
@@ -396,6 +417,20 @@ int lio_srv_molecule_info(lio_server* srv, int mol, long long* points, unsigned 
     *footprint = m.measured ? m.footprint
                             : (unsigned long long)lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, srv->precision);
   if (resident) *resident = m.engine ? 1 : 0;
+  return 0;
+}
+
+int lio_srv_molecule_form(lio_server* srv, int mol, int* form, double* fp64_ms, double* tc_ms) {
+  if (!srv) return 1;
+  std::lock_guard<std::mutex> g(srv->mu);
+  if (mol < 0 || mol >= (int)srv->mols.size()) {
+    srv->error = "lio_srv_molecule_form: no such molecule";
+    return 1;
+  }
+  const Molecule& m = *srv->mols[mol];
+  if (form) *form = m.form;
+  if (fp64_ms) *fp64_ms = m.tuned_ms[0];
+  if (tc_ms) *tc_ms = m.tuned_ms[1];
   return 0;
 }
 

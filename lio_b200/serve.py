@@ -80,6 +80,8 @@ class XCServer:
         L.lio_srv_wait.argtypes = [C.c_void_p, C.c_longlong, C.POINTER(C.c_double), C.c_void_p, C.c_void_p,
                                    C.POINTER(C.c_double)]
         L.lio_srv_stats.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        L.lio_srv_molecule_form.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                            C.POINTER(C.c_double)]
         L.lio_srv_reset_stats.argtypes = [C.c_void_p]
         self.L = L
         self.h = L.lio_srv_create(device, budget_bytes, precision, max_inflight)
@@ -103,6 +105,13 @@ class XCServer:
         if self.L.lio_srv_molecule_info(self.h, mid, C.byref(pts), C.byref(fp), C.byref(res)):
             raise RuntimeError(self.error())
         return dict(points=pts.value, footprint=fp.value, resident=bool(res.value))
+
+    def form(self, mid: int):
+        """(form 0 FP64 / 1 tensor core / -1 not uploaded yet, tuned FP64 ms, tuned tensor-core ms)"""
+        f, a, b = C.c_int(0), C.c_double(0), C.c_double(0)
+        if self.L.lio_srv_molecule_form(self.h, mid, C.byref(f), C.byref(a), C.byref(b)):
+            raise RuntimeError(self.error())
+        return f.value, a.value, b.value
 
     def submit(self, mid: int, rho_a: np.ndarray, rho_b: np.ndarray | None = None) -> int:
         ra = np.ascontiguousarray(rho_a, dtype=np.float64)
@@ -181,41 +190,59 @@ def perturbed_density(wl: W.Workload, rng, eps: float = 1e-3):
     return wl.rho + eps * W.pack_lower(S, True)
 
 
-def serve_poisson(srv: XCServer, mids: list, rate_hz: float, duration_s: float, seed: int = 7):
+def serve_poisson(srv: XCServer, mids: list, rate_hz: float, duration_s: float, seed: int = 7,
+                  sample_frac: float = 0.01, waiters: int = 32):
     """Poisson arrivals at rate_hz over duration_s, each request for a random
-    resident molecule with a fresh perturbed density; returns the latencies (ms)
-    and the request/response pairs of a 1% sample for spot checks."""
+    registered molecule with a fresh perturbed density (P0 + 1e-3 S). Returns the
+    per-request latencies (ms, submit to result) and, for a sample_frac sample,
+    (molecule, density, E_xc, K) for spot checks against the FP64 form."""
+    import queue
+
     rng = np.random.default_rng(seed)
-    lat = []
-    sample = []
-    pending = []
+    lat, sample = [], []
     lock = threading.Lock()
+    todo = queue.Queue()
+
+    def waiter():
+        while True:
+            item = todo.get()
+            if item is None:
+                return
+            rid, mid, rho, keep = item
+            e, ka, _, ms = srv.wait(rid, mid)
+            with lock:
+                lat.append(ms)
+                if keep:
+                    sample.append((mid, rho, e, ka))
+
+    pool = [threading.Thread(target=waiter, daemon=True) for _ in range(waiters)]
+    for th in pool:
+        th.start()
     t_end = time.perf_counter() + duration_s
     t_next = time.perf_counter()
-
-    def waiter(rid, mid, rho, keep):
-        e, ka, _, ms = srv.wait(rid, mid)
-        with lock:
-            lat.append(ms)
-            if keep:
-                sample.append((mid, rho, e, ka))
-
-    threads = []
     while True:
         now = time.perf_counter()
         if now >= t_end:
             break
         if now < t_next:
-            time.sleep(min(t_next - now, 0.001))
+            time.sleep(min(t_next - now, 0.0005))
             continue
-        mid = int(rng.integers(len(mids)))
-        wl = srv.mols[mids[mid]][0]
-        rho = perturbed_density(wl, rng)
-        rid = srv.submit(mids[mid], rho)
-        th = threading.Thread(target=waiter, args=(rid, mids[mid], rho, rng.random() < 0.01))
-        th.start()
-        threads.append(th)
+        mid = mids[int(rng.integers(len(mids)))]
+        rho = perturbed_density(srv.mols[mid][0], rng)
+        todo.put((srv.submit(mid, rho), mid, rho, rng.random() < sample_frac))
         t_next += rng.exponential(1.0 / rate_hz)
-    for th in threads:
+    for _ in pool:
+        todo.put(None)
+    for th in pool:
         th.join()
     return lat, sample
+
+
+def run_all(srv: XCServer, mids: list, dens: dict):
+    """Submits one build per molecule at once and waits for all; returns {mid: (E, Ka, Kb)}."""
+    rids = [(srv.submit(m, *dens[m]), m) for m in mids]
+    out = {}
+    for rid, m in rids:
+        e, ka, kb, _ = srv.wait(rid, m)
+        out[m] = (e, ka, kb)
+    return out
