@@ -17,9 +17,10 @@ functional, E_xc, and accumulation into the packed Kohn-Sham matrices).
   e2e   : the same metric through the public C ABI (g2g_solve_groups_) with
           the caller's host arrays: density H2D, Kohn-Sham D2H and the +=
           into the caller's packed vectors inside the timed region.
-With --gpus N > 1 (one process per GPU under torchrun) every rank builds its
-own molecule of the same composition (seed offset by rank): molecules are
-independent, no collective is on the data path, scaling is weak.
+With --gpus N > 1 (one process per GPU under torchrun) the ranks share the one
+molecule: each builds its cost-balanced share of the groups (g2g_set_shard_)
+and one NCCL all-reduce of [E_xc, K] per build sums the shares (inside the
+timed region); total work is fixed, scaling is strong.
 
 --impl reference times the reference's own CPU g2g path (compiled from its
 sources by oracle/Makefile) on the same molecule with all host cores; the
@@ -131,10 +132,7 @@ def workload(rank: int, name: str = "cfg3") -> W.Workload:
     if name == "cfg2-open":  # the same 64 atoms, open-shell PBE (small case of the open-shell kernels)
         return W.make_workload("cfg2-open: 64 atoms 16C4N4O40H, 40x302, open PBE",
                                {"C": 16, "N": 4, "O": 4, "H": 40}, 14.0, 2000, 9, True, 302, 40)
-    if rank == 0:
-        return W.config(3)
-    return W.make_workload(f"cfg3-rank{rank}", {"C": 64, "N": 16, "O": 16, "H": 160}, 22.0, 3000 + 17 * rank, 9,
-                           True, 302, 40)
+    return W.config(3)
 
 
 def reference_arm(args, rank, world):
@@ -246,26 +244,51 @@ def ours(args, rank, world):
     lib.check("g2g_set_stream_")
     gt = bind(lib, wl)
     lib.set_precision(args.precision)
+    if world > 1:  # this rank's cost-balanced share of the molecule's groups
+        L.g2g_set_shard_(C.byref(C.c_int(rank)), C.byref(C.c_int(world)))
+        lib.check("g2g_set_shard_")
     t0 = time.perf_counter()
     msg = lib.reload_atom_positions(gt)
     if msg:
         raise RuntimeError(msg)
     grid_s = time.perf_counter() - t0
     st = lib.partition_stats()
-    npts = st["points"]
+    npts = st["points"]  # the whole molecule's points (the partition is built whole on every rank)
     npacked = wl.basis.M * (wl.basis.M + 1) // 2
     nspin = 2 if wl.open_shell else 1
+    # the N > 1 exchange: one all-reduce of [E_xc, K_alpha (, K_beta)] per build
+    red = torch.zeros(1 + nspin * npacked, dtype=torch.float64, device="cuda") if world > 1 else None
 
-    # end-to-end through the public ABI (host arrays, H2D + D2H + += inside)
+    def reduce_resident():
+        L.g2g_copy_resident_results_(C.c_void_p(red.data_ptr() + 8), C.c_void_p(red.data_ptr() + 8 + 8 * npacked)
+                                     if nspin == 2 else None, C.c_void_p(red.data_ptr()))
+        torch.distributed.all_reduce(red)
+
+    # end-to-end through the public ABI (host arrays, H2D + D2H + += inside; with
+    # N > 1 the shares are summed by an all-reduce of the host results)
+    host = torch.zeros(1 + nspin * npacked, dtype=torch.float64, pin_memory=True) if world > 1 else None
+
+    def e2e_step():
+        E = lib.solve_groups(0)
+        if world > 1:
+            host[0] = E
+            host[1:1 + npacked] = torch.from_numpy(lib.fock)
+            if nspin == 2:
+                host[1 + npacked:] = torch.from_numpy(lib.fockb)
+            dev_t = host.to("cuda", non_blocking=True)
+            torch.distributed.all_reduce(dev_t)
+            E = float(dev_t[0].cpu())
+        return E
+
     for _ in range(args.warmup):
-        lib.solve_groups(0)
+        e2e_step()
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        E = lib.solve_groups(0)
+        E = e2e_step()
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / args.steps
@@ -274,6 +297,8 @@ def ours(args, rank, world):
     L.g2g_solve_resident_.restype = C.c_int
     for _ in range(args.warmup):
         launches = L.g2g_solve_resident_()
+        if world > 1:
+            reduce_resident()
     lib.check("g2g_solve_resident_")
     if world > 1:
         torch.distributed.barrier()
@@ -282,6 +307,8 @@ def ours(args, rank, world):
         e0.record(stream)
         for _ in range(args.steps):
             L.g2g_solve_resident_()
+            if world > 1:
+                reduce_resident()
         e1.record(stream)
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
@@ -289,11 +316,7 @@ def ours(args, rank, world):
         t = torch.tensor([ms, e2e_ms], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms, e2e_ms = float(t[0]), float(t[1])
-        tot = torch.tensor([float(npts)], device="cuda")
-        torch.distributed.all_reduce(tot)
-        total_pts = float(tot[0])
-    else:
-        total_pts = float(npts)
+    total_pts = float(npts)
 
     # per-stage times (separate profiled pass: events between stages)
     stage_ms = stage_times(L, args.steps)
@@ -304,13 +327,21 @@ def ours(args, rank, world):
         lib.set_precision(0)
         for _ in range(args.warmup):
             L.g2g_solve_resident_()
+            if world > 1:
+                reduce_resident()
         torch.cuda.synchronize()
         e0.record(stream)
         for _ in range(args.steps):
             L.g2g_solve_resident_()
+            if world > 1:
+                reduce_resident()
         e1.record(stream)
         torch.cuda.synchronize()
         fp64_ms = e0.elapsed_time(e1) / args.steps
+        if world > 1:
+            t = torch.tensor([fp64_ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            fp64_ms = float(t[0])
         fp64_stage = stage_times(L, args.steps)
         fp64 = {"value": total_pts / (fp64_ms * 1e-3), "ms_per_step": fp64_ms,
                 "stage_ms": dict(zip(STAGES, fp64_stage))}
@@ -333,7 +364,8 @@ def ours(args, rank, world):
     traffic = measured_traffic(wl.name, tc)
     result = {
         "metric": METRIC, "value": total_pts / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "strong" if world > 1 else "weak",
         "vs_baseline": None, "dtype": "f64" if not tc else "i8-split/f64", "data": "synthetic",
         "config": {"workload": wl.name,
                    "points": npts, "groups": st["groups"], "M": wl.basis.M,

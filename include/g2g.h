@@ -139,6 +139,23 @@ void g2g_set_stream_(void* cuda_stream);
  * number of kernel launches it enqueued. */
 int g2g_solve_resident_(void);
 
+/* No counterpart in the reference, whose multi-GPU form shards groups inside
+ * one process (g2g/partition.cpp:441-511) and sums on the host (:516-574).
+ * Multi-GPU here is one process per GPU: g2g_set_shard_(rank, world) before a
+ * grid build makes this process upload and solve only its share of the groups
+ * (cost-balanced, longest processing time first on the reference's group cost);
+ * g2g_solve_groups_ then returns this share's E_xc and adds this share's
+ * Kohn-Sham contribution, and the caller sums both over the ranks (one
+ * all-reduce). g2g_shard_groups_ writes the owner rank of every group of the
+ * current partition (cubes, then spheres) and returns the group count.
+ * g2g_copy_resident_results_ copies the last resident solve's Kohn-Sham
+ * matrices (packed, per spin; beta may be NULL for closed shell) and energy
+ * into caller device buffers on the library's stream, for a device-side
+ * all-reduce. */
+void g2g_set_shard_(const int* rank, const int* world);
+int g2g_shard_groups_(const int* world, int* owner);
+void g2g_copy_resident_results_(double* d_fock_a, double* d_fock_b, double* d_energy);
+
 /* No counterpart in the reference: replay each solve's kernels from a CUDA
  * graph captured on the first solve after a new grid or precision (on by
  * default; 0 launches the kernels one by one). Profiled solves always launch

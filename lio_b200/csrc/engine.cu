@@ -656,7 +656,7 @@ int DeviceEngine::stage_times(double* ms, int max_stages, int* solves) const {
 }
 long long DeviceEngine::groups() const { return impl_->ngroups; }
 
-void DeviceEngine::upload(const System& sys, const Partition& part) {
+void DeviceEngine::upload(const System& sys, const Partition& part, const std::vector<char>* keep) {
   Impl* d = impl_.get();
   d->M = sys.M;
   d->natoms = sys.natoms;
@@ -684,6 +684,8 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
   const int NA = sys.lda ? 1 : 4;
   const int ngr = part.total_groups();
   for (int g = 0; g < ngr; g++) {
+    if (keep && !(*keep)[g]) continue;  // another rank's group
+    const int gdev = (int)gd.size();    // its index on this device
     const PointGroup& pg = part.group(g);
     GroupDev G{};
     G.npts = (int)pg.points.size();
@@ -708,13 +710,13 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
     G.fb_off = fb_off;
     G.fbe_off = fbe_off;
     const int nI = (G.m + kFkRows - 1) / kFkRows, nJ = (G.m + kFkCols - 1) / kFkCols;
-    for (int i = 0; i < nI * kFkRows; i++) farows.push_back({g, i});
-    for (int j = 0; j < nJ * kFkCols; j++) fbrows.push_back({g, j});
-    for (int i = 0; i < nI * kFkRows; i += 32) fat32.push_back({g, i});
-    for (int j = 0; j < nJ * kFkCols; j += 32) fbt32.push_back({g, j});
+    for (int i = 0; i < nI * kFkRows; i++) farows.push_back({gdev, i});
+    for (int j = 0; j < nJ * kFkCols; j++) fbrows.push_back({gdev, j});
+    for (int i = 0; i < nI * kFkRows; i += 32) fat32.push_back({gdev, i});
+    for (int j = 0; j < nJ * kFkCols; j += 32) fbt32.push_back({gdev, j});
     for (int I = 0; I < nI; I++)
       for (int J = 0; J < nJ; J++)
-        if (J * kFkCols + kFkCols - 1 >= I * kFkRows) fktiles.push_back({g, I, J, 0});
+        if (J * kFkCols + kFkCols - 1 >= I * kFkRows) fktiles.push_back({gdev, I, J, 0});
     for (int p = 0; p < G.ldp; p++) {
       if (p < G.npts) {
         const GridPoint& q = pg.points[p];
@@ -744,15 +746,15 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
         hfcp.push_back((int8_t)((c0 + k) | (normed ? 16 : 0)));
       }
     }
-    for (int b = 0; b < G.ldp / kBasisBlock + (G.ldp % kBasisBlock ? 1 : 0); b++) btiles.push_back({g, b});
-    for (int b = 0; b < (G.ldp + kFuncBlock - 1) / kFuncBlock; b++) ftiles.push_back({g, b});
+    for (int b = 0; b < G.ldp / kBasisBlock + (G.ldp % kBasisBlock ? 1 : 0); b++) btiles.push_back({gdev, b});
+    for (int b = 0; b < (G.ldp + kFuncBlock - 1) / kFuncBlock; b++) ftiles.push_back({gdev, b});
     for (int pt = 0; pt < G.ldp / kTile; pt++)
-      for (int ft = 0; ft < G.nft; ft++) dtiles.push_back({g, pt, ft, 0});
+      for (int ft = 0; ft < G.nft; ft++) dtiles.push_back({gdev, pt, ft, 0});
     for (int it = 0; it < G.nft; it++)
-      for (int jt = it; jt < G.nft; jt++) ktiles.push_back({g, it, jt, 0});
-    for (int T = 0; T < G.ldp / kTcPoints; T++) sbtiles.push_back({g, T});
+      for (int jt = it; jt < G.nft; jt++) ktiles.push_back({gdev, it, jt, 0});
+    for (int T = 0; T < G.ldp / kTcPoints; T++) sbtiles.push_back({gdev, T});
     maxm = std::max(maxm, G.m);
-    for (int ft = 0; ft < G.nftc; ft++) sdtiles.push_back({g, ft});
+    for (int ft = 0; ft < G.nftc; ft++) sdtiles.push_back({gdev, ft});
     pt_off += G.ldp;
     fn_off += G.m;
     sf_off += G.nsimple;
@@ -788,7 +790,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part) {
   d->fb_tiles32.upload(fbt32);
   d->fk_tiles.upload(fktiles);
   d->hgroups = gd;
-  d->ngroups = ngr;
+  d->ngroups = (long long)gd.size();
   d->npoints = npts_total;
   d->total_ldp = pt_off;
 
@@ -1058,6 +1060,16 @@ void DeviceEngine::set_graphs(bool on) {
   impl_->drop_graph();
 }
 void DeviceEngine::set_graphs_dirty() { impl_->drop_graph(); }
+
+void DeviceEngine::copy_results(double* d_fock_a, double* d_fock_b, double* d_energy) {
+  Impl* d = impl_.get();
+  const size_t npacked = (size_t)d->M * (d->M + 1) / 2;
+  if (d_fock_a)
+    LIO_CUDA(cudaMemcpyAsync(d_fock_a, d->K_a.p, npacked * sizeof(double), cudaMemcpyDeviceToDevice, d->stream));
+  if (d_fock_b && d->open)
+    LIO_CUDA(cudaMemcpyAsync(d_fock_b, d->K_b.p, npacked * sizeof(double), cudaMemcpyDeviceToDevice, d->stream));
+  if (d_energy) LIO_CUDA(cudaMemcpyAsync(d_energy, d->energy.p, sizeof(double), cudaMemcpyDeviceToDevice, d->stream));
+}
 
 void DeviceEngine::prepare() {
   if (precision_ == Precision::TensorCore && !impl_->tc_ready) {

@@ -43,9 +43,10 @@ class DeviceEngine {
   DeviceEngine(const DeviceEngine&) = delete;
   DeviceEngine& operator=(const DeviceEngine&) = delete;
 
-  // Uploads basis parameters, points and function lists; evaluates and caches
-  // the basis values of every group that fits the cache budget.
-  void upload(const System& sys, const Partition& part);
+  // Uploads basis parameters, points and function lists and evaluates the
+  // basis values; with `keep`, only the groups g with (*keep)[g] (this rank's
+  // shard of a multi-GPU build).
+  void upload(const System& sys, const Partition& part, const std::vector<char>* keep = nullptr);
   // One XC build: enqueue() puts all of its device work on the engine's stream
   // (density upload unless resident, the kernels, result download into pinned
   // buffers) and returns; ready() polls it; finish() waits for it and delivers
@@ -95,6 +96,9 @@ class DeviceEngine {
   void tuned_times(double* fp64_ms, double* tc_ms) const;
   // releases the tensor-core operands (rebuilt by the next tensor-core solve)
   void drop_tensor_core();
+  // device-to-device copy of the last resident solve's Kohn-Sham matrices and
+  // energy into caller buffers, on the engine's stream
+  void copy_results(double* d_fock_a, double* d_fock_b, double* d_energy);
   // device bytes held by all engines of the process, and an estimate of one
   // molecule's footprint before it is uploaded
   static long long process_device_bytes();

@@ -4,6 +4,7 @@
 // (g2g/init.cpp:27-33). Every entry point catches all exceptions: failures are
 // recorded in a sticky status (g2g_last_error_) and, at verbose > 0, printed;
 // nothing is thrown across the boundary and nothing calls exit().
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -57,6 +58,7 @@ struct State {
   void* stream = nullptr;
   bool graphs = true;
   bool auto_precision = false;
+  int shard_rank = 0, shard_world = 1;  // this process's share of the groups (multi-GPU)
 };
 
 State& st() {
@@ -133,6 +135,26 @@ void refresh_system() {
   }
 }
 
+// Cost-balanced assignment of the partition's groups to `world` ranks: longest
+// processing time first on the reference's group cost (g2g/partition.cpp:257-260),
+// each group to the least-loaded rank (ties to the lower rank).
+std::vector<int> shard_owners(const Partition& part, int world) {
+  const int ng = part.total_groups();
+  std::vector<int> order(ng), owner(ng, 0);
+  for (int g = 0; g < ng; g++) order[g] = g;
+  auto cost = [&](int g) { return part.group(g).cost(part.mincost); };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+  std::vector<long long> load(world, 0);
+  for (int g : order) {
+    int r = 0;
+    for (int k = 1; k < world; k++)
+      if (load[k] < load[r]) r = k;
+    owner[g] = r;
+    load[r] += cost(g);
+  }
+  return owner;
+}
+
 void build_grid(unsigned grid_type) {
   State& s = st();
   if (!s.params_set) throw std::runtime_error("g2g_parameter_init_ has not been called");
@@ -153,7 +175,14 @@ void build_grid(unsigned grid_type) {
   s.engine->set_stream(s.stream);
   s.engine->set_graphs(s.graphs);
   s.engine->set_precision(s.precision);
-  s.engine->upload(s.sys, s.part);
+  if (s.shard_world > 1) {
+    const std::vector<int> owner = shard_owners(s.part, s.shard_world);
+    std::vector<char> keep(owner.size());
+    for (size_t g = 0; g < owner.size(); g++) keep[g] = owner[g] == s.shard_rank;
+    s.engine->upload(s.sys, s.part, &keep);
+  } else {
+    s.engine->upload(s.sys, s.part);
+  }
   if (s.auto_precision) s.precision = s.engine->autotune();
   s.device_ready = true;
   s.last_grid_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -345,6 +374,34 @@ int g2g_solve_resident_(void) {
     n = s.engine->launches_per_solve();
   });
   return n;
+}
+
+void g2g_set_shard_(const int* rank, const int* world) {
+  guarded("g2g_set_shard_", [&] {
+    if (*world < 1 || *rank < 0 || *rank >= *world) throw std::runtime_error("shard rank must be in 0 .. world-1");
+    State& s = st();
+    s.shard_rank = *rank;
+    s.shard_world = *world;
+  });
+}
+
+int g2g_shard_groups_(const int* world, int* owner) {
+  int n = -1;
+  guarded("g2g_shard_groups_", [&] {
+    if (*world < 1) throw std::runtime_error("world must be >= 1");
+    const std::vector<int> o = shard_owners(st().part, *world);
+    for (size_t g = 0; g < o.size(); g++) owner[g] = o[g];
+    n = (int)o.size();
+  });
+  return n;
+}
+
+void g2g_copy_resident_results_(double* d_fock_a, double* d_fock_b, double* d_energy) {
+  guarded("g2g_copy_resident_results_", [&] {
+    State& s = st();
+    if (!s.engine || !s.device_ready) throw std::runtime_error("no device grid");
+    s.engine->copy_results(d_fock_a, d_fock_b, d_energy);
+  });
 }
 
 void g2g_set_graphs_(const unsigned* on) {

@@ -766,13 +766,40 @@ static double solve_group(const oracle_system* s, const group_t* g, const double
   return energy;
 }
 
+static int solve_groups_list(const oracle_system* s, const double* rho, const double* rho_a, const double* rho_b,
+                             double* fock, double* fockb, double* energy, long long* npoints, long long* ngroups,
+                             int first, int stride, const int* ids, int nids);
+
 int oracle_solve_sample(const oracle_system* s, const double* rho, const double* rho_a, const double* rho_b,
                         double* fock, double* fockb, double* energy, long long* npoints, long long* ngroups,
                         int first, int stride) {
+  return solve_groups_list(s, rho, rho_a, rho_b, fock, fockb, energy, npoints, ngroups, first, stride, NULL, 0);
+}
+
+int oracle_solve_subset(const oracle_system* s, const double* rho, const double* rho_a, const double* rho_b,
+                        double* fock, double* fockb, double* energy, long long* npoints, long long* ngroups,
+                        const int* group_ids, int nids) {
+  if (!group_ids || nids < 0) return -1;
+  return solve_groups_list(s, rho, rho_a, rho_b, fock, fockb, energy, npoints, ngroups, 0, 1, group_ids, nids);
+}
+
+/* Groups first, first + stride, ... or, when ids != NULL, exactly ids[0 .. nids) (the
+ * partition's order: cubes, then spheres, each sorted by cost). */
+static int solve_groups_list(const oracle_system* s, const double* rho, const double* rho_a, const double* rho_b,
+                             double* fock, double* fockb, double* energy, long long* npoints, long long* ngroups,
+                             int first, int stride, const int* ids, int nids) {
   if (!s || s->natoms <= 0 || s->M <= 0 || stride <= 0) return -1;
   if (s->open && (!rho_a || !rho_b || !fockb)) return -2;
   int ng = 0;
   group_t* gs = build_groups(s, &ng);
+  int* list = (int*)malloc(sizeof(int) * ((size_t)ng + 1));
+  int nl = 0;
+  if (ids) {
+    for (int k = 0; k < nids; k++)
+      if (ids[k] >= 0 && ids[k] < ng) list[nl++] = ids[k];
+  } else {
+    for (int gi = first; gi < ng; gi += stride) list[nl++] = gi;
+  }
   const size_t np = (size_t)s->M * (s->M + 1) / 2;
   double* eg = (double*)calloc((size_t)ng + 1, sizeof(double));
   int nth = 1;
@@ -785,7 +812,8 @@ int oracle_solve_sample(const oracle_system* s, const double* rho, const double*
   double* Kb = s->open ? (double*)calloc(np * (size_t)nth, sizeof(double)) : NULL;
   long long pts = 0, used = 0;
 #pragma omp parallel for schedule(dynamic, 1) reduction(+ : pts, used)
-  for (int gi = first; gi < ng; gi += stride) {
+  for (int li = 0; li < nl; li++) {
+    const int gi = list[li];
     int t = 0;
 #ifdef _OPENMP
     t = omp_get_thread_num();
@@ -814,6 +842,7 @@ int oracle_solve_sample(const oracle_system* s, const double* rho, const double*
   free(eg);
   free(Ka);
   free(Kb);
+  free(list);
   return 0;
 }
 

@@ -49,6 +49,12 @@ int oracle_solve_sample(const oracle_system* s, const double* rho, const double*
                         double* fock, double* fockb, double* energy, long long* npoints, long long* ngroups,
                         int first, int stride);
 
+/* Same, restricted to the listed groups (indices in the partition's order:
+ * cubes, then spheres, each sorted by cost); for checking a sharded build. */
+int oracle_solve_subset(const oracle_system* s, const double* rho, const double* rho_a, const double* rho_b,
+                        double* fock, double* fockb, double* energy, long long* npoints, long long* ngroups,
+                        const int* group_ids, int nids);
+
 #ifdef __cplusplus
 }
 #endif

@@ -88,8 +88,9 @@ def _dp(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
-def restatement(wl, first=0, stride=1, options=None):
-    """(E, fock, fockb, npoints) from the C restatement (oracle/liboracle.so)."""
+def restatement(wl, first=0, stride=1, options=None, groups=None):
+    """(E, fock, fockb, npoints) from the C restatement (oracle/liboracle.so);
+    with `groups`, only those groups (partition order) are built."""
     L = _libs.get("oracle")
     if L is None:
         L = C.CDLL(ORACLE_LIB)
@@ -126,13 +127,19 @@ def restatement(wl, first=0, stride=1, options=None):
     E = C.c_double(0)
     npts, ngr = C.c_longlong(0), C.c_longlong(0)
     if wl.open_shell:
-        ra, rb = np.ascontiguousarray(wl.rho_a), np.ascontiguousarray(wl.rho_b)
-        rc = L.oracle_solve_sample(C.byref(s), None, _dp(ra), _dp(rb), _dp(fock), _dp(fockb), C.byref(E),
-                                   C.byref(npts), C.byref(ngr), first, stride)
+        dens = (None, _dp(np.ascontiguousarray(wl.rho_a)), _dp(np.ascontiguousarray(wl.rho_b)))
+        keep["ra"], keep["rb"] = wl.rho_a, wl.rho_b
     else:
         r = np.ascontiguousarray(wl.rho)
-        rc = L.oracle_solve_sample(C.byref(s), _dp(r), None, None, _dp(fock), _dp(fockb), C.byref(E),
-                                   C.byref(npts), C.byref(ngr), first, stride)
+        keep["r"] = r
+        dens = (_dp(r), None, None)
+    if groups is not None:
+        ids = np.ascontiguousarray(np.asarray(groups, dtype=np.int32))
+        rc = L.oracle_solve_subset(C.byref(s), *dens, _dp(fock), _dp(fockb), C.byref(E), C.byref(npts),
+                                   C.byref(ngr), ids.ctypes.data_as(C.POINTER(C.c_int)), len(ids))
+    else:
+        rc = L.oracle_solve_sample(C.byref(s), *dens, _dp(fock), _dp(fockb), C.byref(E), C.byref(npts),
+                                   C.byref(ngr), first, stride)
     assert rc == 0, rc
     return E.value, fock, fockb, npts.value
 
