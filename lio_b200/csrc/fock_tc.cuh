@@ -43,6 +43,9 @@ __device__ __forceinline__ const double* f_row(const GroupDev& G, const double* 
 
 // Pass 1, one warp per (group, row): the row's exponent per spin from
 // max_p |v_p|. Rows at or beyond m get exponent 0 (their slices are zeros).
+// The row is read a 128-point tile at a time, four consecutive points per lane
+// (two 16-byte loads of F and of each spin's factors), two tiles in flight.
+static_assert(kPointPad % kTcPoints == 0, "rows are read in whole 128-point tiles");
 template <int NS>
 __global__ void k_fock_rowexp(const int2* __restrict__ rows, int nrows, const GroupDev* __restrict__ groups,
                               const double* __restrict__ basis, const double* __restrict__ fac_a,
@@ -52,17 +55,28 @@ __global__ void k_fock_rowexp(const int2* __restrict__ rows, int nrows, const Gr
   if (warp >= nrows) return;  // whole warps only
   const int2 t = rows[warp];
   const GroupDev& G = groups[t.x];
-  const int i = t.y, ldp = G.ldp;
+  const int i = t.y, ntl = G.ldp / kTcPoints;
   double amax[NS];
 #pragma unroll
   for (int sp = 0; sp < NS; sp++) amax[sp] = 0.0;
   if (i < G.m) {
-    for (int p = lane; p < ldp; p += 32) {
-      const double v = *f_row(G, basis, i, p, nkb);
+#pragma unroll 2
+    for (int T = 0; T < ntl; T++) {
+      const int p = T * kTcPoints + lane * 4;
+      const double* Fi = f_row(G, basis, i, p, nkb);
+      const double2 v01 = *reinterpret_cast<const double2*>(Fi);
+      const double2 v23 = *reinterpret_cast<const double2*>(Fi + 2);
 #pragma unroll
       for (int sp = 0; sp < NS; sp++) {
         const double* fac = sp == 0 ? fac_a : fac_b;
-        amax[sp] = fmax(amax[sp], fabs(fac ? v * fac[G.pt_off + p] : v));
+        double f0 = 1.0, f1 = 1.0, f2 = 1.0, f3 = 1.0;
+        if (fac) {
+          const double2 a01 = *reinterpret_cast<const double2*>(fac + G.pt_off + p);
+          const double2 a23 = *reinterpret_cast<const double2*>(fac + G.pt_off + p + 2);
+          f0 = a01.x, f1 = a01.y, f2 = a23.x, f3 = a23.y;
+        }
+        amax[sp] = fmax(amax[sp], fmax(fmax(fabs(v01.x * f0), fabs(v01.y * f1)),
+                                       fmax(fabs(v23.x * f2), fabs(v23.y * f3))));
       }
     }
   }

@@ -109,6 +109,8 @@ LIO_HD inline void pw92_g(const PW92Set& s, double rtrs, double& g, double& dgdr
 #define LIO_F43 ((double)(4.0f / 3.0f))
 #define LIO_F13 ((double)(1.0f / 3.0f))
 #define LIO_FM16 ((double)(-1.0f / 6.0f))
+// pow(2.0, 4.0 / 3.0) - 2.0 as the C library evaluates it (pbeOS_corr.h)
+#define LIO_GAM 0x1.0a28be635ca2cp-1
 
 // ---------------------------------------------------- PBE closed shell (pbeCS.h)
 struct GgaOut {
@@ -210,10 +212,10 @@ LIO_HD inline GgaOut pbe_closed(double dens, const double g[3], const double h1[
 }
 
 // ----------------------------------------------------- PBE open shell (pbeOS_*.h)
-LIO_HD inline void pbe_exchange_spin(double rho, double s, double u, double v, double& ex, double& vx) {
+// rho13 = cbrt(rho) of the spin-doubled density (pbeOS_exch.h:42-75 takes rho)
+LIO_HD inline void pbe_exchange_spin(double rho13, double s, double u, double v, double& ex, double& vx) {
   const double AX = LIO_F(-0.738558766382022405884230032680836f);
   const double UM = LIO_F(0.2195149727645171f), UK = LIO_F(0.804f), UL = LIO_F(0.273028573090195f);
-  const double rho13 = cbrt(rho);
   const double exunif = AX * rho13;
   const double s2 = s * s, s3 = s * s2;
   const double p0 = 1.0 + UL * s2;
@@ -224,8 +226,10 @@ LIO_HD inline void pbe_exchange_spin(double rho, double s, double u, double v, d
   vx = exunif * (LIO_F43 * fxpbe - (u - LIO_F43 * s3) * Fss - v * Fs);
 }
 
-LIO_HD inline void pbe_correlation_spin(double rs, double zet, double t, double uu, double vv, double ww,
-                                        double& ec, double& vc_a, double& vc_b, double& h,
+// cp, cm = cbrt(1 + zet), cbrt(1 - zet); every (1 +- zet)^(k/3) of the
+// reference's pbeOS_corr.h is formed from them by products.
+LIO_HD inline void pbe_correlation_spin(double rs, double zet, double cp, double cm, double t, double uu, double vv,
+                                        double ww, double& ec, double& vc_a, double& vc_b, double& h,
                                         double& dvc_a, double& dvc_b) {
   const double GAMMA = LIO_F(0.03109069086965489503494086371273f);
   const double BETA = LIO_F(0.06672455060314922f);
@@ -237,22 +241,21 @@ LIO_HD inline void pbe_correlation_spin(double rs, double zet, double t, double 
   pw92_g(pw92_set(2), rtrs, EP, EPRS);
   pw92_g(pw92_set(3), rtrs, ALFM, ALFRSM);
   const double Z2 = zet * zet, Z4 = Z2 * Z2;
-  const double ZET1 = cbrt(pow(1.0 + zet, 4));
-  const double ZET2 = cbrt(pow(1.0 - zet, 4));
-  const double GAM = pow(2.0, 4.0 / 3.0) - 2.0;
+  const double zp = 1.0 + zet, zm = 1.0 - zet, zp2 = zp * zp, zm2 = zm * zm;
+  const double ZET1 = zp * cp, ZET2 = zm * cm;  // (1 +- zet)^(4/3)
+  const double GAM = LIO_GAM;
   const double F = (ZET1 + ZET2 - 2.0) / GAM;
   const double FZZ = 8.0 / (9.0 * GAM);
   ec = EU * (1.0 - F * Z4) + EP * F * Z4 - ALFM * F * (1.0 - Z4) / FZZ;
   const double ECRS = EURS * (1.0 - F * Z4) + EPRS * F * Z4 - ALFRSM * F * (1.0 - Z4) / FZZ;
-  const double ZET3 = cbrt(1.0 + zet), ZET4 = cbrt(1.0 - zet);
+  const double ZET3 = cp, ZET4 = cm;
   const double FZ = LIO_F43 * (ZET3 - ZET4) / GAM;
-  const double ECZET = 4.0 * pow(zet, 3) * F * (EP - EU + ALFM / FZZ) + FZ * (Z4 * EP - Z4 * EU - (1.0 - Z4) * ALFM / FZZ);
+  const double ECZET = 4.0 * (Z2 * zet) * F * (EP - EU + ALFM / FZZ) + FZ * (Z4 * EP - Z4 * EU - (1.0 - Z4) * ALFM / FZZ);
   double COMM = ec - rs * ECRS / 3.0 - zet * ECZET;
   vc_a = COMM + ECZET;
   vc_b = COMM - ECZET;
-  const double ZET5 = cbrt(pow(1.0 + zet, 2)), ZET6 = cbrt(pow(1.0 - zet, 2));
-  const double G = (ZET5 + ZET6) / 2.0;
-  const double G3 = pow(G, 3);
+  const double G = (cp * cp + cm * cm) / 2.0;  // ((1+zet)^(2/3) + (1-zet)^(2/3)) / 2
+  const double G3 = G * G * G;
   const double PON = -ec / (G3 * GAMMA);
   const double B = DELTA / (exp(PON) - 1.0);
   const double B2 = B * B;
@@ -263,13 +266,13 @@ LIO_HD inline void pbe_correlation_spin(double rs, double zet, double t, double 
   const double G4 = G3 * G;
   const double T6 = T4 * T2;
   const double rsthrd = rs / 3.0;
-  const double GZ1 = pow(pow(1.0 + zet, 2) + ETA, LIO_FM16);
-  const double GZ2 = pow(pow(1.0 - zet, 2) + ETA, LIO_FM16);
+  const double GZ1 = pow(zp2 + ETA, LIO_FM16);
+  const double GZ2 = pow(zm2 + ETA, LIO_FM16);
   const double GZ = (GZ1 - GZ2) / 3.0;
   const double FAC = DELTA / B + 1.0;
   const double BG = -3.0 * B2 * ec * FAC / (BETA * G4);
   const double BEC = B2 * FAC / (BETA * G3);
-  const double Q8 = pow(Q5, 2) + DELTA * Q4 * Q5 * T2;
+  const double Q8 = Q5 * Q5 + DELTA * Q4 * Q5 * T2;
   const double Q9 = 1.0 + 2.0 * B * T2;
   const double hB = -BETA * G3 * B * (T6 / Q8) * (2.0 + B * T2);
   const double hRS = -rsthrd * hB * BEC * ECRS;
@@ -297,10 +300,11 @@ struct GgaOpenOut {
 
 LIO_HD inline void spin_scalars(const double g[3], const double h1[3], const double h2[3], double& dgrad,
                                 double& delgrad, double& rlap) {
-  const double grad2 = pow(g[0], 2) + pow(g[1], 2) + pow(g[2], 2);
+  const double gx2 = g[0] * g[0], gy2 = g[1] * g[1], gz2 = g[2] * g[2];
+  const double grad2 = gx2 + gy2 + gz2;
   dgrad = sqrt(grad2);
-  delgrad = (pow(g[0], 2) * h1[0] + 2.0 * g[0] * g[1] * h2[0] + 2.0 * g[1] * g[2] * h2[2] +
-             2.0 * g[0] * g[2] * h2[1] + pow(g[1], 2) * h1[1] + pow(g[2], 2) * h1[2]) /
+  delgrad = (gx2 * h1[0] + 2.0 * g[0] * g[1] * h2[0] + 2.0 * g[1] * g[2] * h2[2] + 2.0 * g[0] * g[2] * h2[1] +
+             gy2 * h1[1] + gz2 * h1[2]) /
             dgrad;
   rlap = h1[0] + h1[1] + h1[2];
 }
@@ -313,16 +317,19 @@ LIO_HD inline GgaOpenOut pbe_open(double da, double db, const double ga[3], cons
   const double MIN_RHO = 1e-18;
   if (!((da > MIN_RHO) || (db > MIN_RHO))) return o;
   const double PI_F = LIO_F(3.141592653589793238462643383279f);
-  const double PI32 = LIO_F(29.608813203268075856503472999628f);
+  // cbrt(PI32) and cbrt(9 PI_F / 4) with PI32 = (double)(float)(3 pi^2) and
+  // PI_F = (double)(float)pi, the values the C library's cbrt gives
+  const double CBRT_PI32 = 0x1.8bfd4d9560ebcp+1, CBRT_ALPHA = 0x1.eb4df5835af6bp+0;
   double dgrad_a, delgrad_a, rlap_a, dgrad_b, delgrad_b, rlap_b;
   spin_scalars(ga, h1a, h2a, dgrad_a, delgrad_a, rlap_a);
   spin_scalars(gb, h1b, h2b, dgrad_b, delgrad_b, rlap_b);
   const double g[3] = {ga[0] + gb[0], ga[1] + gb[1], ga[2] + gb[2]};
   const double h1[3] = {h1a[0] + h1b[0], h1a[1] + h1b[1], h1a[2] + h1b[2]};
   const double h2[3] = {h2a[0] + h2b[0], h2a[1] + h2b[1], h2a[2] + h2b[2]};
-  const double grad2 = pow(g[0], 2) + pow(g[1], 2) + pow(g[2], 2);
+  const double gx2 = g[0] * g[0], gy2 = g[1] * g[1], gz2 = g[2] * g[2];
+  const double grad2 = gx2 + gy2 + gz2;
   const double dgrad = sqrt(grad2);
-  const double delgrad = (pow(g[0], 2) * h1[0] + pow(g[1], 2) * h1[1] + pow(g[2], 2) * h1[2] +
+  const double delgrad = (gx2 * h1[0] + gy2 * h1[1] + gz2 * h1[2] +
                           2.0 * g[0] * g[1] * h2[0] + 2.0 * g[1] * g[2] * h2[2] + 2.0 * g[0] * g[2] * h2[1]) /
                          dgrad;
   // exchange by exact spin scaling: Ex[a,b] = (Ex[2a] + Ex[2b]) / 2
@@ -333,15 +340,16 @@ LIO_HD inline GgaOpenOut pbe_open(double da, double db, const double ga[3], cons
     const double twodens = 2.0 * dens[sp];
     if (twodens > MIN_RHO) {
       const double twodens2 = twodens * twodens;
-      const double fk = cbrt(PI32) * cbrt(twodens);
+      const double td13 = cbrt(twodens);
+      const double fk = CBRT_PI32 * td13;
       const double twofk = 2.0 * fk, twofk2 = twofk * twofk, twofk3 = twofk * twofk2;
       const double s = (2.0 * dg[sp]) / (twodens * twofk);
       const double v = (2.0 * lp[sp]) / (twodens * twofk2);
       const double u = (4.0 * dl[sp]) / (twodens2 * twofk3);
       if (sp == 0)
-        pbe_exchange_spin(twodens, s, u, v, ex_a, vx_a);
+        pbe_exchange_spin(td13, s, u, v, ex_a, vx_a);
       else
-        pbe_exchange_spin(twodens, s, u, v, ex_b, vx_b);
+        pbe_exchange_spin(td13, s, u, v, ex_b, vx_b);
     }
   }
   const double rho = da + db;
@@ -350,11 +358,10 @@ LIO_HD inline GgaOpenOut pbe_open(double da, double db, const double ga[3], cons
   o.vb = vx_b;
   if (rho < (MIN_RHO * 1e5)) return o;
   const double zet = (da - db) / rho;
-  const double g1 = 1.0 + zet, g2 = 1.0 - zet;
-  const double gphi = (cbrt(g1 * g1) + cbrt(g2 * g2)) / 2.0;
-  const double fk = cbrt(PI32) * cbrt(rho);
-  const double alpha = (9.0 * PI_F) / 4.0;
-  const double rs = cbrt(alpha) / fk;
+  const double cp = cbrt(1.0 + zet), cm = cbrt(1.0 - zet);
+  const double gphi = (cp * cp + cm * cm) / 2.0;
+  const double fk = CBRT_PI32 * cbrt(rho);
+  const double rs = CBRT_ALPHA / fk;
   const double sk = sqrt(4.0 * fk / PI_F);
   const double twoksg = 2.0 * sk * gphi;
   const double t = dgrad / (twoksg * rho);
@@ -364,7 +371,7 @@ LIO_HD inline GgaOpenOut pbe_open(double da, double db, const double ga[3], cons
   const double den = (rho * rho) * (twoksg * twoksg);
   const double ww = num / den;
   double ec, vc_a, vc_b, h, dvc_a, dvc_b;
-  pbe_correlation_spin(rs, zet, t, uu, vv, ww, ec, vc_a, vc_b, h, dvc_a, dvc_b);
+  pbe_correlation_spin(rs, zet, cp, cm, t, uu, vv, ww, ec, vc_a, vc_b, h, dvc_a, dvc_b);
   o.ec = ec + h;
   o.va = vx_a + vc_a + dvc_a;
   o.vb = vx_b + vc_b + dvc_b;
@@ -374,6 +381,7 @@ LIO_HD inline GgaOpenOut pbe_open(double da, double db, const double ga[3], cons
 #undef LIO_F43
 #undef LIO_F13
 #undef LIO_FM16
+#undef LIO_GAM
 #undef LIO_F
 
 }  // namespace xc
