@@ -74,7 +74,13 @@ void g2g_reload_atom_positions_(const unsigned int* grid_type);
 void g2g_new_grid_(const unsigned int* grid_type);
 
 /* g2g/init.cpp:332-391 (g2g_solve_groups_): computation_type 0 = Fock (RMM)
- * update, 1 = energy only, 2 = energy + forces, 3 = forces only. */
+ * update, 1 = energy only, 2 = energy + forces, 3 = forces only. The energy is
+ * written (0 when not computed); the Kohn-Sham vectors bound at parameter_init
+ * are added to (type 0 only); types 2 and 3 add each atom's XC force into
+ * fort_forces_ptr, natoms x 3 column-major with leading dimension max_atoms
+ * (g2g/partition.cpp:516-526), with the reference's CPU formula
+ * (g2g/cpu/iteration.cpp:213-267, open shell 496-563) evaluated in FP64 from
+ * the per-point factors of the build (whose form set_precision selects). */
 void g2g_solve_groups_(const unsigned int* computation_type, double* fort_energy_ptr,
                        double* fort_forces_ptr);
 

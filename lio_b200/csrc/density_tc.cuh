@@ -312,6 +312,14 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
     consumed = 0;
     bconsumed = 0;
   }
+  {
+    // The basis ring starts zeroed: a chunk of a group's last function tile is
+    // copied for its m - 32 ft valid functions only, and the rows after them
+    // keep the finite values of earlier chunks, which meet G = 0 in the dots.
+    double* ring = reinterpret_cast<double*>(tc_smem + Cfg::kBRing);
+    for (int i = tid; i < kBStages * kTcChunk; i += blockDim.x) ring[i] = 0.0;
+    lio::umma::fence_proxy_async_smem();
+  }
   lio::umma::fence_before_sync();
   __syncthreads();
   lio::umma::fence_after_sync();
@@ -367,15 +375,17 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
         for (int tt = 0; tt < nft * NP && !*vfail; tt++) {
           const int ft = tt / NP, first = (tt - ft * NP) * KP;
           const double* src = bblk + G.bb_off + (long long)(t.y * nft + ft) * NK * kTcChunk;
+          // rows (functions) of the chunk that exist: 1 KB each, contiguous from row 0
+          const uint32_t bytes = (uint32_t)min(kTcFuncs, G.m - ft * kTcFuncs) * kTcPoints * 8;
           for (int k = unit_klo(first); k <= unit_khi(first, NK); k++, cnt++) {
             const int buf = cnt % kBStages, use = cnt / kBStages;
             if (use > 0 && (*vfail || !lio::umma::mbar_wait(&bempty[buf], (use - 1) & 1))) {
               *vfail = 1;
               break;
             }
-            lio::umma::mbar_expect_tx(&bfull[buf], (uint32_t)(kTcChunk * 8));
+            lio::umma::mbar_expect_tx(&bfull[buf], bytes);
             lio::umma::bulk_copy_g2s_hint(tc_smem + Cfg::kBRing + (size_t)buf * kTcChunk * 8,
-                                          src + (long long)k * kTcChunk, kTcChunk * 8, &bfull[buf],
+                                          src + (long long)k * kTcChunk, bytes, &bfull[buf],
                                           chunk_reused(first, k, KP) ? keep : drop);
             issued = cnt + 1;
           }
@@ -500,8 +510,9 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
         lio::umma::fence_before_sync();
         __syncwarp();
         if (lane == 0 && ok) lio::umma::mbar_arrive(&tempty);
-        // ---- row dots against the unit's basis chunks
+        // ---- row dots against the unit's basis chunks (none for a column half past m)
         const int klo = unit_klo(first), khi = unit_khi(first, NK);
+        const bool cols = cb < m;
         for (int k = klo; k <= khi; k++, bcnt++) {
           const int buf = bcnt % kBStages, use = bcnt / kBStages;
           bool okb = !lfail && !*vfail && lio::umma::mbar_wait(&bfull[buf], use & 1);
@@ -509,7 +520,7 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
           if (!okb) {
             lfail = true;
             *vfail = 1;
-          } else {
+          } else if (cols) {
             const double* ch = bring + (size_t)buf * kTcChunk + (colg * CPW) * kTcPoints + row;
             double d4[4][NS][KP];
 #pragma unroll

@@ -133,17 +133,18 @@ __global__ void k_basis(const int2* __restrict__ tiles, const GroupDev* __restri
                         const int* __restrict__ ncont, const double* __restrict__ ca,
                         const double* __restrict__ cc, const double* __restrict__ ax,
                         const double* __restrict__ ay, const double* __restrict__ az, double dnorm,
-                        int gga, double* __restrict__ basis, int nkb) {
+                        int kinds, double* __restrict__ basis, int nkb, int bscale = 1) {
   const int2 t = tiles[blockIdx.x];
   const GroupDev G = groups[t.x];
   const int p = t.y * kBasisBlock + threadIdx.x;
   if (p >= G.ldp) return;
   const bool valid = p < G.npts;
   const double x = px[G.pt_off + p], y = py[G.pt_off + p], z = pz[G.pt_off + p];
-  // function-major cache (nkb = 0): value (kind, i, p) at bas_off + kind * m * ldp + i * ldp + p;
-  // blocked copy of the tensor-core density (nkb kinds): per (128-point tile, 32-function
-  // tile) the kinds one after the other, each [i mod 32][p mod 128]
-  double* out = basis + (nkb ? G.bb_off : G.bas_off);
+  // function-major cache (nkb = 0): value (kind, i, p) at bas_off * bscale + kind * m * ldp + i * ldp + p
+  // (bscale: kinds of this cache over the kinds bas_off was laid out for); blocked copy of the
+  // tensor-core density (nkb kinds): per (128-point tile, 32-function tile) the kinds one after
+  // the other, each [i mod 32][p mod 128]. kinds: 1 (F), 4 (F, gradient) or 10 (and Hessian).
+  double* out = basis + (nkb ? G.bb_off : G.bas_off * bscale);
   const long long kstride = nkb ? (long long)kTcChunkElems : (long long)G.m * G.ldp;
   auto at = [&](int i) {
     return nkb ? ((long long)((p >> 7) * G.nftc + (i >> 5)) * nkb * kTcChunkElems + (i & 31) * 128 + (p & 127))
@@ -175,13 +176,14 @@ __global__ void k_basis(const int2* __restrict__ tiles, const GroupDev* __restri
       const double P = ipow(r[0], l[0]) * ipow(r[1], l[1]) * ipow(r[2], l[2]);
       const long long o = at(ii);
       out[o] = valid ? scale * P * tt : 0.0;
-      if (!gga) continue;
+      if (kinds < 4) continue;
       double Pa[3];
       Pa[0] = dpow(r[0], l[0]) * ipow(r[1], l[1]) * ipow(r[2], l[2]);
       Pa[1] = ipow(r[0], l[0]) * dpow(r[1], l[1]) * ipow(r[2], l[2]);
       Pa[2] = ipow(r[0], l[0]) * ipow(r[1], l[1]) * dpow(r[2], l[2]);
       for (int a = 0; a < 3; a++)
         out[(1 + a) * kstride + o] = valid ? scale * (Pa[a] * tt - 2.0 * r[a] * P * tg) : 0.0;
+      if (kinds < 10) continue;
       // Hessian: (xx, yy, zz) then (xy, xz, yz)
       const int ha[6] = {0, 1, 2, 0, 0, 1}, hb[6] = {0, 1, 2, 1, 2, 2};
       for (int h = 0; h < 6; h++) {
@@ -318,6 +320,130 @@ __global__ void __launch_bounds__(256) k_density_fp64(const int4* __restrict__ t
 #pragma unroll
       for (int k = 0; k < NQ; k++) dst[((long long)ft * NQ + k) * G.ldp + p] = q[k];
     }
+  }
+}
+
+// ------------------------------------------------------- XC nuclear gradients
+// g2g_solve_groups_ types 2 and 3 (g2g/cpu/iteration.cpp:213-267 closed,
+// 496-563 open). Per point p and function i of a group, with the packed
+// density's off-diagonals halved (the symmetric P),
+//   w_i(p) = 2 sum_j P_ij F_j(p),
+// and the atom of function i gets -f_p w_i(p) grad F_i(p) summed over the
+// points, per spin with its own factor f_p = w_p v_xc(p) (the factors of the
+// solve just run). Tile = (group, 64-point tile, 64-function tile) as the FP64
+// density: G = F P in registers (one accumulator block per spin), then the
+// factor-weighted gradient dots, summed over the tile's points, go to the
+// atoms with FP64 atomics (summation order, not values, varies run to run).
+struct BasisView {
+  const double* base;  // function-major cache (nkb = 0) or the blocked copy (nkb kinds)
+  int nkb;
+  int bscale;          // function-major: kinds of this cache over the kinds bas_off counts
+  __device__ __forceinline__ double at(const GroupDev& G, int kind, int i, int p) const {
+    if (nkb == 0) return base[G.bas_off * bscale + ((long long)kind * G.m + i) * G.ldp + p];
+    return base[G.bb_off + ((long long)((p >> 7) * G.nftc + (i >> 5)) * nkb + kind) * kTcChunkElems +
+                (i & 31) * 128 + (p & 127)];
+  }
+};
+
+template <int NS>
+__global__ void __launch_bounds__(256) k_force_fp64(const int4* __restrict__ tiles, const GroupDev* __restrict__ groups,
+                                                    const int* __restrict__ fn_glob, const int* __restrict__ fn_atom,
+                                                    BasisView bv, const double* __restrict__ P_a,
+                                                    const double* __restrict__ P_b, int M,
+                                                    const double* __restrict__ fac_a,
+                                                    const double* __restrict__ fac_b, double* __restrict__ force) {
+  __shared__ double As[kKStep][kTile];
+  __shared__ double Bs[NS][kKStep][kTile + 1];
+  __shared__ double red[8][kTile][3];
+  const int4 t = tiles[blockIdx.x];
+  const GroupDev G = groups[t.x];
+  const int pt0 = t.y * kTile, ft0 = t.z * kTile;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int* fg = fn_glob + G.fn_off;
+  double acc[NS][4][4];
+#pragma unroll
+  for (int sp = 0; sp < NS; sp++)
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+      for (int c = 0; c < 4; c++) acc[sp][r][c] = 0.0;
+
+  for (int j0 = 0; j0 < G.m; j0 += kKStep) {
+#pragma unroll
+    for (int rr = 0; rr < 4; rr++) {
+      const int idx = tid + 256 * rr, kk = idx >> 6, pp = idx & 63;
+      const int j = j0 + kk;
+      As[kk][pp] = j < G.m ? bv.at(G, 0, j, pt0 + pp) : 0.0;
+    }
+#pragma unroll
+    for (int sp = 0; sp < NS; sp++)
+#pragma unroll
+      for (int rr = 0; rr < 4; rr++) {
+        const int idx = tid + 256 * rr, kk = idx >> 6, ii = idx & 63;
+        const int j = j0 + kk, i = ft0 + ii;
+        double v = 0.0;
+        if (j < G.m && i < G.m) {
+          const int gj = fg[j], gi = fg[i];
+          v = (sp == 0 ? P_a : P_b)[packed_index(gi, gj, M)];
+          if (gi != gj) v *= 0.5;
+        }
+        Bs[sp][kk][ii] = v;
+      }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kKStep; kk++) {
+#pragma unroll
+      for (int sp = 0; sp < NS; sp++) {
+        double b[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++) b[c] = Bs[sp][kk][tx + 16 * c];
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+          const double av = As[kk][ty + 16 * r];
+#pragma unroll
+          for (int c = 0; c < 4; c++) acc[sp][r][c] = fma(av, b[c], acc[sp][r][c]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  // sum_p f_p G_i(p) dF_i/da(p) over this thread's 4 points, per function c and axis a
+  double sx[4][3];
+#pragma unroll
+  for (int c = 0; c < 4; c++)
+#pragma unroll
+    for (int a = 0; a < 3; a++) sx[c][a] = 0.0;
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int p = pt0 + ty + 16 * r;
+    const double fa = fac_a[G.pt_off + p], fb = NS == 2 ? fac_b[G.pt_off + p] : 0.0;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const int i = ft0 + tx + 16 * c;
+      if (i >= G.m) continue;
+      const double h = NS == 2 ? fa * acc[0][r][c] + fb * acc[NS - 1][r][c] : fa * acc[0][r][c];
+#pragma unroll
+      for (int a = 0; a < 3; a++) sx[c][a] = fma(h, bv.at(G, 1 + a, i, p), sx[c][a]);
+    }
+  }
+  // over the 16 threads of a function column: the two of a warp by shuffle, the 8 warps in shared memory
+  const int warp = tid >> 5;
+#pragma unroll
+  for (int c = 0; c < 4; c++)
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const double v = sx[c][a] + __shfl_xor_sync(0xffffffffu, sx[c][a], 16);
+      if ((tid & 31) < 16) red[warp][tx + 16 * c][a] = v;
+    }
+  __syncthreads();
+  for (int k = tid; k < kTile * 3; k += 256) {
+    const int fn = k / 3, a = k - 3 * fn, i = ft0 + fn;
+    if (i >= G.m) continue;
+    double v = 0.0;
+#pragma unroll
+    for (int w = 0; w < 8; w++) v += red[w][fn][a];
+    atomicAdd(&force[fn_atom[G.fn_off + i] * 3 + a], -2.0 * v);
   }
 }
 
@@ -559,7 +685,7 @@ struct DeviceEngine::Impl {
     if (basis_tiles.n > 0 && ngroups > 0) {
       k_basis<<<(unsigned)basis_tiles.n, kBasisBlock, 0, stream>>>(basis_tiles.p, groups.p, px.p, py.p, pz.p,
                                                                     sf_glob.p, sf_type.p, nuc.p, ncont.p, ca.p, cc.p,
-                                                                    ax.p, ay.p, az.p, basis_norm, lda ? 0 : 1, dst.p,
+                                                                    ax.p, ay.p, az.p, basis_norm, nk, dst.p,
                                                                     blocked ? nk : 0);
       LIO_CUDA(cudaGetLastError());
     }
@@ -929,14 +1055,15 @@ void DeviceEngine::prepare_tensor_core() {
     if (need + 256 > (size_t)optin)
       throw std::runtime_error("tensor-core density: a group with " + std::to_string(cap) +
                                " functions needs more shared memory than a block can have; use precision 0");
-    LIO_CUDA(cudaFuncSetAttribute(k_density_tc<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)TcCfg<false, 1>::smem(cap)));
-    LIO_CUDA(cudaFuncSetAttribute(k_density_tc<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)TcCfg<false, 2>::smem(cap)));
-    LIO_CUDA(cudaFuncSetAttribute(k_density_tc<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)TcCfg<true, 1>::smem(cap)));
-    LIO_CUDA(cudaFuncSetAttribute(k_density_tc<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)TcCfg<true, 2>::smem(cap)));
+    // only the variant this system runs (the others may not fit at this cap)
+    if (d->lda && d->open)
+      LIO_CUDA(cudaFuncSetAttribute(k_density_tc<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+    else if (d->lda)
+      LIO_CUDA(cudaFuncSetAttribute(k_density_tc<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+    else if (d->open)
+      LIO_CUDA(cudaFuncSetAttribute(k_density_tc<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+    else
+      LIO_CUDA(cudaFuncSetAttribute(k_density_tc<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
   }
   d->tc_ready = true;
 }
@@ -1262,6 +1389,50 @@ SolveResult DeviceEngine::finish(const SolveRequest& req) {
 SolveResult DeviceEngine::solve(const SolveRequest& req) {
   enqueue(req);
   return finish(req);
+}
+
+SolveResult DeviceEngine::solve_forces(const SolveRequest& req, double* forces, int ld) {
+  Impl* d = impl_.get();
+  if (!forces || ld < d->natoms) throw std::runtime_error("forces: null array or leading dimension below natoms");
+  SolveRequest r = req;
+  r.compute_rmm = false;
+  r.resident = false;
+  const SolveResult res = solve(r);  // densities uploaded, factors in fac_a / fac_b
+  if (d->ngroups == 0) return res;
+  cudaStream_t st = d->stream;
+  // F and its gradient: the resident cache of the GGA forms, or (LDA keeps F
+  // only) a four-kind function-major cache built for this call
+  DevBuf<double> grad;
+  BasisView bv{nullptr, 0, 1};
+  if (d->lda) {
+    grad.alloc((size_t)4 * d->basis_elems);
+    k_basis<<<(unsigned)d->basis_tiles.n, kBasisBlock, 0, st>>>(
+        d->basis_tiles.p, d->groups.p, d->px.p, d->py.p, d->pz.p, d->sf_glob.p, d->sf_type.p, d->nuc.p, d->ncont.p,
+        d->ca.p, d->cc.p, d->ax.p, d->ay.p, d->az.p, d->basis_norm, 4, grad.p, 0, 4);
+    LIO_CUDA(cudaGetLastError());
+    bv = BasisView{grad.p, 0, 4};
+  } else if (precision_ == Precision::TensorCore) {
+    bv = BasisView{d->bblk.p, d->nk, 1};
+  } else {
+    bv = BasisView{d->basis.p, 0, 1};
+  }
+  DevBuf<double> frc;
+  frc.alloc((size_t)3 * d->natoms);
+  LIO_CUDA(cudaMemsetAsync(frc.p, 0, (size_t)3 * d->natoms * sizeof(double), st));
+  const unsigned nd = (unsigned)d->dens_tiles.n;
+  if (d->open)
+    k_force_fp64<2><<<nd, 256, 0, st>>>(d->dens_tiles.p, d->groups.p, d->fn_glob.p, d->fn_atom.p, bv, d->P_a.p,
+                                        d->P_b.p, d->M, d->fac_a.p, d->fac_b.p, frc.p);
+  else
+    k_force_fp64<1><<<nd, 256, 0, st>>>(d->dens_tiles.p, d->groups.p, d->fn_glob.p, d->fn_atom.p, bv, d->P_a.p,
+                                        nullptr, d->M, d->fac_a.p, nullptr, frc.p);
+  LIO_CUDA(cudaGetLastError());
+  std::vector<double> h((size_t)3 * d->natoms);
+  LIO_CUDA(cudaMemcpyAsync(h.data(), frc.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  LIO_CUDA(cudaStreamSynchronize(st));
+  for (int a = 0; a < d->natoms; a++)
+    for (int x = 0; x < 3; x++) forces[a + (size_t)ld * x] += h[(size_t)a * 3 + x];
+  return res;
 }
 
 // ======================================================= no-allocation variant

@@ -332,7 +332,7 @@ void g2g_solve_groups_(const unsigned* computation_type, double* fort_energy_ptr
     const bool compute_forces = (ct == 2 || ct == 3);
     const bool compute_rmm = (ct == 0);
     if (s.opt.energy_all_iterations) compute_energy = true;
-    if (compute_forces) throw std::runtime_error("XC forces (computation types 2, 3) are not implemented");
+    if (compute_forces && !fort_forces_ptr) throw std::runtime_error("XC forces requested with a null forces array");
     lio::SolveRequest req;
     req.compute_rmm = compute_rmm;
     req.compute_energy = compute_energy;
@@ -346,11 +346,14 @@ void g2g_solve_groups_(const unsigned* computation_type, double* fort_energy_ptr
       req.fock = s.arr.fock;
     }
     s.engine->set_precision(s.precision);
-    const lio::SolveResult r = s.engine->solve(req);
+    // forces: += into the caller's natoms x 3 column-major array, leading
+    // dimension max_atoms (g2g/partition.cpp:516-526); no Kohn-Sham update
+    const lio::SolveResult r = compute_forces
+                                   ? s.engine->solve_forces(req, fort_forces_ptr, (int)s.arr.max_atoms)
+                                   : s.engine->solve(req);
     s.last_solve_ms = r.device_ms;
     *fort_energy_ptr = compute_energy ? r.energy : 0.0;
     if (std::isnan(*fort_energy_ptr)) fail("XC energy is NaN", 2);
-    (void)fort_forces_ptr;
   });
 }
 

@@ -141,6 +141,20 @@ class G2GLibrary:
         self.check("g2g_solve_groups_")
         return e.value
 
+    def solve_forces(self, computation_type: int = 2):
+        """g2g_solve_groups_ type 2 (energy + forces) or 3 (forces only): returns
+        (E_xc, forces) with forces natoms x 3, the XC gradient contributions the
+        library added into a zeroed caller array (column-major, leading
+        dimension max_atoms = natoms)."""
+        if computation_type not in (2, 3):
+            raise ValueError("forces are computation types 2 and 3")
+        e = C.c_double(0.0)
+        nat = max(1, self._scal["natom"].value)
+        forces = np.zeros(3 * nat)
+        self.lib.g2g_solve_groups_(C.byref(_u(computation_type)), C.byref(e), _ptr(forces, C.c_double))
+        self.check("g2g_solve_groups_")
+        return e.value, forces.reshape(3, nat).T.copy()
+
     def deinit(self):
         self.lib.g2g_deinit_()
 

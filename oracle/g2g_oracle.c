@@ -695,10 +695,13 @@ static void density_point(int m, int gga, const double* R, double* const* v, siz
   q[7] = d2x; q[8] = d2y; q[9] = d2z;
 }
 
+/* One group's E_xc; with Ka, its Kohn-Sham contributions (+=); with frc
+ * (natoms x 3, [atom * 3 + axis]), its XC forces (+=) instead, the
+ * reference's force loop g2g/cpu/iteration.cpp:213-267 (open: 496-563). */
 static double solve_group(const oracle_system* s, const group_t* g, const double* Pa, const double* Pb, double* Ka,
-                          double* Kb) {
+                          double* Kb, double* frc) {
   const int m = total_functions(g), n = g->p.n, gga = s->iexch > 3;
-  const int nk = gga ? 10 : 1;
+  const int nk = (gga || frc) ? 10 : 1;
   int* gl = (int*)malloc(sizeof(int) * (size_t)m);
   for (int f = 0, ii = 0; f < g->nf; f++) {
     const int gf = g->funcs[f];
@@ -707,7 +710,7 @@ static double solve_group(const oracle_system* s, const group_t* g, const double
   }
   double* v[10] = {0};
   for (int k = 0; k < nk; k++) v[k] = (double*)calloc((size_t)n * m, sizeof(double));
-  basis(s, g, gga, v);
+  basis(s, g, gga || frc, v);
   const int nsp = s->open ? 2 : 1;
   double* R[2] = {0, 0};
   for (int sp = 0; sp < nsp; sp++) {
@@ -744,8 +747,58 @@ static double solve_group(const oracle_system* s, const group_t* g, const double
       fa[p] = w * y2a;
     }
   }
+  if (frc) {
+    /* per point: dd[atom] = -sum over the atom's functions ii of w_ii grad F_ii,
+     * w_ii = sum_j R_j,ii F_j (x 2 for j = ii); forces[atom] += dd * factor over
+     * the points in order, per spin, and the spins added at the end */
+    const int nsp2 = s->open ? 2 : 1;
+    double* dd = (double*)calloc((size_t)s->natoms * 3, sizeof(double));
+    double* acc = (double*)calloc((size_t)s->natoms * 3 * 2, sizeof(double));
+    for (int sp = 0; sp < nsp2; sp++) {
+      const double* Rs = R[sp];
+      const double* fac = sp == 0 ? fa : fb;
+      double* ac = acc + (size_t)sp * s->natoms * 3;
+      for (int p = 0; p < n; p++) {
+        const double* fv = v[0] + (size_t)p * m;
+        for (int f = 0, ii = 0; f < g->nf; f++) {
+          const int gf = g->funcs[f];
+          const int nc = gf < s->s_funcs ? 1 : (gf < s->s_funcs + 3 * s->p_funcs ? 3 : 6);
+          const int atom = s->nuc[gf];
+          double tx = 0.0, ty = 0.0, tz = 0.0;
+          for (int k = 0; k < nc; k++, ii++) {
+            double w = 0.0;
+            for (int j = 0; j < m; j++) w += Rs[(size_t)j * m + ii] * fv[j] * (ii == j ? 2 : 1);
+            const size_t o = (size_t)p * m + ii;
+            tx -= w * v[1][o];
+            ty -= w * v[2][o];
+            tz -= w * v[3][o];
+          }
+          dd[atom * 3 + 0] += tx;
+          dd[atom * 3 + 1] += ty;
+          dd[atom * 3 + 2] += tz;
+        }
+        for (int f = 0; f < g->nf; f++) {  /* each atom of the group once, then cleared */
+          const int atom = s->nuc[g->funcs[f]];
+          for (int x = 0; x < 3; x++) {
+            ac[atom * 3 + x] += dd[atom * 3 + x] * fac[p];
+            dd[atom * 3 + x] = 0.0;
+          }
+        }
+      }
+    }
+    for (int f = 0; f < g->nf; f++) {  /* every atom of the group once: its sum, then cleared */
+      const int atom = s->nuc[g->funcs[f]];
+      for (int x = 0; x < 3; x++) {
+        frc[atom * 3 + x] += acc[atom * 3 + x] + (s->open ? acc[(size_t)s->natoms * 3 + atom * 3 + x] : 0.0);
+        acc[atom * 3 + x] = 0.0;
+        if (s->open) acc[(size_t)s->natoms * 3 + atom * 3 + x] = 0.0;
+      }
+    }
+    free(dd);
+    free(acc);
+  }
   /* Kohn-Sham accumulation: g2g/cpu/iteration.cpp:270-291 (open: 581-604) */
-  for (int i = 0; i < m; i++)
+  for (int i = 0; i < m && Ka; i++)
     for (int j = i; j < m; j++) {
       double ra = 0.0, rb = 0.0;
       for (int p = 0; p < n; p++) {
@@ -768,28 +821,37 @@ static double solve_group(const oracle_system* s, const group_t* g, const double
 
 static int solve_groups_list(const oracle_system* s, const double* rho, const double* rho_a, const double* rho_b,
                              double* fock, double* fockb, double* energy, long long* npoints, long long* ngroups,
-                             int first, int stride, const int* ids, int nids);
+                             int first, int stride, const int* ids, int nids, double* forces);
+
+int oracle_solve_forces(const oracle_system* s, const double* rho, const double* rho_a, const double* rho_b,
+                        double* forces, double* energy, long long* npoints, long long* ngroups) {
+  if (!forces) return -1;
+  return solve_groups_list(s, rho, rho_a, rho_b, NULL, NULL, energy, npoints, ngroups, 0, 1, NULL, 0, forces);
+}
 
 int oracle_solve_sample(const oracle_system* s, const double* rho, const double* rho_a, const double* rho_b,
                         double* fock, double* fockb, double* energy, long long* npoints, long long* ngroups,
                         int first, int stride) {
-  return solve_groups_list(s, rho, rho_a, rho_b, fock, fockb, energy, npoints, ngroups, first, stride, NULL, 0);
+  return solve_groups_list(s, rho, rho_a, rho_b, fock, fockb, energy, npoints, ngroups, first, stride, NULL, 0, NULL);
 }
 
 int oracle_solve_subset(const oracle_system* s, const double* rho, const double* rho_a, const double* rho_b,
                         double* fock, double* fockb, double* energy, long long* npoints, long long* ngroups,
                         const int* group_ids, int nids) {
   if (!group_ids || nids < 0) return -1;
-  return solve_groups_list(s, rho, rho_a, rho_b, fock, fockb, energy, npoints, ngroups, 0, 1, group_ids, nids);
+  return solve_groups_list(s, rho, rho_a, rho_b, fock, fockb, energy, npoints, ngroups, 0, 1, group_ids, nids, NULL);
 }
 
 /* Groups first, first + stride, ... or, when ids != NULL, exactly ids[0 .. nids) (the
- * partition's order: cubes, then spheres, each sorted by cost). */
+ * partition's order: cubes, then spheres, each sorted by cost). With forces
+ * (natoms x 3 column-major, leading dimension natoms), XC forces are added
+ * there and no Kohn-Sham contributions are formed (fock may be NULL). */
 static int solve_groups_list(const oracle_system* s, const double* rho, const double* rho_a, const double* rho_b,
                              double* fock, double* fockb, double* energy, long long* npoints, long long* ngroups,
-                             int first, int stride, const int* ids, int nids) {
+                             int first, int stride, const int* ids, int nids, double* forces) {
   if (!s || s->natoms <= 0 || s->M <= 0 || stride <= 0) return -1;
-  if (s->open && (!rho_a || !rho_b || !fockb)) return -2;
+  if (s->open && (!rho_a || !rho_b || (!forces && !fockb))) return -2;
+  if (!forces && !fock) return -1;
   int ng = 0;
   group_t* gs = build_groups(s, &ng);
   int* list = (int*)malloc(sizeof(int) * ((size_t)ng + 1));
@@ -808,8 +870,9 @@ static int solve_groups_list(const oracle_system* s, const double* rho, const do
 #pragma omp single
   nth = omp_get_num_threads();
 #endif
-  double* Ka = (double*)calloc(np * (size_t)nth, sizeof(double));
-  double* Kb = s->open ? (double*)calloc(np * (size_t)nth, sizeof(double)) : NULL;
+  double* Ka = forces ? NULL : (double*)calloc(np * (size_t)nth, sizeof(double));
+  double* Kb = (s->open && !forces) ? (double*)calloc(np * (size_t)nth, sizeof(double)) : NULL;
+  double* Fr = forces ? (double*)calloc((size_t)s->natoms * 3 * (size_t)nth, sizeof(double)) : NULL;
   long long pts = 0, used = 0;
 #pragma omp parallel for schedule(dynamic, 1) reduction(+ : pts, used)
   for (int li = 0; li < nl; li++) {
@@ -818,18 +881,21 @@ static int solve_groups_list(const oracle_system* s, const double* rho, const do
 #ifdef _OPENMP
     t = omp_get_thread_num();
 #endif
-    eg[gi] = solve_group(s, &gs[gi], s->open ? rho_a : rho, rho_b, Ka + np * (size_t)t,
-                         Kb ? Kb + np * (size_t)t : NULL);
+    eg[gi] = solve_group(s, &gs[gi], s->open ? rho_a : rho, rho_b, Ka ? Ka + np * (size_t)t : NULL,
+                         Kb ? Kb + np * (size_t)t : NULL, Fr ? Fr + (size_t)s->natoms * 3 * (size_t)t : NULL);
     pts += gs[gi].p.n;
     used++;
   }
   double e = 0.0;
   for (int gi = 0; gi < ng; gi++) e += eg[gi];
-  for (int t = 0; t < nth; t++)
+  for (int t = 0; t < nth && Ka; t++)
     for (size_t i = 0; i < np; i++) {
       fock[i] += Ka[np * (size_t)t + i];
       if (s->open) fockb[i] += Kb[np * (size_t)t + i];
     }
+  for (int t = 0; t < nth && Fr; t++)
+    for (int a = 0; a < s->natoms; a++)
+      for (int x = 0; x < 3; x++) forces[a + (size_t)s->natoms * x] += Fr[((size_t)t * s->natoms + a) * 3 + x];
   *energy = e;
   if (npoints) *npoints = pts;
   if (ngroups) *ngroups = used;
@@ -842,6 +908,7 @@ static int solve_groups_list(const oracle_system* s, const double* rho, const do
   free(eg);
   free(Ka);
   free(Kb);
+  free(Fr);
   free(list);
   return 0;
 }

@@ -55,6 +55,12 @@ int oracle_solve_subset(const oracle_system* s, const double* rho, const double*
                         double* fock, double* fockb, double* energy, long long* npoints, long long* ngroups,
                         const int* group_ids, int nids);
 
+/* Partition + XC forces (g2g_solve_groups_ types 2/3): each atom's XC force
+ * added into forces (natoms x 3 column-major, leading dimension natoms),
+ * *energy written, no Kohn-Sham contributions. */
+int oracle_solve_forces(const oracle_system* s, const double* rho, const double* rho_a, const double* rho_b,
+                        double* forces, double* energy, long long* npoints, long long* ngroups);
+
 #ifdef __cplusplus
 }
 #endif

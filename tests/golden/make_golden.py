@@ -4,8 +4,8 @@ oracle/Makefile) on small seeded workloads through its C ABI.
 
     python tests/golden/make_golden.py
 
-Each fixture stores E_xc, the packed Kohn-Sham matrices and the partition
-summary (per group: points, functions, a hash-free digest = sum of weights) so
+Each fixture stores E_xc, the packed Kohn-Sham matrices, the XC forces of a
+g2g_solve_groups_ type 2 call (natoms x 3) and the partition summary (per group: points, functions, a hash-free digest = sum of weights) so
 that the C restatement can be checked even where the reference cannot be built.
 """
 import os
@@ -34,6 +34,7 @@ def main():
         L = H.lib(H.REF_LIB, False)
         L.init()
         E, K, Kb = H.run(L, wl)
+        _, F = L.solve_forces(2)
         # partition summary straight from the reference's groups
         ng = L.num_groups(ref=True)
         npts, wsum, nfun = [], [], []
@@ -44,7 +45,7 @@ def main():
             wsum.append(float(np.sum(d["xyzw"][:, 3])))
         L.deinit()
         order = np.lexsort((np.array(wsum), np.array(nfun), np.array(npts)))
-        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), E=E, K=K, Kb=Kb if wl.open_shell else np.zeros(0),
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), E=E, K=K, Kb=Kb if wl.open_shell else np.zeros(0), F=F,
                             npts=np.array(npts)[order], nfun=np.array(nfun)[order], wsum=np.array(wsum)[order])
         print(name, E, len(K), ng)
 

@@ -58,6 +58,25 @@ def run(L, wl, calls=1, options=None, precision=None):
     return E, L.fock.copy(), L.fockb.copy()
 
 
+def run_forces(L, wl, computation_type=2, options=None, precision=None):
+    """(E, forces natoms x 3) of one g2g_solve_groups_ type 2 or 3 call."""
+    gt = bind(L, wl, options=options)
+    if precision is not None:
+        L.set_precision(precision)
+    msg = L.reload_atom_positions(gt)
+    if msg:
+        raise RuntimeError(msg)
+    return L.solve_forces(computation_type)
+
+
+def reference_forces(wl, computation_type=2, options=None):
+    L = lib(REF_LIB, False)
+    L.init()
+    out = run_forces(L, wl, computation_type, options=options)
+    L.deinit()
+    return out
+
+
 def reference(wl, options=None):
     L = lib(REF_LIB, False)
     L.init()
@@ -88,9 +107,10 @@ def _dp(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
-def restatement(wl, first=0, stride=1, options=None, groups=None):
+def restatement(wl, first=0, stride=1, options=None, groups=None, forces=False):
     """(E, fock, fockb, npoints) from the C restatement (oracle/liboracle.so);
-    with `groups`, only those groups (partition order) are built."""
+    with `groups`, only those groups (partition order) are built; with
+    forces=True, (E, forces natoms x 3, npoints) of the XC force build."""
     L = _libs.get("oracle")
     if L is None:
         L = C.CDLL(ORACLE_LIB)
@@ -133,6 +153,11 @@ def restatement(wl, first=0, stride=1, options=None, groups=None):
         r = np.ascontiguousarray(wl.rho)
         keep["r"] = r
         dens = (_dp(r), None, None)
+    if forces:
+        frc = np.zeros(3 * mol.natom)
+        rc = L.oracle_solve_forces(C.byref(s), *dens, _dp(frc), C.byref(E), C.byref(npts), C.byref(ngr))
+        assert rc == 0, rc
+        return E.value, frc.reshape(3, mol.natom).T.copy(), npts.value
     if groups is not None:
         ids = np.ascontiguousarray(np.asarray(groups, dtype=np.int32))
         rc = L.oracle_solve_subset(C.byref(s), *dens, _dp(fock), _dp(fockb), C.byref(E), C.byref(npts),

@@ -24,6 +24,9 @@ def test_restatement_matches_golden(name):
     if wl.open_shell:
         assert np.max(np.abs(Kb - g["Kb"])) <= 1e-11
     assert npts == int(np.sum(g["npts"]))
+    E2, F, _ = H.restatement(wl, forces=True)
+    assert abs(E2 - float(g["E"])) <= 1e-10
+    assert np.max(np.abs(F - g["F"])) <= 1e-11
 
 
 @pytest.mark.skipif(not os.path.exists(H.REF_LIB), reason="reference build absent")
@@ -36,6 +39,20 @@ def test_restatement_matches_reference_live(seed, natoms, iexch, open_shell):
     assert np.max(np.abs(K - K_r)) <= 1e-11
     if open_shell:
         assert np.max(np.abs(Kb - Kb_r)) <= 1e-11
+
+
+@pytest.mark.skipif(not os.path.exists(H.REF_LIB), reason="reference build absent")
+@pytest.mark.parametrize("seed,natoms,iexch,open_shell", [(101, 9, 9, False), (102, 7, 9, True), (104, 6, 2, False)])
+@pytest.mark.parametrize("ctype", [2, 3])
+def test_restatement_forces_match_reference_live(seed, natoms, iexch, open_shell, ctype):
+    """XC forces (g2g_solve_groups_ types 2 and 3): the restatement's loop
+    against the reference's (g2g/cpu/iteration.cpp:213-267, 496-563)."""
+    wl = W.small_workload(natoms, seed, iexch, open_shell)
+    E_r, F_r = H.reference_forces(wl, ctype)
+    E, F, _ = H.restatement(wl, forces=True)
+    assert abs(E - E_r) <= 1e-10
+    assert np.max(np.abs(F - F_r)) <= 1e-11
+    assert np.max(np.abs(F_r)) > 1e-3  # the case has forces to compare
 
 
 def test_restatement_sampling_partitions_groups():
