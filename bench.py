@@ -389,6 +389,97 @@ def ours(args, rank, world):
     return result
 
 
+def forces_mode(args):
+    """XC nuclear forces (g2g_solve_groups_ type 2: E_xc and the forces, no
+    Kohn-Sham update) of the 256-atom molecule through the public ABI with host
+    arrays; the force kernel's own cost is the difference to an energy-only
+    build (type 1) of the same form."""
+    import torch
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    wl = workload(0, args.workload)
+    lib = G2GLibrary()
+    L = lib.lib
+    L.g2g_set_stream_(C.c_void_p(stream.cuda_stream))
+    gt = bind(lib, wl)
+    lib.set_precision(args.precision)
+    msg = lib.reload_atom_positions(gt)
+    if msg:
+        raise RuntimeError(msg)
+    st = lib.partition_stats()
+    npts, nspin = st["points"], 2 if wl.open_shell else 1
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps, out
+
+    L.g2g_last_force_ms_.restype = C.c_double
+    kernel_ms = []
+
+    def force_call():
+        out = lib.solve_forces(2)
+        kernel_ms.append(L.g2g_last_force_ms_())
+        return out
+
+    with ClockSampler(0) as clk:
+        f_ms, (E, F) = timed(force_call)
+    k_ms = float(np.mean(kernel_ms[-args.steps:]))
+    e_ms, _ = timed(lambda: lib.solve_groups(1))
+    tc = args.precision == 1 and wl.iexch > 3
+    hbm, _, src = load_peaks()
+    if tc:
+        # tensor-core force kernel: reads per (point, function) the int8 slices of F
+        # (6 bytes) and the three gradient values (24 bytes) once, per spin from L2
+        fbytes = st["pm"] * (6.0 + 24.0)
+        roof = {"bound": "hbm", "achieved": fbytes / (k_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                "frac": fbytes / (k_ms * 1e-3) / 1e9 / hbm, "traffic": None, "kernel": "k_force_tc",
+                "peak_source": src}
+    else:
+        # FP64 force kernel: G = F P per spin (2 n m^2 flops) and the gradient dots (6 n m)
+        flops = nspin * (2.0 * st["pm2"] + 6.0 * st["pm"])
+        fp64_peak = 148 * 64 * 2 * 1.965e9 / 1e12  # TFLOP/s: 64 FP64 FMA per clock per SM at the max clock
+        roof = {"bound": "fp64", "achieved": flops / (k_ms * 1e-3) / 1e12, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": flops / (k_ms * 1e-3) / 1e12 / fp64_peak, "traffic": None, "kernel": "k_force_fp64",
+                "peak_source": "nominal FP64 FMA rate at the max SM clock"}
+    res = {"metric": "grid pts/s XC forces (g2g_solve_groups_ type 2)", "value": npts / (f_ms * 1e-3),
+           "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": f_ms,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64" if args.precision == 0 else "i8-split/f64", "data": "synthetic",
+           "mode": "forces",
+           "config": {"workload": wl.name, "points": npts, "atoms": wl.mol.natom,
+                      "precision_of_build": args.precision, "max_abs_force": float(np.max(np.abs(F))), "E_xc": E},
+           "e2e": {"value": npts / (f_ms * 1e-3), "unit": UNIT,
+                   "h2d_bytes_per_step": nspin * 8 * (wl.basis.M * (wl.basis.M + 1) // 2),
+                   "d2h_bytes_per_step": 3 * 8 * wl.mol.natom + 8},
+           "energy_only_ms": e_ms, "force_kernel_ms": k_ms, "roofline": roof,
+           "clocks": clk.summary()}
+    if not args.no_cpu_baseline and os.path.exists(REF_LIB):
+        wl2 = W.Workload(**{**wl.__dict__, "n_ang": 194})
+        R = G2GLibrary(REF_LIB, product=False)
+        R.init()
+        R.reload_atom_positions(bind(R, wl2))
+        n2 = sum(int(R.partition_group(g, ref=True)["meta"][0]) for g in range(R.num_groups(ref=True)))
+        R.solve_forces(2)
+        t0 = time.perf_counter()
+        R.solve_forces(2)
+        dt = time.perf_counter() - t0
+        R.deinit()
+        res["cpu_baseline"] = {"value": n2 / dt, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                               "sample": f"one timed g2g_solve_groups_(2) (after one warm-up) of the same molecule "
+                                         f"on the reference's 40x194 grid, {n2} points, {dt:.2f} s"}
+    return res
+
+
 def batch_mode(args):
     """Many-molecule batch: every build of the batch submitted at once to the
     XC service (continuous batching over per-molecule streams); value = grid
@@ -514,9 +605,10 @@ def main():
     ap.add_argument("--precision", type=int, default=1, help="1 = tensor-core form (default), 0 = FP64 plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 form's comparison timing")
-    ap.add_argument("--mode", default="single", choices=["single", "batch", "serve"],
+    ap.add_argument("--mode", default="single", choices=["single", "batch", "serve", "forces"],
                     help="single = the headline 256-atom build; batch = the 512-molecule batch; "
-                         "serve = Poisson-arrival serving of 64 resident molecules")
+                         "serve = Poisson-arrival serving of 64 resident molecules; "
+                         "forces = XC nuclear forces of the 256-atom molecule")
     ap.add_argument("--batch", type=int, default=512, help="molecules in the batch mode")
     ap.add_argument("--molecules", type=int, default=64, help="resident molecules in the serve mode")
     ap.add_argument("--max-atoms", type=int, default=200, help="largest molecule in the serve mode")
@@ -537,7 +629,8 @@ def main():
         return
     if args.mode != "single":
         if rank == 0:
-            print(json.dumps(batch_mode(args) if args.mode == "batch" else serve_mode(args)), flush=True)
+            fn = {"batch": batch_mode, "serve": serve_mode, "forces": forces_mode}[args.mode]
+            print(json.dumps(fn(args)), flush=True)
         return
     if world > 1:
         import datetime

@@ -79,8 +79,10 @@ void g2g_new_grid_(const unsigned int* grid_type);
  * are added to (type 0 only); types 2 and 3 add each atom's XC force into
  * fort_forces_ptr, natoms x 3 column-major with leading dimension max_atoms
  * (g2g/partition.cpp:516-526), with the reference's CPU formula
- * (g2g/cpu/iteration.cpp:213-267, open shell 496-563) evaluated in FP64 from
- * the per-point factors of the build (whose form set_precision selects). */
+ * (g2g/cpu/iteration.cpp:213-267, open shell 496-563) from the per-point
+ * factors of the build (whose form set_precision selects): G = P F in FP64 in
+ * the FP64 form (and for LDA), on tcgen05 from the build's own int8 slices in
+ * the tensor-core form, the gradient dots and sums in FP64 in both. */
 void g2g_solve_groups_(const unsigned int* computation_type, double* fort_energy_ptr,
                        double* fort_forces_ptr);
 
@@ -177,6 +179,11 @@ void g2g_set_graphs_(const unsigned int* on);
  * contraction, and the number of solves timed. Returns the number of stages. */
 void g2g_profile_(const unsigned int* on);
 int g2g_stage_times_(double* ms, int* solves);
+
+/* No counterpart in the reference: device ms of the force kernel of the last
+ * g2g_solve_groups_ type 2 or 3 call (CUDA events around it; the build before
+ * it is not included), or -1 without a device engine. */
+double g2g_last_force_ms_(void);
 
 /* No counterpart in the reference: an XC build that allocates no device
  * memory, for callers that cannot call cudaMalloc (a host program whose

@@ -617,6 +617,7 @@ __global__ void __launch_bounds__(256) k_fock_fp64(const int4* __restrict__ tile
 
 #include "density_tc.cuh"
 #include "fock_tc.cuh"
+#include "force_tc.cuh"
 
 }  // namespace
 
@@ -645,7 +646,7 @@ struct DeviceEngine::Impl {
   long long tc_sizes[5] = {0, 0, 0, 0, 0};
   // tensor-core Kohn-Sham contraction
   DevBuf<int2> fa_rows, fb_rows, fa_tiles32, fb_tiles32;  // rows, and 32-row pieces, of the Fock slice blocks
-  DevBuf<int4> fk_tiles;
+  DevBuf<int4> fk_tiles, force_tc_tiles;
   DevBuf<int8_t> fa_slices, fb_slices_a, fb_slices_b;
   DevBuf<int16_t> fa_exp, fb_exp_a, fb_exp_b;
   long long fk_sizes[4] = {0, 0, 0, 0};
@@ -702,6 +703,8 @@ struct DeviceEngine::Impl {
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t fev0 = nullptr, fev1 = nullptr;  // around the force kernel
+  double last_force_ms = 0.0;
   int launches = 0;
   bool profiling = false;
   static constexpr int kNumStages = 5;
@@ -729,6 +732,8 @@ struct DeviceEngine::Impl {
     stream = own_stream;
     LIO_CUDA(cudaEventCreate(&ev0));
     LIO_CUDA(cudaEventCreate(&ev1));
+    LIO_CUDA(cudaEventCreate(&fev0));
+    LIO_CUDA(cudaEventCreate(&fev1));
     for (auto& e : sev) LIO_CUDA(cudaEventCreate(&e));
   }
   ~Impl() {
@@ -736,6 +741,8 @@ struct DeviceEngine::Impl {
     free_pinned();
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    if (fev0) cudaEventDestroy(fev0);
+    if (fev1) cudaEventDestroy(fev1);
     for (auto& e : sev)
       if (e) cudaEventDestroy(e);
     if (own_stream) cudaStreamDestroy(own_stream);
@@ -764,6 +771,7 @@ void DeviceEngine::release() {
 }
 
 long long DeviceEngine::points() const { return impl_->npoints; }
+double DeviceEngine::last_force_kernel_ms() const { return impl_->last_force_ms; }
 void DeviceEngine::set_stream(void* s) {
   impl_->stream = s ? (cudaStream_t)s : impl_->own_stream;
 }
@@ -804,7 +812,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
   long long bb_off = 0, sl_off = 0, aexp_off = 0, ds_off = 0, dexp_off = 0;
   long long fa_off = 0, fae_off = 0, fb_off = 0, fbe_off = 0;
   std::vector<int2> farows, fbrows, fat32, fbt32;
-  std::vector<int4> fktiles;
+  std::vector<int4> fktiles, frtiles;
   long long npts_total = 0;
   int maxm = 0;
   const int NA = sys.lda ? 1 : 4;
@@ -881,6 +889,9 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
     for (int T = 0; T < G.ldp / kTcPoints; T++) sbtiles.push_back({gdev, T});
     maxm = std::max(maxm, G.m);
     for (int ft = 0; ft < G.nftc; ft++) sdtiles.push_back({gdev, ft});
+    for (int T = 0; T < G.ldp / kTcPoints; T++)  // tensor-core forces: (tile, function tile, spin)
+      for (int ft = 0; ft < G.nftc; ft++)
+        for (int s = 0; s < (sys.open ? 2 : 1); s++) frtiles.push_back({gdev, T, ft, s});
     pt_off += G.ldp;
     fn_off += G.m;
     sf_off += G.nsimple;
@@ -915,6 +926,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
   d->fa_tiles32.upload(fat32);
   d->fb_tiles32.upload(fbt32);
   d->fk_tiles.upload(fktiles);
+  d->force_tc_tiles.upload(frtiles);
   d->hgroups = gd;
   d->ngroups = (long long)gd.size();
   d->npoints = npts_total;
@@ -1420,16 +1432,33 @@ SolveResult DeviceEngine::solve_forces(const SolveRequest& req, double* forces, 
   frc.alloc((size_t)3 * d->natoms);
   LIO_CUDA(cudaMemsetAsync(frc.p, 0, (size_t)3 * d->natoms * sizeof(double), st));
   const unsigned nd = (unsigned)d->dens_tiles.n;
-  if (d->open)
+  const bool tc = precision_ == Precision::TensorCore && !d->lda;
+  LIO_CUDA(cudaEventRecord(d->fev0, st));
+  if (tc) {
+    // G from the build's own int8 operands (F slices, stacked density slices) on tcgen05
+    LIO_CUDA(cudaFuncSetAttribute(k_force_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FtCfg::kSmem));
+    const int nu = (int)d->force_tc_tiles.n;
+    k_force_tc<<<(unsigned)std::min(nu, 2 * d->nsm), FtCfg::kThreads, FtCfg::kSmem, st>>>(
+        d->force_tc_tiles.p, nu, d->groups.p, 4, d->aslices.p, d->aexp.p, d->dslices_a.p, d->dexp_a.p,
+        d->open ? d->dslices_b.p : nullptr, d->open ? d->dexp_b.p : nullptr, d->bblk.p, d->nk, d->fac_a.p,
+        d->open ? d->fac_b.p : nullptr, d->fn_atom.p, frc.p, d->tc_err.p);
+  } else if (d->open)
     k_force_fp64<2><<<nd, 256, 0, st>>>(d->dens_tiles.p, d->groups.p, d->fn_glob.p, d->fn_atom.p, bv, d->P_a.p,
                                         d->P_b.p, d->M, d->fac_a.p, d->fac_b.p, frc.p);
   else
     k_force_fp64<1><<<nd, 256, 0, st>>>(d->dens_tiles.p, d->groups.p, d->fn_glob.p, d->fn_atom.p, bv, d->P_a.p,
                                         nullptr, d->M, d->fac_a.p, nullptr, frc.p);
   LIO_CUDA(cudaGetLastError());
+  LIO_CUDA(cudaEventRecord(d->fev1, st));
   std::vector<double> h((size_t)3 * d->natoms);
   LIO_CUDA(cudaMemcpyAsync(h.data(), frc.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  int terr = 0;
+  if (tc) LIO_CUDA(cudaMemcpyAsync(&terr, d->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   LIO_CUDA(cudaStreamSynchronize(st));
+  if (terr) throw std::runtime_error("tensor-core forces: an MMA completion wait timed out");
+  float fms = 0.f;
+  LIO_CUDA(cudaEventElapsedTime(&fms, d->fev0, d->fev1));
+  d->last_force_ms = fms;
   for (int a = 0; a < d->natoms; a++)
     for (int x = 0; x < 3; x++) forces[a + (size_t)ld * x] += h[(size_t)a * 3 + x];
   return res;

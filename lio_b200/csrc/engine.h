@@ -58,9 +58,12 @@ class DeviceEngine {
   SolveResult solve(const SolveRequest& req);
   // XC nuclear gradients (g2g_solve_groups_ types 2 and 3): a build without
   // the Kohn-Sham accumulation (E_xc and the per-point factors, in the current
-  // form), then each atom's XC force from those factors in FP64, added (+=) into
-  // forces[atom + ld * axis] (the caller's natoms x 3 column-major array).
+  // form), then each atom's XC force from those factors (G = P F in FP64, or
+  // on tcgen05 from the build's int8 slices in the tensor-core GGA form), added
+  // (+=) into forces[atom + ld * axis] (the caller's natoms x 3 column-major array).
   SolveResult solve_forces(const SolveRequest& req, double* forces, int ld);
+  // device ms of the last solve_forces' force kernel (CUDA events around it)
+  double last_force_kernel_ms() const;
   // Replay the kernels of a solve from a CUDA graph captured on first use
   // (re-captured after a new geometry or precision).
   void set_graphs(bool on);

@@ -422,6 +422,16 @@ void g2g_profile_(const unsigned* on) {
   });
 }
 
+double g2g_last_force_ms_(void) {
+  double ms = -1.0;
+  guarded("g2g_last_force_ms_", [&] {
+    State& s = st();
+    if (!s.engine) throw std::runtime_error("no device engine");
+    ms = s.engine->last_force_kernel_ms();
+  });
+  return ms;
+}
+
 int g2g_stage_times_(double* ms, int* solves) {
   int n = 0;
   guarded("g2g_stage_times_", [&] {
