@@ -180,6 +180,13 @@ void g2g_set_graphs_(const unsigned int* on);
 void g2g_profile_(const unsigned int* on);
 int g2g_stage_times_(double* ms, int* solves);
 
+/* No counterpart in the reference: where the Becke weights of a grid build
+ * (g2g_reload_atom_positions_, g2g_new_grid_) are computed. 1 (default): on
+ * the GPU when one is present, one thread per point with explicitly rounded
+ * FP64 operations in the reference's order, so the partition is the same bit
+ * for bit; 0: on the host cores (OpenMP), as g2g/cpu/weight.cpp:13-112 does. */
+void g2g_set_device_weights_(const unsigned int* on);
+
 /* No counterpart in the reference: device ms of the force kernel of the last
  * g2g_solve_groups_ type 2 or 3 call (CUDA events around it; the build before
  * it is not included), or -1 without a device engine. */

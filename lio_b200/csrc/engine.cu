@@ -323,6 +323,74 @@ __global__ void __launch_bounds__(256) k_density_fp64(const int4* __restrict__ t
   }
 }
 
+// --------------------------------------------------------- Becke weights
+// One thread per grid point of the partition being built: its atom's
+// fuzzy-cell weight over the group's nuclei with the atomic-size adjustment
+// (g2g/cpu/weight.cpp:13-112), in the operation order of the host code
+// (partition.cpp) and with every FP64 operation explicitly rounded (no fused
+// multiply-add), so the factors equal the host's, and the reference's, bit
+// for bit. The host multiplies each point's weight by its factor.
+__device__ __forceinline__ double len3_rn(double x, double y, double z) {
+  return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
+}
+
+__device__ __forceinline__ double becke_step_rn(double u, double rm_j, double rm_k) {
+  double x = __ddiv_rn(rm_j, rm_k);
+  x = __ddiv_rn(__dsub_rn(x, 1.0), __dadd_rn(x, 1.0));
+  u = __dadd_rn(u, __dmul_rn(__ddiv_rn(x, __dsub_rn(__dmul_rn(x, x), 1.0)), __dsub_rn(1.0, __dmul_rn(u, u))));
+#pragma unroll
+  for (int it = 0; it < 3; it++) u = __dsub_rn(__dmul_rn(1.5, u), __dmul_rn(0.5, __dmul_rn(__dmul_rn(u, u), u)));
+  return __dmul_rn(0.5, __dsub_rn(1.0, u));
+}
+
+__global__ void k_becke_weights(const double* __restrict__ px, const double* __restrict__ py,
+                                const double* __restrict__ pz, const int* __restrict__ patom,
+                                const int* __restrict__ pgroup, long long n, const int* __restrict__ nuc_off,
+                                const int* __restrict__ nucs, const double* __restrict__ ax,
+                                const double* __restrict__ ay, const double* __restrict__ az,
+                                const double* __restrict__ rm, const double* __restrict__ adist, int natoms,
+                                double* __restrict__ factor) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double x = px[i], y = py[i], z = pz[i];
+  const int atom = patom[i], g = pgroup[i];
+  const int* nl = nucs + nuc_off[g];
+  const int nn = nuc_off[g + 1] - nuc_off[g];
+  double P_total = 0.0, P_atom = 0.0;
+  bool own_found = false;
+  for (int j = 0; j < nn; ++j) {
+    double P_curr = 1.0;
+    const int aj = nl[j];
+    const double dj = len3_rn(__dsub_rn(x, ax[aj]), __dsub_rn(y, ay[aj]), __dsub_rn(z, az[aj]));
+    for (int k = 0; k < nn; ++k) {
+      const int ak = nl[k];
+      if (ak == aj) continue;
+      const double u = __ddiv_rn(__dsub_rn(dj, len3_rn(__dsub_rn(x, ax[ak]), __dsub_rn(y, ay[ak]), __dsub_rn(z, az[ak]))),
+                                 adist[(long long)aj * natoms + ak]);
+      P_curr = __dmul_rn(P_curr, becke_step_rn(u, rm[aj], rm[ak]));
+      if (P_curr == 0.0) break;
+    }
+    if (aj == atom) {
+      own_found = true;
+      P_atom = P_curr;
+      if (P_atom == 0.0) break;
+    }
+    P_total = __dadd_rn(P_total, P_curr);
+  }
+  if (!own_found) {  // the point's own atom is not among the group's nuclei
+    P_atom = 1.0;
+    const double da = len3_rn(__dsub_rn(x, ax[atom]), __dsub_rn(y, ay[atom]), __dsub_rn(z, az[atom]));
+    for (int k = 0; k < nn; ++k) {
+      const int ak = nl[k];
+      const double u = __ddiv_rn(__dsub_rn(da, len3_rn(__dsub_rn(x, ax[ak]), __dsub_rn(y, ay[ak]), __dsub_rn(z, az[ak]))),
+                                 adist[(long long)atom * natoms + ak]);
+      P_atom = __dmul_rn(P_atom, becke_step_rn(u, rm[atom], rm[ak]));
+      if (P_atom == 0.0) break;
+    }
+  }
+  factor[i] = P_total == 0.0 ? 0.0 : __ddiv_rn(P_atom, P_total);
+}
+
 // ------------------------------------------------------- XC nuclear gradients
 // g2g_solve_groups_ types 2 and 3 (g2g/cpu/iteration.cpp:213-267 closed,
 // 496-563 open). Per point p and function i of a group, with the packed
@@ -771,6 +839,50 @@ void DeviceEngine::release() {
 }
 
 long long DeviceEngine::points() const { return impl_->npoints; }
+
+void DeviceEngine::becke_weights(const System& sys, const std::vector<PointGroup*>& groups) {
+  long long n = 0;
+  for (const PointGroup* g : groups) n += (long long)g->points.size();
+  if (n == 0) return;
+  std::vector<double> hx((size_t)n), hy((size_t)n), hz((size_t)n);
+  std::vector<int> hatom((size_t)n), hgroup((size_t)n), hoff(groups.size() + 1, 0), hnucs;
+  long long k = 0;
+  for (size_t gi = 0; gi < groups.size(); gi++) {
+    for (const GridPoint& p : groups[gi]->points) {
+      hx[k] = p.x;
+      hy[k] = p.y;
+      hz[k] = p.z;
+      hatom[k] = p.atom;
+      hgroup[k] = (int)gi;
+      k++;
+    }
+    hnucs.insert(hnucs.end(), groups[gi]->nucs.begin(), groups[gi]->nucs.end());
+    hoff[gi + 1] = (int)hnucs.size();
+  }
+  DevBuf<double> dx, dy, dz, dax, day, daz, drm, dist, fac;
+  DevBuf<int> datom, dgroup, doff, dnucs;
+  dx.upload(hx);
+  dy.upload(hy);
+  dz.upload(hz);
+  datom.upload(hatom);
+  dgroup.upload(hgroup);
+  doff.upload(hoff);
+  dnucs.upload(hnucs);
+  dax.upload(sys.ax);
+  day.upload(sys.ay);
+  daz.upload(sys.az);
+  drm.upload(sys.rm);
+  dist.upload(sys.atom_dist);
+  fac.alloc((size_t)n);
+  k_becke_weights<<<(unsigned)((n + 127) / 128), 128>>>(dx.p, dy.p, dz.p, datom.p, dgroup.p, n, doff.p, dnucs.p,
+                                                        dax.p, day.p, daz.p, drm.p, dist.p, sys.natoms, fac.p);
+  LIO_CUDA(cudaGetLastError());
+  std::vector<double> hf((size_t)n);
+  LIO_CUDA(cudaMemcpy(hf.data(), fac.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+  k = 0;
+  for (PointGroup* g : groups)
+    for (GridPoint& p : g->points) p.w *= hf[(size_t)k++];
+}
 double DeviceEngine::last_force_kernel_ms() const { return impl_->last_force_ms; }
 void DeviceEngine::set_stream(void* s) {
   impl_->stream = s ? (cudaStream_t)s : impl_->own_stream;

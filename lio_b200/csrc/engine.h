@@ -95,6 +95,10 @@ class DeviceEngine {
 
   // true when a CUDA device can be used from this process
   static bool available();
+  // Becke weights of a partition being built, on the current device: the
+  // bit-exact device form of host_becke_weights (partition.h), for
+  // build_partition's `weights` argument.
+  static void becke_weights(const System& sys, const std::vector<PointGroup*>& groups);
   // builds the tensor-core operands now (otherwise the first tensor-core solve does)
   void prepare();
   // Times one build of this molecule in each form, keeps the faster (both meet

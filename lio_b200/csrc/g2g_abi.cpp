@@ -58,6 +58,7 @@ struct State {
   void* stream = nullptr;
   bool graphs = true;
   bool auto_precision = false;
+  bool device_weights = true;  // Becke weights of the grid build on the GPU when one is present
   int shard_rank = 0, shard_world = 1;  // this process's share of the groups (multi-GPU)
 };
 
@@ -162,7 +163,9 @@ void build_grid(unsigned grid_type) {
   if (it == s.grids.end()) throw std::runtime_error("unknown grid type " + std::to_string(grid_type));
   const auto t0 = std::chrono::steady_clock::now();
   refresh_system();
-  lio::build_partition(s.sys, s.opt, it->second, (int)grid_type, s.part);
+  const bool dev = s.device_weights && lio::DeviceEngine::available();
+  lio::build_partition(s.sys, s.opt, it->second, (int)grid_type, s.part,
+                       dev ? &lio::DeviceEngine::becke_weights : nullptr);
   s.grid_type = (int)grid_type;
   s.last_grid_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   // The partition is host work and is kept even without a GPU (so it can be
@@ -420,6 +423,10 @@ void g2g_profile_(const unsigned* on) {
     State& s = st();
     if (s.engine) s.engine->set_profiling(*on != 0);
   });
+}
+
+void g2g_set_device_weights_(const unsigned* on) {
+  guarded("g2g_set_device_weights_", [&] { st().device_weights = *on != 0; });
 }
 
 double g2g_last_force_ms_(void) {

@@ -91,7 +91,7 @@ inline double becke_step(double u, double rm_j, double rm_k) {
   return 0.5 * (1.0 - u);
 }
 
-void compute_weights(const System& sys, const Options& opt, PointGroup& g) {
+void compute_weights(const System& sys, PointGroup& g) {
   const int nn = (int)g.nucs.size();
   const int np = (int)g.points.size();
   const int* nucs = g.nucs.data();
@@ -135,13 +135,16 @@ void compute_weights(const System& sys, const Options& opt, PointGroup& g) {
     const double atom_weight = (P_total == 0.0 ? 0.0 : (P_atom / P_total));
     pt.w *= atom_weight;
   }
-  if (opt.remove_zero_weights) {
-    std::vector<GridPoint> kept;
-    kept.reserve(g.points.size());
-    for (const GridPoint& p : g.points)
-      if (p.w != 0.0) kept.push_back(p);
-    g.points.swap(kept);
-  }
+}
+
+// zero-weight removal (g2g/cpu/weight.cpp:100-111)
+void remove_zero_weights(const Options& opt, PointGroup& g) {
+  if (!opt.remove_zero_weights) return;
+  std::vector<GridPoint> kept;
+  kept.reserve(g.points.size());
+  for (const GridPoint& p : g.points)
+    if (p.w != 0.0) kept.push_back(p);
+  g.points.swap(kept);
 }
 
 long long env_int(const char* name, long long dflt) {
@@ -151,8 +154,12 @@ long long env_int(const char* name, long long dflt) {
 
 }  // namespace
 
+void host_becke_weights(const System& sys, const std::vector<PointGroup*>& groups) {
+  for (PointGroup* g : groups) compute_weights(sys, *g);
+}
+
 void build_partition(const System& sys, const Options& opt, const AngularGrid& ang,
-                     int grid_type, Partition& out) {
+                     int grid_type, Partition& out, WeightsFn weights) {
   out.cubes.clear();
   out.spheres.clear();
   const int natoms = sys.natoms;
@@ -244,6 +251,7 @@ void build_partition(const System& sys, const Options& opt, const AngularGrid& a
   out.mincost = env_int("LIO_MINCOST_OFFSET", 250000);
 
   // cubes (:331-399): screening against the cube box, then weights
+  std::vector<PointGroup> cand_cubes, cand_spheres;
   std::vector<double> dists(natoms);
   for (unsigned i = 0; i < psize[0]; i++)
     for (unsigned j = 0; j < psize[1]; j++)
@@ -268,9 +276,7 @@ void build_partition(const System& sys, const Options& opt, const AngularGrid& a
         assign_functions(sys, opt, dists, min_exps_func, g);
         if (g.funcs.empty() || pts.size() < opt.min_points_per_cube) continue;
         g.points.swap(pts);
-        compute_weights(sys, opt, g);
-        if (g.points.size() < opt.min_points_per_cube) continue;
-        out.cubes.push_back(std::move(g));
+        cand_cubes.push_back(std::move(g));
       }
 
   // spheres (:402-462)
@@ -290,9 +296,22 @@ void build_partition(const System& sys, const Options& opt, const AngularGrid& a
       assign_functions(sys, opt, dists, min_exps_func, g);
       if (sph[a].size() < opt.min_points_per_cube) continue;
       g.points.swap(sph[a]);
-      compute_weights(sys, opt, g);
+      cand_spheres.push_back(std::move(g));
+    }
+  }
+
+  // weights of every candidate group in one pass, then the filters in group order
+  std::vector<PointGroup*> all;
+  all.reserve(cand_cubes.size() + cand_spheres.size());
+  for (PointGroup& g : cand_cubes) all.push_back(&g);
+  for (PointGroup& g : cand_spheres) all.push_back(&g);
+  (weights ? weights : host_becke_weights)(sys, all);
+  for (int pass = 0; pass < 2; pass++) {
+    std::vector<PointGroup>& cand = pass == 0 ? cand_cubes : cand_spheres;
+    for (PointGroup& g : cand) {
+      remove_zero_weights(opt, g);
       if (g.points.size() < opt.min_points_per_cube) continue;
-      out.spheres.push_back(std::move(g));
+      (pass == 0 ? out.cubes : out.spheres).push_back(std::move(g));
     }
   }
 

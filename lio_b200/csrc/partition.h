@@ -36,9 +36,20 @@ struct Partition {
   }
 };
 
+// Becke weights of many groups at once (g2g/cpu/weight.cpp:13-112): every
+// point's weight is multiplied by its atom's fuzzy-cell weight, restricted to
+// the group's nuclei, bit for bit as the reference computes it. The groups'
+// zero-weight points are not removed here.
+using WeightsFn = void (*)(const System& sys, const std::vector<PointGroup*>& groups);
+// host implementation (OpenMP over each group's points)
+void host_becke_weights(const System& sys, const std::vector<PointGroup*>& groups);
+
 // Builds the partition. `grid_type` selects the radial shell table (0: Nr,
-// otherwise Nr2) exactly as g2g/init.cpp:238-266 does.
+// otherwise Nr2) exactly as g2g/init.cpp:238-266 does. The Becke weights of all
+// candidate groups are computed in one call of `weights` (default: the host
+// implementation); zero-weight removal and the minimum-size filter follow, in
+// the reference's group order.
 void build_partition(const System& sys, const Options& opt, const AngularGrid& ang,
-                     int grid_type, Partition& out);
+                     int grid_type, Partition& out, WeightsFn weights = nullptr);
 
 }  // namespace lio

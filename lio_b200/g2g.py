@@ -192,6 +192,11 @@ class G2GLibrary:
     def set_precision(self, mode: int):
         self.lib.g2g_set_precision_(C.byref(_u(mode)))
 
+    def set_device_weights(self, on: bool):
+        """Becke weights of the next grid builds on the GPU (default) or the host."""
+        self.lib.g2g_set_device_weights_(C.byref(_u(1 if on else 0)))
+        self.check("g2g_set_device_weights_")
+
     def partition_stats(self) -> dict:
         out = (C.c_longlong * 6)()
         self.lib.g2g_partition_stats_(out)
