@@ -51,7 +51,7 @@ typedef struct lio_molecule {
   const double* c;          /* M x 13 contraction coefficients */
   int s_funcs, p_funcs, d_funcs; /* simple function counts (a p counts once, not three times) */
   int normalize;            /* 1: d xx, yy, zz carry 1/sqrt(3) (LIO's norm) */
-  int iexch;                /* 1, 2, 3: LDA; 9: PBE */
+  int iexch;                /* 1-3: LDA; 4-9: GGA (4 P86, 5 B88+P86, 6 B88+VWN, 7 BLYP, 8 P86+LYP, 9 PBE; open shell: PBE) */
   int open;                 /* 1: open shell (alpha and beta densities) */
   int nang;                 /* angular grid: points and unit directions/weights (sum 4 pi) */
   const double *ang_x, *ang_y, *ang_z, *ang_w;

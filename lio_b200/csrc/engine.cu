@@ -577,7 +577,8 @@ __global__ void __launch_bounds__(kFuncBlock) k_functional(const int2* __restric
         e = (qa[0] * w) * (o.ex + o.ec);
         va = w * o.v;
       } else if (MODE == 1) {
-        const xc::GgaOut o = xc::pbe_closed(qa[0], qa + 1, qa + 4, qa + 7);
+        const xc::GgaOut o = iexch == 9 ? xc::pbe_closed(qa[0], qa + 1, qa + 4, qa + 7)
+                                        : xc::gga_closed_other(qa[0], qa + 1, qa + 4, qa + 7, iexch);
         e = (qa[0] * w) * (o.ex + o.ec);
         va = w * o.v;
       }

@@ -272,9 +272,11 @@ void g2g_parameter_init_(const unsigned* norm, const unsigned* natom, const unsi
       if (ncont[i] > (unsigned)lio::kMaxContractions)
         throw std::runtime_error("Maximum functions per contraction reached!");
     if (*Iexch < 1 || *Iexch > 9) throw std::runtime_error("Iexch out of range 1..9");
-    if (*Iexch != 1 && *Iexch != 2 && *Iexch != 3 && *Iexch != 9)
-      throw std::runtime_error("Iexch " + std::to_string(*Iexch) +
-                               " is not implemented on the device (supported: 1, 2, 3 LDA; 9 PBE)");
+    // 1-3: LDA (Slater; + Gunnarsson-Lundqvist; + VWN); 4-9: GGA (closed shell:
+    // 4 P86+P86, 5 B88+P86, 6 B88+VWN-form, 7 B88+LYP, 8 P86+LYP, 9 PBE; open
+    // shell: PBE for every GGA value, as g2g/cpu/iteration.cpp:478-480 calls it)
+    if (*Iexch < 1 || *Iexch > 9)
+      throw std::runtime_error("Iexch " + std::to_string(*Iexch) + " is not implemented (supported: 1-3 LDA, 4-9 GGA)");
     if (*use_libxc) throw std::runtime_error("libxc functionals are not supported");
     System& y = s.sys;
     y.s_funcs = (int)nshell[0];

@@ -297,8 +297,7 @@ void lio_server::loop() {
 namespace {
 lio::System to_system(const lio_molecule* d) {
   if (d->natoms <= 0 || d->M <= 0) throw std::runtime_error("empty molecule");
-  if (d->iexch != 1 && d->iexch != 2 && d->iexch != 3 && d->iexch != 9)
-    throw std::runtime_error("iexch must be 1, 2, 3 (LDA) or 9 (PBE)");
+  if (d->iexch < 1 || d->iexch > 9) throw std::runtime_error("iexch must be 1-3 (LDA) or 4-9 (GGA)");
   if (d->s_funcs + 3 * d->p_funcs + 6 * d->d_funcs != d->M) throw std::runtime_error("s/p/d counts do not add up to M");
   lio::System y;
   y.natoms = d->natoms;

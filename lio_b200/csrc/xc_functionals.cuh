@@ -211,6 +211,148 @@ LIO_HD inline GgaOut pbe_closed(double dens, const double g[3], const double h1[
   return o;
 }
 
+// ------------------------------------- other closed-shell GGAs (calc_ggaCS.h)
+// iexch 4: Perdew 86 exchange + Perdew 86 correlation; 5: Becke 88 exchange +
+// Perdew 86; 6: Becke 88 + the VWN-form local correlation alone; 7: Becke 88 +
+// Lee-Yang-Parr; 8: Perdew 86 exchange + LYP (g2g/pointxc/calc_ggaCS.h:36-262).
+// The reference's constants, including its float literals (LIO_F), and its
+// operation order are kept; rho, grad, (xx, yy, zz), (xy, xz, yz) -> ex, ec, y2a.
+LIO_HD inline GgaOut gga_closed_other(double dens, const double g[3], const double h1[3], const double h2[3],
+                                      int iexch) {
+  GgaOut o{0.0, 0.0, 0.0};
+  if (dens < 1e-18) return o;
+  const double ALPHA = -0.738558766382022447, GL = 0.620350490899400087;
+  const double VA1 = 0.03109205, VB1 = 3.72744, VC1 = 12.9352, VX0 = -0.10498, VQ = 6.15199066246304849;
+  const double VA16 = 0.005182008333, VQ2 = 4.7309269;
+  const double ALYP = 0.04918, BLYP = 0.132, CLYP = 0.2533, CLYP3 = 0.0844333333, DLYP = 0.349,
+               DLYP3 = 0.116333333, CF = 2.87123400018819;
+  const double B88 = 0.0042, ALF = 0.023266, BET = 7.389, GAM = 8.723, DEL = 0.472;
+  const double y = cbrt(dens);
+  double grad2 = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+  if (grad2 < DBL_MIN) grad2 = DBL_MIN;
+  const double dgrad = sqrt(grad2);
+  const double lap = h1[0] + h1[1] + h1[2];
+  const double u0 = ((g[0] * g[0]) * h1[0] + 2.0 * g[0] * g[1] * h2[0] + 2.0 * g[1] * g[2] * h2[2] +
+                     2.0 * g[0] * g[2] * h2[1] + (g[1] * g[1]) * h1[1] + (g[2] * g[2]) * h1[2]) /
+                    dgrad;
+  double v = 0.0;
+  if (iexch == 4 || iexch == 8) {  // exchange: Perdew, PRB 33, 8800 (1986)
+    const double dens2 = dens * dens;
+    const double ckf = 3.0936677 * y;
+    const double s = dgrad / (2.0 * ckf * dens);
+    const double fx = 1.0 / 15.0;
+    const double s2 = s * s, s3 = s * s * s, s4 = pow(s, 4);
+    const double g0 = 1.0 + 1.296 * s2 + 14.0 * s4 + 0.2 * pow(s, 6);
+    const double F = pow(g0, fx);
+    o.ex = ALPHA * F * y;
+    const double t = lap / (dens * 4.0 * (ckf * ckf));
+    const double u = u0 / (pow(2.0 * ckf, 3) * dens2);
+    const double g2 = 2.592 * s + 56.0 * s3 + 1.2 * pow(s, 5);
+    const double g3 = 2.592 + 56.0 * s2 + 1.2 * s4;
+    const double g4 = 112.0 * s + 4.8 * s3;
+    const double dF = fx * F / g0 * g2;
+    const double dsF = fx * F / g0 * (-14.0 * fx * g3 * g2 / g0 + g4);
+    v = ALPHA * y * (1.33333333333 * F - t / s * dF - (u - 1.3333333333 * s3) * dsF);
+  } else {  // exchange: Becke, PRA 38, 3098 (1988)
+    const double e0 = ALPHA * y;
+    const double half = dens / 2.0;
+    const double r13 = cbrt(half);
+    const double r43 = cbrt(pow(half, 4));
+    const double xs = dgrad / (2.0 * r43);
+    const double ash = asinh(xs);
+    const double dn = 1.0 + 6.0 * B88 * xs * ash;
+    o.ex = e0 + (-2.0 * B88 * r43 * xs * xs / (dn * dens));
+    const double v0 = 1.33333333333333 * e0;
+    const double fb = 1.0 / dn;
+    const double xa1 = xs / sqrt(1.0 + xs * xs);
+    const double dn1 = 1.0 + fb * (1.0 - 6.0 * B88 * xs * xa1);
+    const double dn2 = 1.0 / (1.0 + xs * xs) + 2.0 * fb * (2.0 - 6.0 * B88 * xs * xa1);
+    const double dn3 = ash * (1.0 + 2.0 * fb) + xa1 * dn2;
+    const double d02 = lap / 2.0;
+    const double de1 = 1.33333333333333 / (cbrt(pow(dens, 7)));
+    const double c2 = cbrt(2.0);
+    // d|grad|/da along each axis and the gradient of x_sigma
+    const double dgx = (g[0] * h1[0] + g[1] * h2[0] + g[2] * h2[1]) / dgrad;
+    const double gxx = c2 * (1.0 / (dens * y) * dgx - de1 * g[0] * dgrad);
+    const double dgy = (g[0] * h2[0] + g[1] * h1[1] + g[2] * h2[2]) / dgrad;
+    const double gxy = c2 * (1.0 / (dens * y) * dgy - de1 * g[1] * dgrad);
+    const double dgz = (g[0] * h2[1] + g[1] * h2[2] + g[2] * h1[2]) / dgrad;
+    const double gxz = c2 * (1.0 / (dens * y) * dgz - de1 * g[2] * dgrad);
+    const double dn4 = 6.0 * B88 * fb * (g[0] / 2.0 * gxx + g[1] / 2.0 * gxy + g[2] / 2.0 * gxz);
+    const double dn5 = 1.33333333333333 * r43 * r13 * xs * xs;
+    const double tot2 = dn5 - d02 * dn1 + dn4 * dn3;
+    v = v0 + (-B88 * fb / r43 * tot2);
+  }
+  if (iexch >= 4 && iexch <= 6) {  // correlation: VWN-form local part (+ Perdew, PRB 33, 8822 (1986))
+    const double dens2 = dens * dens;
+    const double rs = GL / y;
+    const double x1 = sqrt(rs);
+    const double Xx = rs + VB1 * x1 + VC1;
+    const double Xxo = (VX0 * VX0) + VB1 * VX0 + VC1;
+    const double t1 = 2.0 * x1 + VB1;
+    const double t2 = log(Xx);
+    const double t3 = atan(VQ / t1);
+    const double t4 = VB1 * VX0 / Xxo;
+    double ec = VA1 * (2.0 * log(x1) - t2 + 2.0 * VB1 / VQ * t3 -
+                       t4 * (2.0 * log(x1 - VX0) - t2 + 2.0 * (VB1 + 2.0 * VX0) / VQ * t3));
+    const double t5 = (VB1 * x1 + 2.0 * VC1) / x1;
+    const double t6 = VX0 / Xxo;
+    double vc = ec - VA16 * x1 *
+                         (t5 / Xx - 4.0 * VB1 / ((t1 * t1) + (VQ * VQ2)) * (1.0 - t6 * (VB1 - 2.0 * VX0)) -
+                          t4 * (2.0 / (x1 - VX0) - t1 / Xx));
+    if (iexch != 6) {
+      const double rs2 = rs * rs;
+      const double cx1 = LIO_F(0.002568f) + ALF * rs + BET * rs2;
+      const double cx2 = 1.0 + GAM * rs + DEL * rs2 + 1.0e4 * BET * (rs * rs * rs);
+      const double C = 0.001667 + cx1 / cx2;
+      const double cx3 = ALF + 2.0 * BET * rs;
+      const double cx4 = GAM + 2.0 * DEL * rs + 3.0e4 * BET * rs2;
+      double dC = cx3 / cx2 - cx1 / (cx2 * cx2) * cx4;
+      dC = LIO_F(-0.333333333333333f) * dC * GL / (y * dens);
+      const double phi = LIO_F(0.0008129082f) / C * dgrad / pow(dens, (double)(7.0f / 6.0f));
+      const double ex_ = exp(-phi);
+      const double ex0 = ex_ * C;
+      ec = ec + ex0 * grad2 / (y * dens2);
+      const double D1 = (2.0 - phi) * lap / dens;
+      const double phi2 = phi * phi;
+      double D2 = LIO_F(1.33333333333333333f) - LIO_F(3.666666666666666666f) * phi + LIO_F(1.166666666666666f) * phi2;
+      D2 = D2 * grad2 / dens2;
+      const double D3 = phi * (phi - 3.0) * u0 / (dens * dgrad);
+      const double D4 = ex_ * grad2 / (y * dens) * (phi2 - phi - 1.0) * dC;
+      vc = vc - 1.0 * (ex0 / y * (D1 - D2 + D3) - D4);
+    }
+    o.ec = ec;
+    v = v + vc;
+  } else {  // correlation: Lee, Yang, Parr, PRB 37, 785 (1988)
+    const double rom13 = 1 / cbrt(dens);
+    const double rom53 = cbrt(pow(dens, 5));
+    const double ecro = exp(-CLYP * rom13);
+    const double f1 = 1.0 / (1.0 + DLYP * rom13);
+    const double tw = 0.125 * (grad2 / dens - lap);
+    double term = (tw / 9.0 + lap / 18.0) - 2.0 * tw + CF * rom53;
+    term = dens + BLYP * (rom13 * rom13) * ecro * term;
+    o.ec = -ALYP * f1 * term / dens;
+    const double hh1 = ecro / rom53;
+    const double gg1 = f1 * hh1;
+    const double tm1 = DLYP3 * (rom13 / dens);
+    const double fp1 = tm1 * (f1 * f1);
+    const double tm2 = LIO_F(-1.666666666f) + CLYP3 * rom13;
+    const double hp1 = hh1 * tm2 / dens;
+    const double gp1 = fp1 * hh1 + hp1 * f1;
+    const double fp2 = tm1 * 2.0 * f1 * (fp1 - LIO_F(0.6666666666f) * f1 / dens);
+    const double tm3 = LIO_F(1.6666666666f) - CLYP3 * LIO_F(1.3333333333f) * rom13;
+    const double hp2 = hp1 * tm2 / dens + hh1 * tm3 / (dens * dens);
+    const double gp2 = fp2 * hh1 + 2.0 * fp1 * hp1 + hp2 * f1;
+    const double term3 = -ALYP * (fp1 * dens + f1) - ALYP * BLYP * CF * (gp1 * dens + (double)(8.0f / 3.0f) * gg1) * rom53;
+    const double term4 = (gp2 * dens * grad2 + gp1 * (3.0 * grad2 + 2.0 * dens * lap) + 4.0 * gg1 * lap) * ALYP * BLYP / 4.0;
+    const double term5 =
+        (3.0 * gp2 * dens * grad2 + gp1 * (5.0 * grad2 + 6.0 * dens * lap) + 4.0 * gg1 * lap) * ALYP * BLYP / 72.0;
+    v = v + (term3 - term4 - term5);
+  }
+  o.v = v;
+  return o;
+}
+
 // ----------------------------------------------------- PBE open shell (pbeOS_*.h)
 // rho13 = cbrt(rho) of the spin-doubled density (pbeOS_exch.h:42-75 takes rho)
 LIO_HD inline void pbe_exchange_spin(double rho13, double s, double u, double v, double& ex, double& vx) {

@@ -25,6 +25,9 @@ CASES = {
     "pbe_open_10": lambda: W.small_workload(10, 31, 9, True),
     "lda_gl_8": lambda: W.small_workload(8, 41, 2, False),
     "slater_6": lambda: W.small_workload(6, 43, 1, False),
+    "p86_9": lambda: W.small_workload(9, 205, 4, False),
+    "b88_vwn_8": lambda: W.small_workload(8, 207, 6, False),
+    "blyp_10": lambda: W.small_workload(10, 208, 7, False),
 }
 
 

@@ -61,7 +61,7 @@ def test_errors_are_reported_not_thrown():
 
 def test_invalid_parameters_are_rejected():
     wl = W.small_workload(4, 3, 9, False)
-    wl.iexch = 7  # LYP: implemented by the reference CPU path, not by the device functionals here
+    wl.iexch = 10  # no such functional in the reference (g2g/pointxc/calc_ggaCS.h:264-300)
     L = G2GLibrary(PROD)
     L.set_options()
     with pytest.raises(RuntimeError, match="Iexch"):

@@ -14,6 +14,12 @@ CASES = [
     ("pbe-open-10", lambda: W.small_workload(10, 31, 9, True)),
     ("lda-gl-8", lambda: W.small_workload(8, 41, 2, False)),
     ("slater-8", lambda: W.small_workload(8, 43, 1, False)),
+    ("p86-9", lambda: W.small_workload(9, 205, 4, False)),
+    ("b88-p86-9", lambda: W.small_workload(9, 206, 5, False)),
+    ("b88-vwn-8", lambda: W.small_workload(8, 207, 6, False)),
+    ("blyp-10", lambda: W.small_workload(10, 208, 7, False)),
+    ("p86-lyp-9", lambda: W.small_workload(9, 209, 8, False)),
+    ("blyp-open-8", lambda: W.small_workload(8, 210, 7, True)),  # open shell: PBE, as the reference
 ]
 
 

@@ -42,7 +42,19 @@ def test_restatement_matches_reference_live(seed, natoms, iexch, open_shell):
 
 
 @pytest.mark.skipif(not os.path.exists(H.REF_LIB), reason="reference build absent")
-@pytest.mark.parametrize("seed,natoms,iexch,open_shell", [(101, 9, 9, False), (102, 7, 9, True), (104, 6, 2, False)])
+@pytest.mark.parametrize("iexch", [4, 5, 6, 7, 8])
+def test_restatement_other_ggas_match_reference_live(iexch):
+    """Closed-shell GGAs other than PBE (g2g/pointxc/calc_ggaCS.h:36-262)."""
+    wl = W.small_workload(10, 300 + iexch, iexch, False)
+    E_r, K_r, _ = H.reference(wl)
+    E, K, _, _ = H.restatement(wl)
+    assert abs(E - E_r) <= 1e-10
+    assert np.max(np.abs(K - K_r)) <= 1e-11
+
+
+@pytest.mark.skipif(not os.path.exists(H.REF_LIB), reason="reference build absent")
+@pytest.mark.parametrize("seed,natoms,iexch,open_shell", [(101, 9, 9, False), (102, 7, 9, True), (104, 6, 2, False),
+                                                          (105, 8, 7, False)])
 @pytest.mark.parametrize("ctype", [2, 3])
 def test_restatement_forces_match_reference_live(seed, natoms, iexch, open_shell, ctype):
     """XC forces (g2g_solve_groups_ types 2 and 3): the restatement's loop
