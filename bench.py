@@ -558,20 +558,24 @@ def serve_mode(args):
         cap = 2 * len(mids) / (time.perf_counter() - t0)  # builds per second, closed loop
         if rates is None:  # offered loads: fractions of the tensor-core form's capacity, for both forms
             rates = [f * cap for f in (0.25, 0.5, 0.75, 0.9)]
-        sweep = []
+        sweep, samples = [], []
         for rate in rates:
             srv.reset_stats()
-            lat, sample = S.serve_poisson(srv, mids, rate, args.duration, seed=int(rate) % 1000)
+            lat, sample, failed = S.serve_poisson(srv, mids, rate, args.duration, seed=int(rate) % 1000)
             st = srv.stats()
             row = {"rate_hz": round(rate, 2), "requests": len(lat), "p50_ms": st["p50_ms"],
                    "p99_ms": st["p99_ms"], "points_per_s": st["points"] / max(st["wall_s"], 1e-9),
-                   "peak_inflight": st["peak_inflight"], "evictions": st["evictions"]}
-            if prec == args.service_precision and sample:
-                row["spot_checks"] = len(sample)
-                row["spot_max_abs_dE_vs_fp64"], row["spot_max_abs_dK_vs_fp64"] = spot_check(wls, mids, sample)
+                   "peak_inflight": st["peak_inflight"], "evictions": st["evictions"],
+                   "failed": failed}
             sweep.append(row)
+            samples.append(sample)
         forms = [srv.form(m)[0] for m in mids]
         srv.close()
+        if prec == args.service_precision:  # after the server has released the GPU's memory
+            for row, sample in zip(sweep, samples):
+                if sample:
+                    row["spot_checks"] = len(sample)
+                    row["spot_max_abs_dE_vs_fp64"], row["spot_max_abs_dK_vs_fp64"] = spot_check(wls, mids, sample)
         out["tensor" if prec else "fp64_plain"] = {
             "capacity_builds_per_s": cap, "sweep": sweep,
             "forms": {"tensor": sum(1 for f in forms if f == 1), "fp64": sum(1 for f in forms if f == 0)}}
@@ -593,6 +597,7 @@ def spot_check(wls, mids, sample):
         E0, K0, _ = H.run(L, wl2, precision=0)
         de = max(de, abs(e - E0))
         dk = max(dk, float(np.max(np.abs(ka - K0))))
+    L.deinit()  # the single-molecule engine's device memory goes before the next server
     return de, dk
 
 

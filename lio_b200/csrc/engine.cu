@@ -1324,11 +1324,33 @@ void DeviceEngine::copy_results(double* d_fock_a, double* d_fock_b, double* d_en
 }
 
 void DeviceEngine::prepare() {
-  if (precision_ == Precision::TensorCore && !impl_->tc_ready) {
+  Impl* d = impl_.get();
+  if (precision_ == Precision::TensorCore && !d->tc_ready) {
     prepare_tensor_core();
-    impl_->drop_graph();
-    LIO_CUDA(cudaStreamSynchronize(impl_->stream));
+    d->drop_graph();
+    LIO_CUDA(cudaStreamSynchronize(d->stream));
+  } else if (precision_ == Precision::FP64 && !d->basis_valid && d->ngroups > 0) {
+    d->compute_basis();  // synchronises
+    d->drop_graph();
   }
+}
+
+size_t DeviceEngine::cache_bytes() const {
+  const Impl* d = impl_.get();
+  size_t b = (d->basis.n + d->bblk.n) * sizeof(double);
+  for (const auto* x : {&d->aslices, &d->dslices_a, &d->dslices_b, &d->fa_slices, &d->fb_slices_a, &d->fb_slices_b})
+    b += x->n;
+  for (const auto* x : {&d->aexp, &d->dexp_a, &d->dexp_b, &d->fa_exp, &d->fb_exp_a, &d->fb_exp_b})
+    b += x->n * sizeof(int16_t);
+  return b;
+}
+
+void DeviceEngine::release_caches() {
+  Impl* d = impl_.get();
+  LIO_CUDA(cudaStreamSynchronize(d->stream));  // no build in flight reads them
+  d->basis.free();
+  d->basis_valid = false;
+  drop_tensor_core();
 }
 
 long long DeviceEngine::process_device_bytes() { return g_devbuf_bytes.load(); }

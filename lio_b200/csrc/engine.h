@@ -99,8 +99,15 @@ class DeviceEngine {
   // bit-exact device form of host_becke_weights (partition.h), for
   // build_partition's `weights` argument.
   static void becke_weights(const System& sys, const std::vector<PointGroup*>& groups);
-  // builds the tensor-core operands now (otherwise the first tensor-core solve does)
+  // builds the current form's per-geometry caches now (tensor-core operands or
+  // the FP64 basis cache; otherwise the next solve does)
   void prepare();
+  // releases the per-geometry caches (basis values, tensor-core operands), the
+  // bulk of a molecule's device bytes; the grid, tiles and per-solve buffers stay
+  // and the next prepare() or solve rebuilds the caches on the device
+  void release_caches();
+  // device bytes release_caches() would free
+  size_t cache_bytes() const;
   // Times one build of this molecule in each form, keeps the faster (both meet
   // the accuracy bar; memory_aware: the smaller time x device-bytes product)
   // and releases the other's device buffers; returns it.

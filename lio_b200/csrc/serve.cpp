@@ -1,18 +1,23 @@
 // XC build service with continuous batching (C ABI in include/lio_serve.h).
 //
-// One worker thread owns every DeviceEngine (one per resident molecule, each
-// with its own CUDA stream) and makes all CUDA calls of the service; callers
-// only enqueue requests and wait for them. The loop:
+// Two threads make the service's CUDA calls; callers only enqueue requests and
+// wait for them. The worker owns the running builds (one DeviceEngine per
+// resident molecule, each with its own CUDA stream). Its loop:
 //   1. completes requests whose device work has finished (event query) and
 //      wakes their waiters;
 //   2. admits queued requests in arrival order while fewer than max_inflight
-//      run: a request whose molecule is busy stays queued (one build in flight
-//      per molecule: its engine holds one set of per-solve buffers) and later
-//      requests may pass it; a molecule that is not resident is uploaded when
-//      its footprint fits the budget, after evicting idle residents least
-//      recently used first (plan_admission);
+//      run: a request whose molecule is busy or loading stays queued (one build
+//      in flight per molecule: its engine holds one set of per-solve buffers)
+//      and later requests may pass it; for a molecule that is not resident it
+//      plans the room (plan_admission, least recently used idle molecules
+//      first: their per-geometry caches, and only if that is not enough whole
+//      molecules), books the bytes and hands the eviction and the upload to the
+//      loader thread;
 //   3. enqueues the admitted build on the molecule's stream and moves on, so
 //      builds of different molecules overlap on the GPU.
+// The loader frees the evicted memory and uploads (or, for a molecule whose
+// caches were evicted, recomputes them on the device) without holding the
+// lock, so requests for resident molecules keep being served meanwhile.
 // Requests arriving while others run are therefore admitted as soon as a slot
 // and memory free up (continuous batching), not after the current batch.
 #pragma GCC visibility push(default)
@@ -75,6 +80,13 @@ struct Molecule {
   std::unique_ptr<lio::DeviceEngine> engine;  // null while not resident
   unsigned long long footprint = 0;           // device bytes while resident
   bool measured = false;
+  // cold: resident grid (points, tiles, buffers) without the per-geometry
+  // caches (basis values, tensor-core operands), which the next build
+  // recomputes on the device; core = the bytes a cold molecule still holds
+  bool cold = false;
+  unsigned long long core = 0;
+  bool loading = false;    // in the loader's hands (being uploaded, restored or evicted)
+  std::string load_error;  // an upload that failed: its requests fail with this
   int form = -1;  // the form it runs in (0 FP64, 1 tensor core) once resident
   double tuned_ms[2] = {0.0, 0.0};
   bool busy = false;
@@ -97,6 +109,13 @@ struct Request {
 
 }  // namespace
 
+struct LoadJob {
+  int mol = -1;                                          // made resident (hot)
+  std::vector<int> demote;                               // idle molecules whose caches go
+  std::vector<std::unique_ptr<lio::DeviceEngine>> drop;  // engines of molecules evicted whole
+  unsigned long long reserved = 0;                       // bytes booked for `mol`
+};
+
 struct lio_server {
   int device = 0;
   lio::Precision precision = lio::Precision::TensorCore;
@@ -104,8 +123,10 @@ struct lio_server {
   int max_inflight = 16;
   unsigned long long budget = 0, used = 0;
   std::mutex mu;
-  std::condition_variable cv_work, cv_done;
-  std::thread worker;
+  std::condition_variable cv_work, cv_done, cv_load;
+  std::thread worker, loader;
+  std::deque<LoadJob> jobs;
+  unsigned long long epoch = 0;  // bumped by submissions and finished loads (the worker's wake-ups)
   bool stop = false;
   std::string error;
   std::vector<std::unique_ptr<Molecule>> mols;
@@ -119,65 +140,165 @@ struct lio_server {
   double points_done = 0.0;
   bool any_submit = false;
   Clock::time_point t_first, t_last;
-  long long evictions = 0, uploads = 0;
+  long long evictions = 0, uploads = 0, oom_retries = 0;
   size_t peak_inflight = 0;
 
   void loop();
-  bool admit(Molecule& m, std::string& why);
+  void loader_loop();
+  bool plan_load(int mi, std::string& why);
+  bool any_loading() const {
+    for (auto& x : mols)
+      if (x->loading) return true;
+    return false;
+  }
 };
 
-bool lio_server::admit(Molecule& m, std::string& why) {
-  if (m.engine) return true;
+// Under the lock: books room for molecule mi (not hot, not loading) and queues
+// its load; false with `why` empty when it cannot fit yet, or a reason when it
+// never can.
+bool lio_server::plan_load(int mi, std::string& why) {
+  Molecule& m = *mols[mi];
   // before the first upload: the estimate of its form (autotuned: the larger of
-  // the two, held one after the other while both are timed)
+  // the two, held one after the other while both are timed); a cold molecule
+  // needs its caches back only
   const unsigned long long need =
-      m.measured ? m.footprint
+      m.engine ? m.footprint - m.core
+      : m.measured ? m.footprint
       : autotune ? (unsigned long long)std::max(
                        lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, lio::Precision::FP64),
                        lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, lio::Precision::TensorCore))
                  : (unsigned long long)lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, precision);
-  std::vector<unsigned long long> fp, lu;
+  // Eviction in two levels, least recently used idle molecules first: their
+  // caches (the bulk of a footprint; they go cold and keep their grid), and only
+  // if that cannot make room, whole molecules (hot or cold).
+  std::vector<unsigned long long> fp_cache, fp_all, lu;
   std::vector<int> busy;
-  for (auto& x : mols) {
-    fp.push_back(x->engine ? x->footprint : 0);
-    busy.push_back(x->busy ? 1 : 0);
-    lu.push_back(x->last_use);
+  for (size_t i = 0; i < mols.size(); i++) {
+    const Molecule& x = *mols[i];
+    const bool cand = (int)i != mi && x.engine && !x.loading;
+    fp_cache.push_back(cand && !x.cold ? (unsigned long long)x.engine->cache_bytes() : 0);
+    fp_all.push_back(cand ? (x.cold ? x.core : x.footprint) : 0);
+    busy.push_back(x.busy || x.loading ? 1 : 0);
+    lu.push_back(x.last_use);
   }
+  LoadJob job;
   std::vector<int> evict;
-  if (!plan_admission((int)mols.size(), fp.data(), busy.data(), lu.data(), budget, used, need, evict)) {
+  if (plan_admission((int)mols.size(), fp_cache.data(), busy.data(), lu.data(), budget, used, need, evict)) {
+    for (int i : evict) {
+      Molecule& x = *mols[i];
+      x.core = x.footprint > fp_cache[i] ? x.footprint - fp_cache[i] : 0;
+      x.cold = true;
+      x.loading = true;
+      used -= fp_cache[i];
+      evictions++;
+      job.demote.push_back(i);
+    }
+  } else if (plan_admission((int)mols.size(), fp_all.data(), busy.data(), lu.data(), budget, used, need, evict)) {
+    for (int i : evict) {
+      Molecule& x = *mols[i];
+      job.drop.push_back(std::move(x.engine));
+      x.cold = false;
+      used -= fp_all[i];
+      evictions++;
+    }
+  } else {
     why = need > budget ? "molecule footprint exceeds the server's HBM budget" : "";
     return false;
   }
-  for (int i : evict) {
-    Molecule& x = *mols[i];
-    x.engine.reset();  // frees its device memory
-    used -= x.footprint;
-    evictions++;
-  }
-  const long long before = lio::DeviceEngine::process_device_bytes();
-  std::unique_ptr<lio::DeviceEngine> e(new lio::DeviceEngine());
-  e->set_graphs(true);
-  if (autotune && m.form >= 0) {  // decided at an earlier upload
-    e->set_precision(m.form ? lio::Precision::TensorCore : lio::Precision::FP64);
-    e->upload(m.sys, m.part);
-    e->prepare();
-  } else if (autotune) {
-    e->upload(m.sys, m.part);
-    m.form = e->autotune(true) == lio::Precision::TensorCore ? 1 : 0;
-    e->tuned_times(&m.tuned_ms[0], &m.tuned_ms[1]);
-  } else {
-    e->set_precision(precision);
-    e->upload(m.sys, m.part);
-    e->prepare();
-    m.form = precision == lio::Precision::TensorCore ? 1 : 0;
-  }
-  const long long after = lio::DeviceEngine::process_device_bytes();
-  m.footprint = (unsigned long long)std::max<long long>(after - before, 1);
-  m.measured = true;
-  m.engine = std::move(e);
-  used += m.footprint;
-  uploads++;
+  used += need;
+  job.mol = mi;
+  job.reserved = need;
+  m.loading = true;
+  jobs.push_back(std::move(job));
+  cv_load.notify_one();
   return true;
+}
+
+void lio_server::loader_loop() {
+  cudaSetDevice(device);
+  std::unique_lock<std::mutex> lk(mu);
+  while (true) {
+    cv_load.wait(lk, [&] { return stop || !jobs.empty(); });
+    if (stop) break;
+    LoadJob job = std::move(jobs.front());
+    jobs.pop_front();
+    Molecule& m = *mols[job.mol];
+    std::vector<lio::DeviceEngine*> demote;
+    for (int i : job.demote) demote.push_back(mols[i]->engine.get());
+    lio::DeviceEngine* cold = m.engine.get();  // non-null: caches to rebuild
+    const int form = m.form;
+    lk.unlock();
+    std::string err;
+    std::unique_ptr<lio::DeviceEngine> e;
+    int new_form = form;
+    double tuned[2] = {0.0, 0.0};
+    long long delta = 0;
+    try {
+      job.drop.clear();  // frees the memory of the molecules evicted whole
+      for (lio::DeviceEngine* x : demote) x->release_caches();
+      const long long before = lio::DeviceEngine::process_device_bytes();
+      if (cold) {
+        cold->prepare();
+      } else {
+        e.reset(new lio::DeviceEngine());
+        e->set_graphs(true);
+        if (autotune && form >= 0) {  // decided at an earlier upload
+          e->set_precision(form ? lio::Precision::TensorCore : lio::Precision::FP64);
+          e->upload(m.sys, m.part);
+          e->prepare();
+        } else if (autotune) {
+          e->upload(m.sys, m.part);
+          new_form = e->autotune(true) == lio::Precision::TensorCore ? 1 : 0;
+          e->tuned_times(&tuned[0], &tuned[1]);
+        } else {
+          e->set_precision(precision);
+          e->upload(m.sys, m.part);
+          e->prepare();
+          new_form = precision == lio::Precision::TensorCore ? 1 : 0;
+        }
+      }
+      delta = lio::DeviceEngine::process_device_bytes() - before;
+    } catch (const std::exception& ex) {
+      err = ex.what();
+      e.reset();  // a partial upload's memory goes before the lock is taken
+      try {
+        if (cold) cold->release_caches();
+      } catch (...) {
+      }
+    }
+    lk.lock();
+    for (int i : job.demote) mols[i]->loading = false;
+    m.loading = false;
+    if (!err.empty()) {
+      used -= job.reserved;
+      if (err.find("out of memory") != std::string::npos && budget > job.reserved) {
+        // memory the accounting counted as free is held elsewhere (another
+        // user of the GPU): shrink the budget by this request and let the
+        // request retry, evicting more
+        budget -= job.reserved;
+        oom_retries++;
+      } else {
+        m.load_error = err;
+      }
+    } else {
+      used = (unsigned long long)std::max<long long>((long long)used - (long long)job.reserved + delta, 0);
+      if (cold) {
+        m.cold = false;
+      } else {
+        m.engine = std::move(e);
+        m.footprint = (unsigned long long)std::max<long long>(delta, 1);
+        m.measured = true;
+        if (new_form != form) {
+          m.form = new_form;
+          m.tuned_ms[0] = tuned[0];
+          m.tuned_ms[1] = tuned[1];
+        }
+      }
+      uploads++;
+    }
+    epoch++;
+    cv_work.notify_all();
+  }
 }
 
 void lio_server::loop() {
@@ -185,6 +306,7 @@ void lio_server::loop() {
   std::unique_lock<std::mutex> lk(mu);
   while (!stop) {
     bool progressed = false;
+    const unsigned long long seen = epoch;
     // 1. completions
     for (size_t k = 0; k < running.size();) {
       Request& r = *reqs[running[k]];
@@ -219,19 +341,27 @@ void lio_server::loop() {
     for (auto it = queue.begin(); it != queue.end() && (int)running.size() < max_inflight;) {
       Request& r = *reqs[*it];
       Molecule& m = *mols[r.mol];
-      if (m.busy) {
+      if (m.busy || m.loading) {
         ++it;
         continue;
       }
-      std::string why;
-      bool ok = false;
-      try {
-        ok = admit(m, why);
-      } catch (const std::exception& ex) {
-        why = ex.what();
+      if (!m.load_error.empty()) {
+        r.error = m.load_error;
+        r.state = Request::kDone;
+        it = queue.erase(it);
+        cv_done.notify_all();
+        continue;
       }
-      if (!ok) {
-        if (!why.empty() || running.empty()) {  // cannot fit now and nothing will free memory
+      if (!m.engine || m.cold) {  // not resident: book room, the loader makes it so
+        std::string why;
+        bool ok = false;
+        try {
+          ok = plan_load(r.mol, why);
+        } catch (const std::exception& ex) {
+          why = ex.what();
+        }
+        if (!ok && (!why.empty() || (running.empty() && jobs.empty() && !any_loading()))) {
+          // cannot fit now and nothing will free memory
           r.error = why.empty() ? "molecule does not fit the HBM budget" : why;
           r.state = Request::kDone;
           it = queue.erase(it);
@@ -271,8 +401,8 @@ void lio_server::loop() {
       progressed = true;
     }
     if (!progressed) {
-      if (running.empty())
-        cv_work.wait(lk, [&] { return stop || !queue.empty(); });
+      if (running.empty())  // nothing on the GPU: sleep until a submission or a finished load
+        cv_work.wait(lk, [&] { return stop || epoch != seen; });
       else {  // device work in flight: poll its completion events
         lk.unlock();
         std::this_thread::sleep_for(std::chrono::microseconds(20));
@@ -361,6 +491,7 @@ lio_server* lio_srv_create(int device, unsigned long long hbm_budget_bytes, int 
     s->budget = hbm_budget_bytes ? hbm_budget_bytes : (unsigned long long)(0.9 * (double)fr);
     lio_server* p = s.release();
     p->worker = std::thread([p] { p->loop(); });
+    p->loader = std::thread([p] { p->loader_loop(); });
     return p;
   } catch (...) {
     return nullptr;
@@ -374,7 +505,9 @@ void lio_srv_destroy(lio_server* srv) {
     srv->stop = true;
   }
   srv->cv_work.notify_all();
+  srv->cv_load.notify_all();
   if (srv->worker.joinable()) srv->worker.join();
+  if (srv->loader.joinable()) srv->loader.join();
   delete srv;
 }
 
@@ -415,7 +548,7 @@ int lio_srv_molecule_info(lio_server* srv, int mol, long long* points, unsigned 
   if (footprint)
     *footprint = m.measured ? m.footprint
                             : (unsigned long long)lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, srv->precision);
-  if (resident) *resident = m.engine ? 1 : 0;
+  if (resident) *resident = m.engine && !m.cold ? 1 : 0;
   return 0;
 }
 
@@ -453,6 +586,7 @@ long long lio_srv_submit(lio_server* srv, int mol, const double* rho_a, const do
   const long long id = srv->next_id++;
   srv->reqs[id] = std::move(r);
   srv->queue.push_back(id);
+  srv->epoch++;
   srv->cv_work.notify_one();
   return id;
 }

@@ -194,12 +194,13 @@ def serve_poisson(srv: XCServer, mids: list, rate_hz: float, duration_s: float, 
                   sample_frac: float = 0.01, waiters: int = 32):
     """Poisson arrivals at rate_hz over duration_s, each request for a random
     registered molecule with a fresh perturbed density (P0 + 1e-3 S). Returns the
-    per-request latencies (ms, submit to result) and, for a sample_frac sample,
-    (molecule, density, E_xc, K) for spot checks against the FP64 form."""
+    per-request latencies (ms, submit to result), for a sample_frac sample
+    (molecule, density, E_xc, K) for spot checks against the FP64 form, and the
+    number of requests that failed (their errors are not latencies)."""
     import queue
 
     rng = np.random.default_rng(seed)
-    lat, sample = [], []
+    lat, sample, failed = [], [], [0]
     lock = threading.Lock()
     todo = queue.Queue()
 
@@ -209,7 +210,12 @@ def serve_poisson(srv: XCServer, mids: list, rate_hz: float, duration_s: float, 
             if item is None:
                 return
             rid, mid, rho, keep = item
-            e, ka, _, ms = srv.wait(rid, mid)
+            try:
+                e, ka, _, ms = srv.wait(rid, mid)
+            except RuntimeError:
+                with lock:
+                    failed[0] += 1
+                continue
             with lock:
                 lat.append(ms)
                 if keep:
@@ -235,7 +241,7 @@ def serve_poisson(srv: XCServer, mids: list, rate_hz: float, duration_s: float, 
         todo.put(None)
     for th in pool:
         th.join()
-    return lat, sample
+    return lat, sample, failed[0]
 
 
 def run_all(srv: XCServer, mids: list, dens: dict):
