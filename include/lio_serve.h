@@ -17,8 +17,11 @@
  *     CUDA stream per resident molecule);
  *   - admission by HBM footprint: a molecule is made resident only when its
  *     device footprint fits the server's byte budget, evicting idle resident
- *     molecules least recently used first; a request waits in the queue until
- *     its molecule fits.
+ *     molecules least recently used first — their basis-value and tensor-core
+ *     caches first (the molecule keeps its grid and rebuilds them on the device
+ *     when next needed), whole molecules only if that is not enough; a request
+ *     waits in the queue until its molecule fits. Evictions and uploads run on
+ *     a loader thread, so builds of resident molecules continue meanwhile.
  *
  * Every call returns a status (0 = success) or a handle >= 0; on failure the
  * message is read with lio_srv_last_error. Calls are thread-safe; results are
