@@ -96,8 +96,11 @@ int lio_srv_wait(lio_server* srv, long long req, double* energy, double* fock_a,
 /* Service statistics since creation or the last reset: out[0] completed
  * requests, out[1] p50 latency ms, out[2] p99 latency ms, out[3] mean latency
  * ms, out[4] grid points processed, out[5] wall seconds from the first
- * submission to the last completion, out[6] evictions, out[7] uploads,
- * out[8] peak requests in flight. Returns the number of values written (9). */
+ * submission to the last completion, out[6] evictions (whole molecules or their
+ * caches), out[7] uploads (or cache rebuilds), out[8] peak requests in flight,
+ * out[9] loads retried after the device ran out of memory (each shrinks the
+ * budget), out[10] the current HBM budget in bytes. out must hold 11 values;
+ * returns the number written (11). */
 int lio_srv_stats(lio_server* srv, double* out);
 void lio_srv_reset_stats(lio_server* srv);
 

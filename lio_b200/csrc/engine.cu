@@ -84,7 +84,13 @@ struct DevBuf {
   void alloc(size_t count) {
     free();
     if (count == 0) count = 1;
-    LIO_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    const cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) {  // clear the thread's last error: later launch checks must not see it
+      cudaGetLastError();
+      p = nullptr;
+      throw std::runtime_error(std::string("CUDA error ") + cudaGetErrorString(e) + " allocating " +
+                               std::to_string(count * sizeof(T)) + " bytes");
+    }
     n = count;
     g_devbuf_bytes += (long long)(n * sizeof(T));
   }

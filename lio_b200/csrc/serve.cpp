@@ -260,22 +260,30 @@ void lio_server::loader_loop() {
       delta = lio::DeviceEngine::process_device_bytes() - before;
     } catch (const std::exception& ex) {
       err = ex.what();
-      e.reset();  // a partial upload's memory goes before the lock is taken
+      cudaGetLastError();  // an allocation failure is not sticky; clear it for this thread's next launches
+      e.reset();           // a partial upload's memory goes before the lock is taken
       try {
         if (cold) cold->release_caches();
       } catch (...) {
       }
+    }
+    size_t free_now = 0, total = 0;
+    const bool oom = err.find("out of memory") != std::string::npos;
+    if (oom && cudaMemGetInfo(&free_now, &total) != cudaSuccess) {
+      cudaGetLastError();
+      free_now = 0;
     }
     lk.lock();
     for (int i : job.demote) mols[i]->loading = false;
     m.loading = false;
     if (!err.empty()) {
       used -= job.reserved;
-      if (err.find("out of memory") != std::string::npos && budget > job.reserved) {
-        // memory the accounting counted as free is held elsewhere (another
-        // user of the GPU): shrink the budget by this request and let the
-        // request retry, evicting more
-        budget -= job.reserved;
+      const unsigned long long fit = used + (unsigned long long)(0.9 * (double)free_now);
+      if (oom && fit < budget) {
+        // memory the accounting counted as free is held elsewhere (another user
+        // of the GPU): the budget becomes what the server holds plus 90 % of
+        // what is free now, and the request retries, evicting more
+        budget = fit;
         oom_retries++;
       } else {
         m.load_error = err;
@@ -634,7 +642,9 @@ int lio_srv_stats(lio_server* srv, double* out) {
   out[6] = (double)srv->evictions;
   out[7] = (double)srv->uploads;
   out[8] = (double)srv->peak_inflight;
-  return 9;
+  out[9] = (double)srv->oom_retries;
+  out[10] = (double)srv->budget;
+  return 11;
 }
 
 void lio_srv_reset_stats(lio_server* srv) {
@@ -643,7 +653,7 @@ void lio_srv_reset_stats(lio_server* srv) {
   srv->lat_ms.clear();
   srv->points_done = 0.0;
   srv->any_submit = false;
-  srv->evictions = srv->uploads = 0;
+  srv->evictions = srv->uploads = srv->oom_retries = 0;
   srv->peak_inflight = 0;
 }
 

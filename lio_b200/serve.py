@@ -134,10 +134,10 @@ class XCServer:
         return e.value, ka, kb, lat.value
 
     def stats(self) -> dict:
-        out = (C.c_double * 9)()
+        out = (C.c_double * 11)()
         self.L.lio_srv_stats(self.h, out)
         keys = ("completed", "p50_ms", "p99_ms", "mean_ms", "points", "wall_s", "evictions", "uploads",
-                "peak_inflight")
+                "peak_inflight", "oom_retries", "budget")
         return dict(zip(keys, list(out)))
 
     def reset_stats(self):

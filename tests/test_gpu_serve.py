@@ -103,3 +103,36 @@ def test_admission_by_footprint_evicts_and_reuploads():
     st = srv.stats()
     assert st["evictions"] >= 1 and st["uploads"] > len(mids), st
     srv.close()
+
+
+def test_memory_taken_by_another_user_shrinks_the_budget():
+    """After the server sized its budget (90 % of the free HBM), another user of
+    the GPU (a torch allocation here) takes most of that memory. Loads that run
+    out of device memory shrink the budget and are retried after more eviction,
+    so every build still completes and equals the build without the squeeze."""
+    import torch
+
+    wls = _molecules()
+    probe = S.XCServer(precision=1)
+    mids = [probe.add(wl) for wl in wls]
+    dens = {m: S.densities(probe.mols[m][0]) for m in mids}
+    ref = S.run_all(probe, mids, dens)
+    fps = [probe.info(m)["footprint"] for m in mids]
+    probe.close()
+    srv = S.XCServer(precision=1, max_inflight=4)
+    mids2 = [srv.add(wl) for wl in wls]
+    free, _ = torch.cuda.mem_get_info()
+    room = max(fps) + (sum(fps) - max(fps)) // 3 + (256 << 20)  # all molecules never fit at once
+    hog = torch.empty(max(free - room, 0), dtype=torch.uint8, device="cuda")
+    try:
+        for _ in range(2):
+            out = S.run_all(srv, mids2, {m2: dens[m] for m2, m in zip(mids2, mids)})
+            for m2, m in zip(mids2, mids):
+                assert abs(out[m2][0] - ref[m][0]) <= MIX_E
+                assert np.max(np.abs(out[m2][1] - ref[m][1])) <= MIX_K
+        st = srv.stats()
+        assert st["oom_retries"] >= 1 and st["evictions"] >= 1, st
+    finally:
+        srv.close()
+        del hog
+        torch.cuda.empty_cache()
