@@ -252,10 +252,9 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
           for (int c = 0; c < 8; c++) {
             const int j = J * kFkCols + c0 + c;
             if (i >= G.m || j >= G.m || i > j) continue;
-            long long V = 0;
-#pragma unroll
-            for (int l = 0; l < kSlices; l += 2) V = V * (1LL << 14) + (long long)(lv[l][c] * 128 + lv[l + 1][c]);
-            const double v = (double)V * pow2(ea + bexp[G.fbe_off + j] - 7 * (kSlices + 1));
+            // each level converted on its own (the reduction runs over all the
+            // group's points, so level pairs need not fit int32), one rounding
+            const double v = level_sum(lv, c, false) * pow2(ea + bexp[G.fbe_off + j] - 7 * (kSlices + 1));
             atomicAdd(K + packed_index(gi, fn_glob[G.fn_off + j], M), v);
           }
         }
