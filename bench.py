@@ -566,7 +566,10 @@ def serve_mode(args):
             row = {"rate_hz": round(rate, 2), "requests": len(lat), "p50_ms": st["p50_ms"],
                    "p99_ms": st["p99_ms"], "points_per_s": st["points"] / max(st["wall_s"], 1e-9),
                    "peak_inflight": st["peak_inflight"], "evictions": st["evictions"],
-                   "failed": failed}
+                   "failed": failed, "oom_retries": st["oom_retries"]}
+            if srv.last_errors:
+                row["errors"] = sorted(srv.last_errors)[:3]
+                srv.last_errors.clear()
             sweep.append(row)
             samples.append(sample)
         forms = [srv.form(m)[0] for m in mids]

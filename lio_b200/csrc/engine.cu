@@ -1371,15 +1371,8 @@ void DeviceEngine::drop_tensor_core() {
   d->drop_graph();
 }
 
-// The autotuner: one resident build of each form after a warm-up (the density
-// contents do not change the work of either), the faster one kept and the
-// other's buffers released. Memory-aware (for many resident molecules): the
-// tensor-core form is kept only when its time x device-bytes product is the
-// smaller, so a form that buys little time with much more HBM (small groups,
-// whose 32-function tiles are mostly padding) does not crowd other molecules out.
-Precision DeviceEngine::autotune(bool memory_aware) {
+void DeviceEngine::autotune_measure(double* fp64_ms, double* tc_ms, size_t* fp64_cache, size_t* tc_cache) {
   Impl* d = impl_.get();
-  if (d->ngroups == 0) return precision_;
   auto time_form = [&](Precision p) {
     set_precision(p);
     SolveRequest req;
@@ -1397,21 +1390,40 @@ Precision DeviceEngine::autotune(bool memory_aware) {
     LIO_CUDA(cudaEventElapsedTime(&ms, a, b));
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    return ms;
+    return ms / 2;
   };
-  const long long b0 = g_devbuf_bytes.load();
-  const float t64 = time_form(Precision::FP64);
-  const long long b64 = g_devbuf_bytes.load() - b0;
-  const float ttc = time_form(Precision::TensorCore);  // its operands replace the FP64 cache
-  const long long btc = g_devbuf_bytes.load() - b0;
-  d->tuned_fp64_ms = t64 / 2;
-  d->tuned_tc_ms = ttc / 2;
-  const bool tc_wins = memory_aware ? (double)ttc * (double)(btc + 1) < (double)t64 * (double)(b64 + 1) : ttc < t64;
-  if (!tc_wins) {
+  d->tuned_fp64_ms = time_form(Precision::FP64);
+  *fp64_cache = cache_bytes();
+  d->tuned_tc_ms = time_form(Precision::TensorCore);  // its operands replace the FP64 cache
+  *tc_cache = cache_bytes();
+  *fp64_ms = d->tuned_fp64_ms;
+  *tc_ms = d->tuned_tc_ms;
+}
+
+void DeviceEngine::keep_form(Precision p) {
+  Impl* d = impl_.get();
+  if (p == Precision::FP64) {
     drop_tensor_core();
     set_precision(Precision::FP64);
-    if (!d->basis_valid) d->compute_basis();
+    if (!d->basis_valid && d->ngroups > 0) d->compute_basis();
+  } else {
+    set_precision(Precision::TensorCore);
+    prepare();
   }
+}
+
+// The autotuner: one resident build of each form after a warm-up (the density
+// contents do not change the work of either), the faster one kept and the
+// other's caches released. Memory-aware: the tensor-core form is kept only when
+// its time x cache-bytes product is the smaller.
+Precision DeviceEngine::autotune(bool memory_aware) {
+  Impl* d = impl_.get();
+  if (d->ngroups == 0) return precision_;
+  double t64 = 0, ttc = 0;
+  size_t c64 = 0, ctc = 0;
+  autotune_measure(&t64, &ttc, &c64, &ctc);
+  const bool tc_wins = memory_aware ? ttc * (double)(ctc + 1) < t64 * (double)(c64 + 1) : ttc < t64;
+  keep_form(tc_wins ? Precision::TensorCore : Precision::FP64);
   return precision_;
 }
 

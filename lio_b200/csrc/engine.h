@@ -112,6 +112,11 @@ class DeviceEngine {
   // the accuracy bar; memory_aware: the smaller time x device-bytes product)
   // and releases the other's device buffers; returns it.
   Precision autotune(bool memory_aware = false);
+  // The autotuner's measurement alone: ms per resident build of each form and
+  // the bytes of each form's per-geometry caches; leaves the tensor-core form
+  // active. keep_form() then keeps one form and releases the other's caches.
+  void autotune_measure(double* fp64_ms, double* tc_ms, size_t* fp64_cache, size_t* tc_cache);
+  void keep_form(Precision p);
   void tuned_times(double* fp64_ms, double* tc_ms) const;
   // releases the tensor-core operands (rebuilt by the next tensor-core solve)
   void drop_tensor_core();

@@ -114,6 +114,7 @@ struct LoadJob {
   std::vector<int> demote;                               // idle molecules whose caches go
   std::vector<std::unique_ptr<lio::DeviceEngine>> drop;  // engines of molecules evicted whole
   unsigned long long reserved = 0;                       // bytes booked for `mol`
+  unsigned long long room = 0;                           // budget minus the other molecules' bytes, at booking
 };
 
 struct lio_server {
@@ -205,6 +206,7 @@ bool lio_server::plan_load(int mi, std::string& why) {
     why = need > budget ? "molecule footprint exceeds the server's HBM budget" : "";
     return false;
   }
+  job.room = budget > used ? budget - used : 0;
   used += need;
   job.mol = mi;
   job.reserved = need;
@@ -247,9 +249,25 @@ void lio_server::loader_loop() {
           e->upload(m.sys, m.part);
           e->prepare();
         } else if (autotune) {
-          e->upload(m.sys, m.part);
-          new_form = e->autotune(true) == lio::Precision::TensorCore ? 1 : 0;
-          e->tuned_times(&tuned[0], &tuned[1]);
+          // both forms timed alone; the tensor-core form is kept only when it is
+          // at least twice as fast, its time x device-bytes product (whole
+          // footprint) is the smaller, and it takes at most half of the room the
+          // molecule was booked in. Twice: its kernels are persistent (one CTA per
+          // SM), so among other molecules' builds they lose the overlap the FP64
+          // form's kernels get. Bytes: a form that buys time with proportionally
+          // more HBM (small groups, whose 32-function tiles are mostly padding)
+          // would crowd the other molecules out and turn into evictions.
+          e->upload(m.sys, m.part);  // FP64 form: grid plus its basis cache
+          const long long up = lio::DeviceEngine::process_device_bytes() - before;
+          size_t c64 = 0, ctc = 0;
+          e->autotune_measure(&tuned[0], &tuned[1], &c64, &ctc);
+          const double core = (double)std::max<long long>(up - (long long)c64, 0);
+          const double fp64 = core + (double)c64, fptc = core + (double)ctc;
+          const bool faster = 2.0 * tuned[1] < tuned[0];
+          const bool plenty = fptc <= 0.5 * (double)job.room;
+          const bool tc = faster && plenty && tuned[1] * fptc < tuned[0] * fp64;
+          e->keep_form(tc ? lio::Precision::TensorCore : lio::Precision::FP64);
+          new_form = tc ? 1 : 0;
         } else {
           e->set_precision(precision);
           e->upload(m.sys, m.part);

@@ -85,6 +85,7 @@ class XCServer:
         L.lio_srv_reset_stats.argtypes = [C.c_void_p]
         self.L = L
         self.h = L.lio_srv_create(device, budget_bytes, precision, max_inflight)
+        self.last_errors = set()
         if not self.h:
             raise RuntimeError("lio_srv_create failed (no CUDA device?)")
         self.mols = {}
@@ -196,7 +197,8 @@ def serve_poisson(srv: XCServer, mids: list, rate_hz: float, duration_s: float, 
     registered molecule with a fresh perturbed density (P0 + 1e-3 S). Returns the
     per-request latencies (ms, submit to result), for a sample_frac sample
     (molecule, density, E_xc, K) for spot checks against the FP64 form, and the
-    number of requests that failed (their errors are not latencies)."""
+    number of requests that failed (their errors are not latencies; the distinct
+    messages are kept in srv.last_errors)."""
     import queue
 
     rng = np.random.default_rng(seed)
@@ -212,9 +214,10 @@ def serve_poisson(srv: XCServer, mids: list, rate_hz: float, duration_s: float, 
             rid, mid, rho, keep = item
             try:
                 e, ka, _, ms = srv.wait(rid, mid)
-            except RuntimeError:
+            except RuntimeError as ex:
                 with lock:
                     failed[0] += 1
+                    srv.last_errors.add(str(ex)[:200])
                 continue
             with lock:
                 lat.append(ms)
