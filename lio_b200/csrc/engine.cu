@@ -542,7 +542,7 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
 // energy and potential stay zero). Compile-time so the per-point sums live in
 // registers.
 template <int MODE>
-__global__ void __launch_bounds__(kFuncBlock) k_functional(const int2* __restrict__ tiles,
+__global__ void __launch_bounds__(kFuncBlock, 8) k_functional(const int2* __restrict__ tiles,
                                                            const GroupDev* __restrict__ groups,
                                                            const double* __restrict__ pw,
                                                            const double* __restrict__ part_a,
