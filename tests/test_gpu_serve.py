@@ -5,8 +5,8 @@
   different densities) are submitted at once so they overlap on the device; the
   results agree to summation-order noise of the Kohn-Sham atomics.
 * The service's result equals the single-molecule C ABI (g2g_solve_groups_) on
-  the same molecule and density, and the FP64 form within the north-star
-  tolerances.
+  the same molecule and density, and the FP64 form within the parity
+  tolerances (tests/helpers.py).
 * Admission by HBM footprint: with a budget that holds only some molecules,
   builds still complete correctly while residents are evicted and re-uploaded.
 """
