@@ -180,6 +180,18 @@ void g2g_set_graphs_(const unsigned int* on);
 void g2g_profile_(const unsigned int* on);
 int g2g_stage_times_(double* ms, int* solves);
 
+/* No counterpart in the reference: external accumulators for device-resident
+ * solves (g2g_solve_resident_). With device pointers set, each resident
+ * solve's Kohn-Sham contraction adds (+=) its contributions into d_fock_a
+ * (and d_fock_b for open shell) with its own FP64 atomics, and its E_xc into
+ * *d_energy, instead of into the engine's buffers; the caller zeroes them. The
+ * shards of a build (g2g_set_shard_) on several GPUs can all be given one
+ * GPU's buffers, mapped into every process over NVLink (CUDA IPC or symmetric
+ * memory), so that the contraction itself performs the cross-GPU sum and no
+ * separate all-reduce follows. All three NULL: off. Replaces the result
+ * buffers of g2g_copy_resident_results_ while set. */
+void g2g_set_accumulators_(double* d_fock_a, double* d_fock_b, double* d_energy);
+
 /* No counterpart in the reference: where the Becke weights of a grid build
  * (g2g_reload_atom_positions_, g2g_new_grid_) are computed. 1 (default): on
  * the GPU when one is present, one thread per point with explicitly rounded

@@ -613,12 +613,19 @@ void launch_functional(bool lda, bool open, unsigned nblocks, cudaStream_t st, c
                                                     eblocks);
 }
 
-__global__ void k_sum_blocks(const double* __restrict__ in, int n, double* __restrict__ out) {
+// E_xc of the build from the per-block partials: written, or (accumulate) added
+// to an external accumulator that other shards of the build also add to
+__global__ void k_sum_blocks(const double* __restrict__ in, int n, double* __restrict__ out, int accumulate) {
   __shared__ double sh[32];
   double v = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) v += in[i];
   v = block_sum(v, sh);
-  if (threadIdx.x == 0) *out = v;
+  if (threadIdx.x == 0) {
+    if (accumulate)
+      atomicAdd(out, v);
+    else
+      *out = v;
+  }
 }
 
 // ------------------------------------------------ Kohn-Sham update (FP64 GEMM)
@@ -779,6 +786,7 @@ struct DeviceEngine::Impl {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t fev0 = nullptr, fev1 = nullptr;  // around the force kernel
+  double *ext_ka = nullptr, *ext_kb = nullptr, *ext_e = nullptr;  // external accumulators (resident solves)
   double last_force_ms = 0.0;
   int launches = 0;
   bool profiling = false;
@@ -891,6 +899,16 @@ void DeviceEngine::becke_weights(const System& sys, const std::vector<PointGroup
     for (GridPoint& p : g->points) p.w *= hf[(size_t)k++];
 }
 double DeviceEngine::last_force_kernel_ms() const { return impl_->last_force_ms; }
+
+void DeviceEngine::set_accumulators(double* d_fock_a, double* d_fock_b, double* d_energy) {
+  Impl* d = impl_.get();
+  if (d_fock_a && (!d_energy || (d->open && !d_fock_b)))
+    throw std::runtime_error("accumulators: the energy (and for open shell the beta matrix) are needed too");
+  d->ext_ka = d_fock_a;
+  d->ext_kb = d_fock_a ? d_fock_b : nullptr;
+  d->ext_e = d_fock_a ? d_energy : nullptr;
+  d->drop_graph();  // the pointers are part of a captured build
+}
 void DeviceEngine::set_stream(void* s) {
   impl_->stream = s ? (cudaStream_t)s : impl_->own_stream;
 }
@@ -1200,10 +1218,13 @@ void DeviceEngine::prepare_tensor_core() {
 }
 
 // The device work of one solve, from the densities in d->P_a / d->P_b to E_xc in
-// d->energy and the Kohn-Sham contributions in d->K_a / d->K_b; captured once
-// into a CUDA graph when graphs are on. Returns the number of kernel launches.
-int DeviceEngine::run_kernels(bool compute_rmm) {
+// d->energy and the Kohn-Sham contributions in d->K_a / d->K_b (ext: added into
+// the external accumulators instead); captured once into a CUDA graph when
+// graphs are on. Returns the number of kernel launches.
+int DeviceEngine::run_kernels(bool compute_rmm, bool ext) {
   Impl* d = impl_.get();
+  double* Ka = ext ? d->ext_ka : d->K_a.p;
+  double* Kb = ext ? d->ext_kb : d->K_b.p;
   const size_t npacked = (size_t)d->M * (d->M + 1) / 2;
   cudaStream_t st = d->stream;
   int launches = 0;
@@ -1258,13 +1279,15 @@ int DeviceEngine::run_kernels(bool compute_rmm) {
                     d->open ? d->part_b.p : nullptr, tc ? (1 << 30) : kTile, d->iexch, d->fac_a.p,
                     d->open ? d->fac_b.p : nullptr, d->eblocks.p);
   LIO_CUDA(cudaGetLastError());
-  k_sum_blocks<<<1, 1024, 0, st>>>(d->eblocks.p, (int)nf, d->energy.p);
+  k_sum_blocks<<<1, 1024, 0, st>>>(d->eblocks.p, (int)nf, ext ? d->ext_e : d->energy.p, ext ? 1 : 0);
   LIO_CUDA(cudaGetLastError());
   launches += 2;
   d->mark(3);
   if (compute_rmm) {
-    LIO_CUDA(cudaMemsetAsync(d->K_a.p, 0, npacked * sizeof(double), st));
-    if (d->open) LIO_CUDA(cudaMemsetAsync(d->K_b.p, 0, npacked * sizeof(double), st));
+    if (!ext) {  // an external accumulator is zeroed by its owner, once for all shards
+      LIO_CUDA(cudaMemsetAsync(d->K_a.p, 0, npacked * sizeof(double), st));
+      if (d->open) LIO_CUDA(cudaMemsetAsync(d->K_b.p, 0, npacked * sizeof(double), st));
+    }
     if (tc) {
       // f * F slices of both spins: row exponents, then the slices (one pass over F each)
       const int nrows = (int)d->fb_rows.n;
@@ -1291,19 +1314,19 @@ int DeviceEngine::run_kernels(bool compute_rmm) {
       if (d->open)
         k_fock_tc<2><<<(unsigned)d->fk_tiles.n, FkCfg<2>::kThreads, FkCfg<2>::kSmem, st>>>(
             d->fk_tiles.p, d->groups.p, d->fn_glob.p, d->fa_slices.p, d->fa_exp.p, d->fb_slices_a.p, d->fb_exp_a.p,
-            d->fb_slices_b.p, d->fb_exp_b.p, d->M, d->K_a.p, d->K_b.p, d->tc_err.p);
+            d->fb_slices_b.p, d->fb_exp_b.p, d->M, Ka, Kb, d->tc_err.p);
       else
         k_fock_tc<1><<<(unsigned)d->fk_tiles.n, FkCfg<1>::kThreads, FkCfg<1>::kSmem, st>>>(
             d->fk_tiles.p, d->groups.p, d->fn_glob.p, d->fa_slices.p, d->fa_exp.p, d->fb_slices_a.p, d->fb_exp_a.p,
-            nullptr, nullptr, d->M, d->K_a.p, nullptr, d->tc_err.p);
+            nullptr, nullptr, d->M, Ka, nullptr, d->tc_err.p);
     } else if (d->open) {
       d->mark(4);  // no operand preparation in the FP64 form
       k_fock_fp64<2><<<nk, 256, 0, st>>>(d->fock_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, d->fac_a.p,
-                                         d->fac_b.p, d->M, d->K_a.p, d->K_b.p);
+                                         d->fac_b.p, d->M, Ka, Kb);
     } else {
       d->mark(4);
       k_fock_fp64<1><<<nk, 256, 0, st>>>(d->fock_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, d->fac_a.p,
-                                         nullptr, d->M, d->K_a.p, nullptr);
+                                         nullptr, d->M, Ka, nullptr);
     }
     LIO_CUDA(cudaGetLastError());
     launches++;
@@ -1478,7 +1501,8 @@ void DeviceEngine::enqueue(const SolveRequest& req) {
     LIO_CUDA(cudaMemcpyAsync(d->P_a.p, req.rho, npacked * sizeof(double), cudaMemcpyHostToDevice, st));
   }
   // graph replay when on (not while profiling: the stage events are recorded eagerly)
-  const int key = (tc ? 2 : 0) | (req.compute_rmm ? 1 : 0);
+  const bool ext = req.resident && d->ext_ka != nullptr;
+  const int key = (tc ? 2 : 0) | (req.compute_rmm ? 1 : 0) | (ext ? 4 : 0);
   if (d->use_graphs && !d->profiling) {
     if (!d->graph_exec || d->graph_key != key) {
       d->drop_graph();
@@ -1486,7 +1510,7 @@ void DeviceEngine::enqueue(const SolveRequest& req) {
       LIO_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
       int n = 0;
       try {
-        n = run_kernels(req.compute_rmm);
+        n = run_kernels(req.compute_rmm, ext);
       } catch (...) {
         cudaStreamEndCapture(st, &g);
         if (g) cudaGraphDestroy(g);
@@ -1501,7 +1525,7 @@ void DeviceEngine::enqueue(const SolveRequest& req) {
     LIO_CUDA(cudaGraphLaunch(d->graph_exec, st));
     d->launches = d->graph_launches;
   } else {
-    d->launches = run_kernels(req.compute_rmm);
+    d->launches = run_kernels(req.compute_rmm, ext);
     d->pending = d->profiling;
   }
   if (!req.resident) {
@@ -1726,7 +1750,7 @@ void DeviceEngine::solve_noalloc(const double* rho_a, const double* rho_b, doubl
     launch_functional(d->lda, d->open, (unsigned)nf, st, d->func_tiles.p + ft0, d->groups.p, d->pw.p, pa,
                       d->open ? pb : nullptr, kTile, d->iexch, fa, d->open ? fb : nullptr, eblk);
     LIO_CUDA(cudaGetLastError());
-    k_sum_blocks<<<1, 1024, 0, st>>>(eblk, (int)nf, eparts + nbatch);
+    k_sum_blocks<<<1, 1024, 0, st>>>(eblk, (int)nf, eparts + nbatch, 0);
     LIO_CUDA(cudaGetLastError());
     if (d->open)
       k_fock_fp64<2><<<(unsigned)nk, 256, 0, st>>>(d->fock_tiles.p + kt0, d->groups.p, d->fn_glob.p, d->basis.p,
@@ -1741,7 +1765,7 @@ void DeviceEngine::solve_noalloc(const double* rho_a, const double* rho_b, doubl
     nbatch++;
     g0 = g1;
   }
-  k_sum_blocks<<<1, 1024, 0, st>>>(eparts, nbatch, energy);
+  k_sum_blocks<<<1, 1024, 0, st>>>(eparts, nbatch, energy, 0);
   LIO_CUDA(cudaGetLastError());
 }
 

@@ -64,6 +64,12 @@ class DeviceEngine {
   SolveResult solve_forces(const SolveRequest& req, double* forces, int ld);
   // device ms of the last solve_forces' force kernel (CUDA events around it)
   double last_force_kernel_ms() const;
+  // External accumulators for resident solves (nullptr: off): the Kohn-Sham
+  // contraction's FP64 atomics and the energy sum add (+=) into these device
+  // buffers, which the caller zeroes, instead of the engine's own. Shards of a
+  // build on several GPUs can all add into one GPU's buffers, mapped into each
+  // process over NVLink, so the contraction itself does the cross-GPU sum.
+  void set_accumulators(double* d_fock_a, double* d_fock_b, double* d_energy);
   // Replay the kernels of a solve from a CUDA graph captured on first use
   // (re-captured after a new geometry or precision).
   void set_graphs(bool on);
@@ -134,7 +140,7 @@ class DeviceEngine {
 
  private:
   void prepare_tensor_core();
-  int run_kernels(bool compute_rmm);
+  int run_kernels(bool compute_rmm, bool ext = false);
   void set_graphs_dirty();
   struct Impl;
   std::unique_ptr<Impl> impl_;

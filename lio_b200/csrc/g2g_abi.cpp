@@ -427,6 +427,14 @@ void g2g_profile_(const unsigned* on) {
   });
 }
 
+void g2g_set_accumulators_(double* d_fock_a, double* d_fock_b, double* d_energy) {
+  guarded("g2g_set_accumulators_", [&] {
+    State& s = st();
+    if (!s.engine) throw std::runtime_error("no device engine: build a grid first");
+    s.engine->set_accumulators(d_fock_a, d_fock_b, d_energy);
+  });
+}
+
 void g2g_set_device_weights_(const unsigned* on) {
   guarded("g2g_set_device_weights_", [&] { st().device_weights = *on != 0; });
 }

@@ -39,3 +39,45 @@ def test_shards_add_up_to_the_whole_build(precision, world):
     assert abs(Es - E) <= 1e-10
     assert np.max(np.abs(Ks - K)) <= 1e-12
     assert np.max(np.abs(Kbs - Kb)) <= 1e-12
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_shards_accumulate_into_one_set_of_buffers(precision):
+    """g2g_set_accumulators_: every shard's resident solve adds its Kohn-Sham
+    contributions (the contraction's own atomics) and E_xc into the same device
+    buffers, as the shards of a multi-GPU build add into one GPU's buffers over
+    NVLink; the buffers then hold the whole build without any reduction step."""
+    import torch
+
+    wl = W.small_workload(14, 77, 9, True, n_ang=302)
+    L = H.lib(PROD, True)
+    E, K, Kb = _share(L, wl, 0, 1, precision)
+    npk = K.size
+    acc = torch.zeros(2 * npk + 1, dtype=torch.float64, device="cuda")
+    pa, pb, pe = (C.c_void_p(acc.data_ptr() + 8 * o) for o in (0, npk, 2 * npk))
+    L.lib.g2g_solve_resident_.restype = C.c_int
+    world = 3
+    for r in range(world):
+        L.lib.g2g_set_shard_(C.byref(C.c_int(r)), C.byref(C.c_int(world)))
+        try:
+            gt = H.bind(L, wl)
+            L.set_precision(precision)
+            assert not L.reload_atom_positions(gt)
+            L.solve_groups(0)  # uploads the densities; resident solves reuse them
+            L.lib.g2g_set_accumulators_(pa, pb, pe)
+            L.check("g2g_set_accumulators_")
+            for _ in range(2 if r == 0 else 1):  # the first shard twice: graph capture, then replay
+                if r == 0:
+                    acc.zero_()
+                torch.cuda.synchronize()  # the library's stream is not torch's
+                assert L.lib.g2g_solve_resident_() > 0
+                L.check("g2g_solve_resident_")
+                torch.cuda.synchronize()
+        finally:
+            L.lib.g2g_set_accumulators_(None, None, None)
+            L.lib.g2g_set_shard_(C.byref(C.c_int(0)), C.byref(C.c_int(1)))
+    torch.cuda.synchronize()
+    out = acc.cpu().numpy()
+    assert abs(out[2 * npk] - E) <= 1e-10
+    assert np.max(np.abs(out[:npk] - K)) <= 1e-12
+    assert np.max(np.abs(out[npk:2 * npk] - Kb)) <= 1e-12
