@@ -35,7 +35,6 @@ constexpr int kTcSliceA = 32 * kTcPoints;    // bytes of one A slice per 32-byte
 constexpr int kTcStepA = kSlices * kTcSliceA;  // one kind's A slices per K step (contiguous)
 constexpr int kTcStepD = 32 * kTcTall;         // one spin's stacked D slices per K step (contiguous)
 constexpr int kTcChunk = kTcFuncs * kTcPoints;  // doubles of one blocked basis chunk (kind, 32 functions)
-constexpr int kTcMaxFnCap = 512; // functions per group the shared memory leaves table room for
 
 // KP = kinds per unit: all NS x KP x S x 32 level columns of a unit fit in 384
 // TMEM columns. Open shell: one kind per unit (F, x, y, z); closed shell GGA:

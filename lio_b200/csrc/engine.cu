@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <limits>
 #include <cstdio>
 #include <cstring>
 #include <stdexcept>
@@ -1417,8 +1418,17 @@ void DeviceEngine::autotune_measure(double* fp64_ms, double* tc_ms, size_t* fp64
   };
   d->tuned_fp64_ms = time_form(Precision::FP64);
   *fp64_cache = cache_bytes();
-  d->tuned_tc_ms = time_form(Precision::TensorCore);  // its operands replace the FP64 cache
-  *tc_cache = cache_bytes();
+  try {
+    d->tuned_tc_ms = time_form(Precision::TensorCore);  // its operands replace the FP64 cache
+    *tc_cache = cache_bytes();
+  } catch (const std::exception&) {
+    // a form this molecule cannot run (e.g. a group too large for the tensor-core
+    // kernel's shared memory): it is never the faster
+    cudaGetLastError();
+    drop_tensor_core();
+    d->tuned_tc_ms = std::numeric_limits<double>::infinity();
+    *tc_cache = 0;
+  }
   *fp64_ms = d->tuned_fp64_ms;
   *tc_ms = d->tuned_tc_ms;
 }
