@@ -43,6 +43,32 @@ def bind(L, wl, grid_type=2, options=None):
     return 3
 
 
+def subset_tables(n):
+    """The first n directions of the 194-point table with their weights scaled to
+    sum to 4 pi: a caller table for grid types 0 (n = 50) and 1 (n = 116) that
+    both libraries receive alike (parity needs the same table, not a Lebedev one)."""
+    e, w = angular_tables(194)
+    e, w = np.asfortranarray(e[:n]), np.ascontiguousarray(w[:n])
+    return e, w * (4.0 * np.pi / w.sum())
+
+
+def run_grid_type(L, wl, grid_type, precision=None, options=None):
+    """(E, fock, fockb) of one build on grid type 0 (50 directions, radial table
+    Nr) or 1 (116 directions, Nr2), the tables passed through g2g_parameter_init_."""
+    opts = dict(eai=True)
+    if options:
+        opts.update(options)
+    L.set_options(**opts)
+    L.bind_workload(wl, {0: subset_tables(50), 1: subset_tables(116)})
+    if precision is not None:
+        L.set_precision(precision)
+    msg = L.reload_atom_positions(grid_type)
+    if msg:
+        raise RuntimeError(msg)
+    E = L.solve_groups(0)
+    return E, L.fock.copy(), L.fockb.copy()
+
+
 def run(L, wl, calls=1, options=None, precision=None):
     """Returns (E, fock, fockb) after `calls` solves (each accumulates into the
     caller's Fock vectors, like consecutive SCF iterations without a reset)."""

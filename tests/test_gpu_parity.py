@@ -82,3 +82,19 @@ def test_tensor_core_matches_restatement_302(name, make):
     assert np.max(np.abs(K - K_ref)) <= H.K_TOL
     if wl.open_shell:
         assert np.max(np.abs(Kb - Kb_ref)) <= H.K_TOL
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("grid_type", [0, 1])
+def test_grid_types_0_1_match_reference(grid_type, precision):
+    """Grid types 0 and 1 (their own radial and angular tables) through both forms."""
+    wl = W.small_workload(10, 23, 9, True)
+    R = H.lib(H.REF_LIB, False)
+    R.init()
+    E_ref, K_ref, Kb_ref = H.run_grid_type(R, wl, grid_type)
+    R.deinit()
+    P = H.lib(H.os.path.join(H.ROOT, "lio_b200", "libg2g_b200.so"), True)
+    E, K, Kb = H.run_grid_type(P, wl, grid_type, precision=precision)
+    assert abs(E - E_ref) <= H.E_TOL, (E, E_ref)
+    assert np.max(np.abs(K - K_ref)) <= H.K_TOL
+    assert np.max(np.abs(Kb - Kb_ref)) <= H.K_TOL

@@ -73,3 +73,31 @@ def test_partition_matches_golden_summary(name):
     o = np.lexsort((wsum, nfun, npts))
     assert np.array_equal(npts[o], g["npts"]) and np.array_equal(nfun[o], g["nfun"])
     assert np.array_equal(wsum[o], g["wsum"])
+
+
+@pytest.mark.skipif(not os.path.exists(H.REF_LIB), reason="reference build absent")
+@pytest.mark.parametrize("grid_type", [0, 1])
+def test_partition_bit_exact_vs_reference_grid_types_0_1(grid_type):
+    """Grid types 0 (radial table Nr, 50 directions) and 1 (Nr2, 116) select
+    their tables as g2g/init.cpp:238-266 does."""
+    wl = W.small_workload(10, 23, 9, False)
+    tables = {0: H.subset_tables(50), 1: H.subset_tables(116)}
+
+    def groups(path, product):
+        L = H.lib(path, product)
+        if not product:
+            L.init()
+        L.set_options(eai=True)
+        L.bind_workload(wl, tables)
+        L.reload_atom_positions(grid_type)
+        out = {}
+        for g in range(L.num_groups(ref=not product)):
+            d = L.partition_group(g, ref=not product)
+            out[tuple(sorted(map(tuple, d["ids"].tolist())))] = d
+        if not product:
+            L.deinit()
+        return out
+
+    prod, ref = groups(PROD, True), groups(H.REF_LIB, False)
+    assert_same(prod, ref)
+    assert len(prod) > 0
