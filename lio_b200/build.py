@@ -31,7 +31,7 @@ CXXFLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-fopenmp", "-fvi
             "-I" + os.path.join(CUDA_HOME, "include"),
             "-Wall", "-Wextra", "-Wno-unused-parameter"]
 NVCCFLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-             "-Xcompiler", "-fPIC,-fvisibility=hidden", "--expt-relaxed-constexpr", "-Xptxas", "-v"]
+             "-Xcompiler", "-fPIC,-fvisibility=hidden,-fopenmp", "--expt-relaxed-constexpr", "-Xptxas", "-v"]
 
 
 def _stale(target: str, deps: list[str]) -> bool:

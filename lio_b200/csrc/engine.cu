@@ -110,6 +110,17 @@ struct DevBuf {
   ~DevBuf() { free(); }
 };
 
+// Host copies of the packed matrices (millions of doubles for a few thousand
+// functions), threaded: dst = src, and dst += src.
+void host_copy(double* dst, const double* src, size_t n) {
+#pragma omp parallel for schedule(static) if (n > (1u << 16))
+  for (long long i = 0; i < (long long)n; i++) dst[i] = src[i];
+}
+void host_accumulate(double* dst, const double* src, size_t n) {
+#pragma omp parallel for schedule(static) if (n > (1u << 16))
+  for (long long i = 0; i < (long long)n; i++) dst[i] += src[i];
+}
+
 __device__ __forceinline__ long long packed_index(int gi, int gj, int M) {
   const long long lo = gi < gj ? gi : gj, hi = gi < gj ? gj : gi;
   return lo * M - (lo * (lo - 1)) / 2 + (hi - lo);
@@ -741,6 +752,7 @@ struct DeviceEngine::Impl {
   DevBuf<int4> dens_tiles, fock_tiles;
   DevBuf<double> P_a, P_b, K_a, K_b, part_a, part_b, fac_a, fac_b, eblocks, energy;
   double* hK = nullptr;  // pinned: Kohn-Sham result of the last solve (nspin x npacked)
+  double* hP = nullptr;  // pinned: staging of the caller's densities (nspin x npacked)
   double* hE = nullptr;  // pinned: its energy
   int* hErr = nullptr;   // pinned: the tensor-core error flag
   bool enqueued = false;
@@ -778,6 +790,8 @@ struct DeviceEngine::Impl {
   }
   void free_pinned() {
     if (hK) cudaFreeHost(hK);
+    if (hP) cudaFreeHost(hP);
+    hP = nullptr;
     if (hE) cudaFreeHost(hE);
     if (hErr) cudaFreeHost(hErr);
     hK = hE = nullptr;
@@ -1131,6 +1145,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
   d->drop_graph();
   d->free_pinned();
   LIO_CUDA(cudaMallocHost(&d->hK, npacked * (sys.open ? 2 : 1) * sizeof(double)));
+  LIO_CUDA(cudaMallocHost(&d->hP, npacked * (sys.open ? 2 : 1) * sizeof(double)));
   LIO_CUDA(cudaMallocHost(&d->hE, sizeof(double)));
   LIO_CUDA(cudaMallocHost(&d->hErr, sizeof(int)));
   *d->hErr = 0;
@@ -1502,13 +1517,16 @@ void DeviceEngine::enqueue(const SolveRequest& req) {
   }
   d->collect();
   LIO_CUDA(cudaEventRecord(d->ev0, st));
-  if (req.resident) {
-    // density already on the device
-  } else if (d->open) {
-    LIO_CUDA(cudaMemcpyAsync(d->P_a.p, req.rho_a, npacked * sizeof(double), cudaMemcpyHostToDevice, st));
-    LIO_CUDA(cudaMemcpyAsync(d->P_b.p, req.rho_b, npacked * sizeof(double), cudaMemcpyHostToDevice, st));
-  } else {
-    LIO_CUDA(cudaMemcpyAsync(d->P_a.p, req.rho, npacked * sizeof(double), cudaMemcpyHostToDevice, st));
+  if (!req.resident) {
+    // the caller's (pageable) densities through pinned staging: a threaded host
+    // copy, then one full-speed copy per spin
+    const int nspin = d->open ? 2 : 1;
+    for (int s = 0; s < nspin; s++) {
+      const double* src = d->open ? (s == 0 ? req.rho_a : req.rho_b) : req.rho;
+      host_copy(d->hP + s * npacked, src, npacked);
+      LIO_CUDA(cudaMemcpyAsync(s == 0 ? d->P_a.p : d->P_b.p, d->hP + s * npacked, npacked * sizeof(double),
+                               cudaMemcpyHostToDevice, st));
+    }
   }
   // graph replay when on (not while profiling: the stage events are recorded eagerly)
   const bool ext = req.resident && d->ext_ka != nullptr;
@@ -1573,9 +1591,7 @@ SolveResult DeviceEngine::finish(const SolveRequest& req) {
   if (req.compute_rmm) {
     const int nspin = d->open ? 2 : 1;
     for (int s = 0; s < nspin; s++) {
-      double* dst = s == 0 ? req.fock : req.fock_b;
-      const double* src = d->hK + s * npacked;
-      for (size_t i = 0; i < npacked; i++) dst[i] += src[i];
+      host_accumulate(s == 0 ? req.fock : req.fock_b, d->hK + s * npacked, npacked);
     }
   }
   float ms = 0.f;
