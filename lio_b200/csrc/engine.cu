@@ -801,6 +801,11 @@ struct DeviceEngine::Impl {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t fev0 = nullptr, fev1 = nullptr;  // around the force kernel
+  // chunked result download: the host adds each chunk of the Kohn-Sham matrices
+  // into the caller's vectors while the next one is in flight
+  static constexpr int kMaxChunks = 32;
+  cudaEvent_t kev[kMaxChunks] = {};
+  int nchunks = 0;
   double *ext_ka = nullptr, *ext_kb = nullptr, *ext_e = nullptr;  // external accumulators (resident solves)
   double last_force_ms = 0.0;
   int launches = 0;
@@ -832,6 +837,7 @@ struct DeviceEngine::Impl {
     LIO_CUDA(cudaEventCreate(&ev1));
     LIO_CUDA(cudaEventCreate(&fev0));
     LIO_CUDA(cudaEventCreate(&fev1));
+    for (auto& e : kev) LIO_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     for (auto& e : sev) LIO_CUDA(cudaEventCreate(&e));
   }
   ~Impl() {
@@ -841,6 +847,8 @@ struct DeviceEngine::Impl {
     if (ev1) cudaEventDestroy(ev1);
     if (fev0) cudaEventDestroy(fev0);
     if (fev1) cudaEventDestroy(fev1);
+    for (auto& e : kev)
+      if (e) cudaEventDestroy(e);
     for (auto& e : sev)
       if (e) cudaEventDestroy(e);
     if (own_stream) cudaStreamDestroy(own_stream);
@@ -1521,11 +1529,16 @@ void DeviceEngine::enqueue(const SolveRequest& req) {
     // the caller's (pageable) densities through pinned staging: a threaded host
     // copy, then one full-speed copy per spin
     const int nspin = d->open ? 2 : 1;
+    // in pieces, so that the host copy of one piece overlaps the transfer of the last
+    const size_t piece = std::max<size_t>(npacked / 8, 1 << 16);
     for (int s = 0; s < nspin; s++) {
       const double* src = d->open ? (s == 0 ? req.rho_a : req.rho_b) : req.rho;
-      host_copy(d->hP + s * npacked, src, npacked);
-      LIO_CUDA(cudaMemcpyAsync(s == 0 ? d->P_a.p : d->P_b.p, d->hP + s * npacked, npacked * sizeof(double),
-                               cudaMemcpyHostToDevice, st));
+      double* dst = s == 0 ? d->P_a.p : d->P_b.p;
+      for (size_t o = 0; o < npacked; o += piece) {
+        const size_t n = std::min(piece, npacked - o);
+        host_copy(d->hP + s * npacked + o, src + o, n);
+        LIO_CUDA(cudaMemcpyAsync(dst + o, d->hP + s * npacked + o, n * sizeof(double), cudaMemcpyHostToDevice, st));
+      }
     }
   }
   // graph replay when on (not while profiling: the stage events are recorded eagerly)
@@ -1560,10 +1573,22 @@ void DeviceEngine::enqueue(const SolveRequest& req) {
     const int nspin = d->open ? 2 : 1;
     LIO_CUDA(cudaMemcpyAsync(d->hE, d->energy.p, sizeof(double), cudaMemcpyDeviceToHost, st));
     if (tc) LIO_CUDA(cudaMemcpyAsync(d->hErr, d->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-    if (req.compute_rmm)
-      for (int s = 0; s < nspin; s++)
-        LIO_CUDA(cudaMemcpyAsync(d->hK + s * npacked, s == 0 ? d->K_a.p : d->K_b.p, npacked * sizeof(double),
-                                 cudaMemcpyDeviceToHost, st));
+    d->nchunks = 0;
+    if (req.compute_rmm) {  // nspin x npacked values in up to kMaxChunks pieces, an event after each
+      const size_t total = (size_t)nspin * npacked;
+      const size_t piece = std::max<size_t>((total + Impl::kMaxChunks - 1) / Impl::kMaxChunks, 1 << 16);
+      for (size_t o = 0; o < total; o += piece, d->nchunks++) {
+        const size_t n = std::min(piece, total - o);
+        for (size_t e = o; e < o + n;) {  // a piece may span the two spins' device buffers
+          const int s = (int)(e / npacked);
+          const size_t in_s = e - (size_t)s * npacked, m = std::min(o + n - e, npacked - in_s);
+          LIO_CUDA(cudaMemcpyAsync(d->hK + e, (s == 0 ? d->K_a.p : d->K_b.p) + in_s, m * sizeof(double),
+                                   cudaMemcpyDeviceToHost, st));
+          e += m;
+        }
+        LIO_CUDA(cudaEventRecord(d->kev[d->nchunks], st));
+      }
+    }
   }
   LIO_CUDA(cudaEventRecord(d->ev1, st));
   d->enqueued = true;
@@ -1585,15 +1610,29 @@ SolveResult DeviceEngine::finish(const SolveRequest& req) {
   d->enqueued = false;
   if (req.resident) return res;
   const size_t npacked = (size_t)d->M * (d->M + 1) / 2;
-  LIO_CUDA(cudaEventSynchronize(d->ev1));
-  if (precision_ == Precision::TensorCore && *d->hErr)
+  // the energy and the error flag are downloaded before the first Kohn-Sham piece
+  LIO_CUDA(cudaEventSynchronize(req.compute_rmm && d->nchunks > 0 ? d->kev[0] : d->ev1));
+  if (precision_ == Precision::TensorCore && *d->hErr) {
+    LIO_CUDA(cudaEventSynchronize(d->ev1));
     throw std::runtime_error("tensor-core density: an MMA completion wait timed out");
-  if (req.compute_rmm) {
+  }
+  if (req.compute_rmm) {  // chunk by chunk as they arrive (the same pieces enqueue downloaded)
     const int nspin = d->open ? 2 : 1;
-    for (int s = 0; s < nspin; s++) {
-      host_accumulate(s == 0 ? req.fock : req.fock_b, d->hK + s * npacked, npacked);
+    const size_t total = (size_t)nspin * npacked;
+    const size_t piece = std::max<size_t>((total + Impl::kMaxChunks - 1) / Impl::kMaxChunks, 1 << 16);
+    int c = 0;
+    for (size_t o = 0; o < total; o += piece, c++) {
+      LIO_CUDA(cudaEventSynchronize(d->kev[c]));
+      const size_t n = std::min(piece, total - o);
+      for (size_t e = o; e < o + n;) {
+        const int s = (int)(e / npacked);
+        const size_t in_s = e - (size_t)s * npacked, m = std::min(o + n - e, npacked - in_s);
+        host_accumulate((s == 0 ? req.fock : req.fock_b) + in_s, d->hK + e, m);
+        e += m;
+      }
     }
   }
+  LIO_CUDA(cudaEventSynchronize(d->ev1));
   float ms = 0.f;
   LIO_CUDA(cudaEventElapsedTime(&ms, d->ev0, d->ev1));
   res.energy = *d->hE;
