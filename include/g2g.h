@@ -135,6 +135,12 @@ int g2g_partition_group_(const int* g, int* meta, int* ids, double* xyzw, int* f
  * device work) and of the last partition build (ms, host clock). */
 void g2g_last_timings_(double* solve_ms, double* grid_ms);
 
+/* No counterpart in the reference: wall ms of the last grid build's phases:
+ * phase_ms[0] the partition (grid, screening, Becke weights, ordering),
+ * phase_ms[1] the device upload (arrays, basis values), phase_ms[2] the
+ * autotuner (precision mode 2; else 0). */
+void g2g_grid_timings_(double* phase_ms);
+
 /* Runs all device work of this library on the given cudaStream_t. NULL (the
  * legacy default stream's handle) selects the library's own non-blocking
  * stream, which does not order with the legacy default stream. */

@@ -54,6 +54,7 @@ struct State {
   int status = 0;
   std::string message;
   double last_solve_ms = 0.0, last_grid_ms = 0.0;
+  double grid_phase_ms[3] = {0.0, 0.0, 0.0};  // partition (incl. weights), device upload, autotune
   bool device_ready = false;
   void* stream = nullptr;
   bool graphs = true;
@@ -168,6 +169,8 @@ void build_grid(unsigned grid_type) {
                        dev ? &lio::DeviceEngine::becke_weights : nullptr);
   s.grid_type = (int)grid_type;
   s.last_grid_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  s.grid_phase_ms[0] = s.last_grid_ms;
+  s.grid_phase_ms[1] = s.grid_phase_ms[2] = 0.0;
   // The partition is host work and is kept even without a GPU (so it can be
   // inspected); the device upload and every solve need a CUDA device.
   if (!lio::DeviceEngine::available()) {
@@ -186,9 +189,12 @@ void build_grid(unsigned grid_type) {
   } else {
     s.engine->upload(s.sys, s.part);
   }
+  const double t_up = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  s.grid_phase_ms[1] = t_up - s.grid_phase_ms[0];
   if (s.auto_precision) s.precision = s.engine->autotune();
   s.device_ready = true;
   s.last_grid_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  s.grid_phase_ms[2] = s.last_grid_ms - t_up;
 }
 
 // ---- Fortran-named timers (g2g/timer.cpp:117-296): host wall clock
@@ -555,6 +561,10 @@ int g2g_partition_group_(const int* g, int* meta, int* ids, double* xyzw, int* f
 void g2g_last_timings_(double* solve_ms, double* grid_ms) {
   *solve_ms = st().last_solve_ms;
   *grid_ms = st().last_grid_ms;
+}
+
+void g2g_grid_timings_(double* phase_ms) {
+  for (int i = 0; i < 3; i++) phase_ms[i] = st().grid_phase_ms[i];
 }
 
 void g2g_timer_start_(const char* n, unsigned len) { timer_start(n, len); }
