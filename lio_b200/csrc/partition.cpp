@@ -19,31 +19,50 @@
 namespace lio {
 namespace {
 
-// g2g/partition.cpp:230-254
-bool is_significative(int type /*1,3,6*/, double exponent, double d2, unsigned mfe) {
-  if (type == 1) {
-    return (exponent * d2 < mfe - std::log(std::pow((2. * exponent / M_PI), 3)) / 4);
-  }
-  double x = 1;
-  double delta;
-  const double e = 0.1;
-  double factor = std::pow((2.0 * exponent / M_PI), 3);
-  factor = std::sqrt(factor * 4.0 * exponent);
-  double norm = (type == 3 ? std::sqrt(factor) : std::fabs(factor));
-  do {
-    double div = (type == 3 ? std::log(x) : 2 * std::log(x));
-    double x1 = std::sqrt((mfe - std::log(norm) + div) / exponent);
-    delta = std::fabs(x - x1);
-    x = x1;
-  } while (delta > e);
-  return (std::sqrt(d2) < x);
-}
-
 inline double len3(double x, double y, double z) { return std::sqrt(x * x + y * y + z * z); }
+
+// The significance test of g2g/partition.cpp:230-254 (is_significative), split into its part that
+// depends on the function alone (computed once per function) and the comparison
+// with the squared distance (per cube or sphere): s functions compare
+// exponent * d2 with a bound, p and d functions sqrt(d2) with a radius found by
+// fixed-point iteration. Same expressions, so the same bits as calling
+// is_significative per group.
+struct Screen {
+  std::vector<double> bound;  // per function index f (first component): s bound or p/d radius
+};
+Screen make_screen(const System& sys, const Options& opt, const std::vector<double>& min_exps) {
+  Screen sc;
+  sc.bound.assign(sys.M, 0.0);
+  const unsigned mfe = opt.max_function_exponent;
+  const int s_end = sys.s_funcs, p_end = sys.s_funcs + sys.p_funcs * 3,
+            d_end = sys.s_funcs + sys.p_funcs * 3 + sys.d_funcs * 6;
+  for (int f = 0; f < d_end; f += (f < s_end ? 1 : (f < p_end ? 3 : 6))) {
+    const double exponent = min_exps[f];
+    if (f < s_end) {
+      sc.bound[f] = mfe - std::log(std::pow((2. * exponent / M_PI), 3)) / 4;
+      continue;
+    }
+    const int type = f < p_end ? 3 : 6;
+    double x = 1;
+    double delta;
+    const double e = 0.1;
+    double factor = std::pow((2.0 * exponent / M_PI), 3);
+    factor = std::sqrt(factor * 4.0 * exponent);
+    double norm = (type == 3 ? std::sqrt(factor) : std::fabs(factor));
+    do {
+      double div = (type == 3 ? std::log(x) : 2 * std::log(x));
+      double x1 = std::sqrt((mfe - std::log(norm) + div) / exponent);
+      delta = std::fabs(x - x1);
+      x = x1;
+    } while (delta > e);
+    sc.bound[f] = x;
+  }
+  return sc;
+}
 
 // g2g/classify_functions.cpp:13-65: walks s, then p (stride 3), then d (stride 6).
 void assign_functions(const System& sys, const Options& opt, const std::vector<double>& dists,
-                      const std::vector<double>& min_exps, PointGroup& g) {
+                      const std::vector<double>& min_exps, const Screen& sc, PointGroup& g) {
   std::set<int> nuc_set;
   g.funcs.clear();
   int f = 0;
@@ -51,8 +70,7 @@ void assign_functions(const System& sys, const Options& opt, const std::vector<d
             d_end = sys.s_funcs + sys.p_funcs * 3 + sys.d_funcs * 6;
   for (; f < s_end; f++) {
     int atom = sys.nuc[f];
-    if (opt.assign_all_functions ||
-        is_significative(1, min_exps[f], dists[atom], opt.max_function_exponent)) {
+    if (opt.assign_all_functions || min_exps[f] * dists[atom] < sc.bound[f]) {
       g.funcs.push_back(f);
       g.s++;
       nuc_set.insert(atom);
@@ -60,8 +78,7 @@ void assign_functions(const System& sys, const Options& opt, const std::vector<d
   }
   for (; f < p_end; f += 3) {
     int atom = sys.nuc[f];
-    if (opt.assign_all_functions ||
-        is_significative(3, min_exps[f], dists[atom], opt.max_function_exponent)) {
+    if (opt.assign_all_functions || std::sqrt(dists[atom]) < sc.bound[f]) {
       g.funcs.push_back(f);
       g.p++;
       nuc_set.insert(atom);
@@ -69,8 +86,7 @@ void assign_functions(const System& sys, const Options& opt, const std::vector<d
   }
   for (; f < d_end; f += 6) {
     int atom = sys.nuc[f];
-    if (opt.assign_all_functions ||
-        is_significative(6, min_exps[f], dists[atom], opt.max_function_exponent)) {
+    if (opt.assign_all_functions || std::sqrt(dists[atom]) < sc.bound[f]) {
       g.funcs.push_back(f);
       g.d++;
       nuc_set.insert(atom);
@@ -212,15 +228,27 @@ void build_partition(const System& sys, const Options& opt, const AngularGrid& a
     }
   }
 
-  // points: Gauss-Chebyshev radial (Becke mapping) x angular (:274-322)
+  // points: Gauss-Chebyshev radial (Becke mapping) x angular (:274-322). Each
+  // atom's points are generated in parallel (in the reference's shell, point
+  // order) with their destination (a cube, or the atom's sphere, -1); the cubes
+  // are then filled by threads that each own a range of cubes and scan the atoms
+  // in order, so every cube holds its points in the serial loop's order.
   const size_t ncubes_all = (size_t)psize[0] * psize[1] * psize[2];
   std::vector<std::vector<GridPoint>> prism(ncubes_all);
   std::vector<std::vector<GridPoint>> sph(opt.sphere_radius > 0 ? natoms : 0);
+  std::vector<std::vector<GridPoint>> apts(natoms);
+  std::vector<std::vector<long long>> adst(natoms);
+  bool outside = false;
+#pragma omp parallel for schedule(dynamic, 1) reduction(|| : outside)
   for (int atom = 0; atom < natoms; atom++) {
     const unsigned ns = shells[atom];
     const double t0 = M_PI / (ns + 1);
     const double rm = sys.rm[atom];
     const unsigned inc = (unsigned)std::ceil(opt.sphere_radius * ns);
+    std::vector<GridPoint>& P = apts[atom];
+    std::vector<long long>& D = adst[atom];
+    P.reserve((size_t)ns * ang.size());
+    D.reserve((size_t)ns * ang.size());
     for (unsigned shell = 0; shell < ns; shell++) {
       const double t1 = t0 * (shell + 1);
       const double x = std::cos(t1);
@@ -234,21 +262,39 @@ void build_partition(const System& sys, const Options& opt, const AngularGrid& a
         const bool inside = (x0[0] <= px && px <= x1[0]) && (x0[1] <= py && py <= x1[1]) &&
                             (x0[2] <= pz && pz <= x1[2]);
         if (!inside) continue;
-        GridPoint gp{atom, (int)shell, p, px, py, pz, wrad * ang.w[p]};
+        P.push_back(GridPoint{atom, (int)shell, p, px, py, pz, wrad * ang.w[p]});
         if (shell >= (ns - inc)) {
-          sph[atom].push_back(gp);
+          D.push_back(-1);
         } else {
           const unsigned cx = (unsigned)std::floor((px - x0[0]) / lcs);
           const unsigned cy = (unsigned)std::floor((py - x0[1]) / lcs);
           const unsigned cz = (unsigned)std::floor((pz - x0[2]) / lcs);
-          if (cx >= psize[0] || cy >= psize[1] || cz >= psize[2])
-            throw std::runtime_error("grid point outside the cube prism");
-          prism[((size_t)cx * psize[1] + cy) * psize[2] + cz].push_back(gp);
+          if (cx >= psize[0] || cy >= psize[1] || cz >= psize[2]) outside = true;
+          D.push_back((long long)(((size_t)cx * psize[1] + cy) * psize[2] + cz));
         }
       }
     }
   }
-  out.mincost = env_int("LIO_MINCOST_OFFSET", 250000);
+  if (outside) throw std::runtime_error("grid point outside the cube prism");
+#pragma omp parallel
+  {
+    const int nt = omp_get_num_threads(), t = omp_get_thread_num();
+    const long long c0 = (long long)(ncubes_all * t / nt), c1 = (long long)(ncubes_all * (t + 1) / nt);
+    for (int atom = 0; atom < natoms; atom++) {
+      const std::vector<GridPoint>& P = apts[atom];
+      const std::vector<long long>& D = adst[atom];
+      for (size_t q = 0; q < P.size(); q++)
+        if (D[q] >= c0 && D[q] < c1) prism[(size_t)D[q]].push_back(P[q]);
+    }
+#pragma omp for schedule(dynamic, 8)
+    for (int atom = 0; atom < (int)sph.size(); atom++)
+      for (size_t q = 0; q < apts[atom].size(); q++)
+        if (adst[atom][q] < 0) sph[atom].push_back(apts[atom][q]);
+  }
+  apts.clear();
+  adst.clear();
+
+  const Screen screen = make_screen(sys, opt, min_exps_func);
 
   // cubes (:331-399): screening against the cube box, then weights
   std::vector<PointGroup> cand_cubes, cand_spheres;
@@ -257,6 +303,8 @@ void build_partition(const System& sys, const Options& opt, const AngularGrid& a
     for (unsigned j = 0; j < psize[1]; j++)
       for (unsigned k = 0; k < psize[2]; k++) {
         std::vector<GridPoint>& pts = prism[((size_t)i * psize[1] + j) * psize[2] + k];
+        // an empty cube never becomes a group (it has fewer than min_points_per_cube >= 1 points)
+        if (pts.empty() && opt.min_points_per_cube > 0) continue;
         const double cc[3] = {x0[0] + i * lcs, x0[1] + j * lcs, x0[2] + k * lcs};
         for (int a = 0; a < natoms; a++) {
           const double pos[3] = {sys.ax[a], sys.ay[a], sys.az[a]};
@@ -273,7 +321,7 @@ void build_partition(const System& sys, const Options& opt, const AngularGrid& a
         }
         PointGroup g;
         g.sphere = false;
-        assign_functions(sys, opt, dists, min_exps_func, g);
+        assign_functions(sys, opt, dists, min_exps_func, screen, g);
         if (g.funcs.empty() || pts.size() < opt.min_points_per_cube) continue;
         g.points.swap(pts);
         cand_cubes.push_back(std::move(g));
@@ -293,7 +341,7 @@ void build_partition(const System& sys, const Options& opt, const AngularGrid& a
       }
       PointGroup g;
       g.sphere = true;
-      assign_functions(sys, opt, dists, min_exps_func, g);
+      assign_functions(sys, opt, dists, min_exps_func, screen, g);
       if (sph[a].size() < opt.min_points_per_cube) continue;
       g.points.swap(sph[a]);
       cand_spheres.push_back(std::move(g));
@@ -306,10 +354,11 @@ void build_partition(const System& sys, const Options& opt, const AngularGrid& a
   for (PointGroup& g : cand_cubes) all.push_back(&g);
   for (PointGroup& g : cand_spheres) all.push_back(&g);
   (weights ? weights : host_becke_weights)(sys, all);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (long long gi = 0; gi < (long long)all.size(); gi++) remove_zero_weights(opt, *all[gi]);
   for (int pass = 0; pass < 2; pass++) {
     std::vector<PointGroup>& cand = pass == 0 ? cand_cubes : cand_spheres;
     for (PointGroup& g : cand) {
-      remove_zero_weights(opt, g);
       if (g.points.size() < opt.min_points_per_cube) continue;
       (pass == 0 ? out.cubes : out.spheres).push_back(std::move(g));
     }
