@@ -78,13 +78,21 @@ struct GroupDev {
 // device bytes held by every DevBuf of the process (footprint accounting)
 std::atomic<long long> g_devbuf_bytes{0};
 
+// Device array with process-wide byte accounting. alloc() keeps the existing
+// allocation when it is large enough (a new geometry of similar size reuses it:
+// no cudaFree / cudaMalloc, which synchronise the device, per grid build).
 template <class T>
 struct DevBuf {
   T* p = nullptr;
-  size_t n = 0;
+  size_t n = 0;    // elements in use
+  size_t cap = 0;  // elements allocated
   void alloc(size_t count) {
-    free();
     if (count == 0) count = 1;
+    if (p && count <= cap) {
+      n = count;
+      return;
+    }
+    free();
     const cudaError_t e = cudaMalloc(&p, count * sizeof(T));
     if (e != cudaSuccess) {  // clear the thread's last error: later launch checks must not see it
       cudaGetLastError();
@@ -92,8 +100,8 @@ struct DevBuf {
       throw std::runtime_error(std::string("CUDA error ") + cudaGetErrorString(e) + " allocating " +
                                std::to_string(count * sizeof(T)) + " bytes");
     }
-    n = count;
-    g_devbuf_bytes += (long long)(n * sizeof(T));
+    n = cap = count;
+    g_devbuf_bytes += (long long)(cap * sizeof(T));
   }
   void upload(const std::vector<T>& v) {
     alloc(v.size());
@@ -102,10 +110,10 @@ struct DevBuf {
   void free() {
     if (p) {
       cudaFree(p);
-      g_devbuf_bytes -= (long long)(n * sizeof(T));
+      g_devbuf_bytes -= (long long)(cap * sizeof(T));
     }
     p = nullptr;
-    n = 0;
+    n = cap = 0;
   }
   ~DevBuf() { free(); }
 };
@@ -753,6 +761,7 @@ struct DeviceEngine::Impl {
   DevBuf<double> P_a, P_b, K_a, K_b, part_a, part_b, fac_a, fac_b, eblocks, energy;
   double* hK = nullptr;  // pinned: Kohn-Sham result of the last solve (nspin x npacked)
   double* hP = nullptr;  // pinned: staging of the caller's densities (nspin x npacked)
+  size_t pinned_elems = 0;
   double* hE = nullptr;  // pinned: its energy
   int* hErr = nullptr;   // pinned: the tensor-core error flag
   bool enqueued = false;
@@ -792,6 +801,7 @@ struct DeviceEngine::Impl {
     if (hK) cudaFreeHost(hK);
     if (hP) cudaFreeHost(hP);
     hP = nullptr;
+    pinned_elems = 0;
     if (hE) cudaFreeHost(hE);
     if (hErr) cudaFreeHost(hErr);
     hK = hE = nullptr;
@@ -879,13 +889,20 @@ void DeviceEngine::release() {
 long long DeviceEngine::points() const { return impl_->npoints; }
 
 void DeviceEngine::becke_weights(const System& sys, const std::vector<PointGroup*>& groups) {
-  long long n = 0;
-  for (const PointGroup* g : groups) n += (long long)g->points.size();
+  const long long ng = (long long)groups.size();
+  std::vector<long long> first(ng + 1, 0);  // first point of each group in the flat arrays
+  for (long long gi = 0; gi < ng; gi++) first[gi + 1] = first[gi] + (long long)groups[gi]->points.size();
+  const long long n = first[ng];
   if (n == 0) return;
   std::vector<double> hx((size_t)n), hy((size_t)n), hz((size_t)n);
   std::vector<int> hatom((size_t)n), hgroup((size_t)n), hoff(groups.size() + 1, 0), hnucs;
-  long long k = 0;
   for (size_t gi = 0; gi < groups.size(); gi++) {
+    hnucs.insert(hnucs.end(), groups[gi]->nucs.begin(), groups[gi]->nucs.end());
+    hoff[gi + 1] = (int)hnucs.size();
+  }
+#pragma omp parallel for schedule(dynamic, 4)
+  for (long long gi = 0; gi < ng; gi++) {
+    long long k = first[gi];
     for (const GridPoint& p : groups[gi]->points) {
       hx[k] = p.x;
       hy[k] = p.y;
@@ -894,8 +911,6 @@ void DeviceEngine::becke_weights(const System& sys, const std::vector<PointGroup
       hgroup[k] = (int)gi;
       k++;
     }
-    hnucs.insert(hnucs.end(), groups[gi]->nucs.begin(), groups[gi]->nucs.end());
-    hoff[gi + 1] = (int)hnucs.size();
   }
   DevBuf<double> dx, dy, dz, dax, day, daz, drm, dist, fac;
   DevBuf<int> datom, dgroup, doff, dnucs;
@@ -917,10 +932,13 @@ void DeviceEngine::becke_weights(const System& sys, const std::vector<PointGroup
   LIO_CUDA(cudaGetLastError());
   std::vector<double> hf((size_t)n);
   LIO_CUDA(cudaMemcpy(hf.data(), fac.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
-  k = 0;
-  for (PointGroup* g : groups)
-    for (GridPoint& p : g->points) p.w *= hf[(size_t)k++];
+#pragma omp parallel for schedule(dynamic, 4)
+  for (long long gi = 0; gi < ng; gi++) {
+    long long k = first[gi];
+    for (GridPoint& p : groups[gi]->points) p.w *= hf[(size_t)k++];
+  }
 }
+
 double DeviceEngine::last_force_kernel_ms() const { return impl_->last_force_ms; }
 
 void DeviceEngine::set_accumulators(double* d_fock_a, double* d_fock_b, double* d_energy) {
@@ -964,6 +982,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
 
   std::vector<GroupDev> gd;
   std::vector<double> hx, hy, hz, hw;
+  std::vector<int> src_group;  // partition group of each device group
   std::vector<int> hfn, hsf, hst, hfsh, hfat;
   std::vector<int8_t> hfcp;
   std::vector<int2> btiles, ftiles, sbtiles, sdtiles;
@@ -1011,20 +1030,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
     for (int I = 0; I < nI; I++)
       for (int J = 0; J < nJ; J++)
         if (J * kFkCols + kFkCols - 1 >= I * kFkRows) fktiles.push_back({gdev, I, J, 0});
-    for (int p = 0; p < G.ldp; p++) {
-      if (p < G.npts) {
-        const GridPoint& q = pg.points[p];
-        hx.push_back(q.x);
-        hy.push_back(q.y);
-        hz.push_back(q.z);
-        hw.push_back(q.w);
-      } else {  // padded slot: a copy of the first point with zero weight
-        hx.push_back(pg.points[0].x);
-        hy.push_back(pg.points[0].y);
-        hz.push_back(pg.points[0].z);
-        hw.push_back(0.0);
-      }
-    }
+    src_group.push_back(g);  // its points are packed after this loop, all groups at once
     for (size_t i = 0; i < pg.funcs.size(); i++) {
       const int f = pg.funcs[i];
       const int type = f < sys.s_funcs ? 0 : (f < sys.s_funcs + 3 * sys.p_funcs ? 1 : 2);
@@ -1069,6 +1075,25 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
     fbe_off += (long long)nJ * kFkCols;
     npts_total += G.npts;
     gd.push_back(G);
+  }
+  // points of every device group in parallel, SoA at the group's pt_off;
+  // padded slots hold a copy of the first point with zero weight
+  hx.resize(pt_off);
+  hy.resize(pt_off);
+  hz.resize(pt_off);
+  hw.resize(pt_off);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (long long gi = 0; gi < (long long)gd.size(); gi++) {
+    const GroupDev& G = gd[gi];
+    const PointGroup& pg = part.group(src_group[gi]);
+    for (int p = 0; p < G.ldp; p++) {
+      const GridPoint& q = pg.points[p < G.npts ? p : 0];
+      const long long o = G.pt_off + p;
+      hx[o] = q.x;
+      hy[o] = q.y;
+      hz[o] = q.z;
+      hw[o] = p < G.npts ? q.w : 0.0;
+    }
   }
   d->tc_sizes[0] = bb_off;
   d->bblk_elems = bb_off;
@@ -1151,11 +1176,15 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
   d->eblocks.alloc(ftiles.size());
   d->energy.alloc(1);
   d->drop_graph();
-  d->free_pinned();
-  LIO_CUDA(cudaMallocHost(&d->hK, npacked * (sys.open ? 2 : 1) * sizeof(double)));
-  LIO_CUDA(cudaMallocHost(&d->hP, npacked * (sys.open ? 2 : 1) * sizeof(double)));
-  LIO_CUDA(cudaMallocHost(&d->hE, sizeof(double)));
-  LIO_CUDA(cudaMallocHost(&d->hErr, sizeof(int)));
+  const size_t pinned = npacked * (sys.open ? 2 : 1);
+  if (!d->hK || d->pinned_elems != pinned) {  // a new geometry of the same molecule keeps them
+    d->free_pinned();
+    LIO_CUDA(cudaMallocHost(&d->hK, pinned * sizeof(double)));
+    LIO_CUDA(cudaMallocHost(&d->hP, pinned * sizeof(double)));
+    LIO_CUDA(cudaMallocHost(&d->hE, sizeof(double)));
+    LIO_CUDA(cudaMallocHost(&d->hErr, sizeof(int)));
+    d->pinned_elems = pinned;
+  }
   *d->hErr = 0;
 
   // basis values, computed once per geometry and kept resident (the tensor-core
@@ -1390,11 +1419,11 @@ void DeviceEngine::prepare() {
 
 size_t DeviceEngine::cache_bytes() const {
   const Impl* d = impl_.get();
-  size_t b = (d->basis.n + d->bblk.n) * sizeof(double);
+  size_t b = (d->basis.cap + d->bblk.cap) * sizeof(double);
   for (const auto* x : {&d->aslices, &d->dslices_a, &d->dslices_b, &d->fa_slices, &d->fb_slices_a, &d->fb_slices_b})
-    b += x->n;
+    b += x->cap;
   for (const auto* x : {&d->aexp, &d->dexp_a, &d->dexp_b, &d->fa_exp, &d->fb_exp_a, &d->fb_exp_b})
-    b += x->n * sizeof(int16_t);
+    b += x->cap * sizeof(int16_t);
   return b;
 }
 
