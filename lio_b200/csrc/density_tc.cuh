@@ -111,10 +111,25 @@ __global__ void k_slice_basis(const int2* __restrict__ tiles, const GroupDev* __
     const int e = slice_exponent(amax);
     aexp[G.aexp_off + (long long)a * G.ldp + p] = (int16_t)e;
     int8_t* dst = aslices + G.sl_off + (long long)(t.y * NA + a) * nks * kTcStepA;
-    for (int j = 0; j < G.m32; j++) {
-      double x = j < G.m ? ldexp(val(a, j), -e) : 0.0;
-      int8_t* blk = dst + (j >> 5) * kTcStepA + lio::umma::kmajor_offset(r, j & 31, kTcPoints);
-      for (int s = 0; s < kSlices; s++) blk[s * kTcSliceA] = next_digit(x);
+    // 16 consecutive functions at a time: per slice their 16 digits are one
+    // contiguous 16-byte row segment of the K-major block, one store
+    for (int j0 = 0; j0 < G.m32; j0 += 16) {
+      double x[16];
+#pragma unroll
+      for (int k = 0; k < 16; k++) x[k] = j0 + k < G.m ? ldexp(val(a, j0 + k), -e) : 0.0;
+      int8_t* blk = dst + (j0 >> 5) * kTcStepA + lio::umma::kmajor_offset(r, j0 & 31, kTcPoints);
+#pragma unroll
+      for (int s = 0; s < kSlices; s++) {
+        uint32_t w[4];
+#pragma unroll
+        for (int k4 = 0; k4 < 4; k4++) {
+          uint32_t packed = 0;
+#pragma unroll
+          for (int k = 0; k < 4; k++) packed |= ((uint32_t)(uint8_t)next_digit(x[k4 * 4 + k])) << (8 * k);
+          w[k4] = packed;
+        }
+        *reinterpret_cast<uint4*>(blk + s * kTcSliceA) = make_uint4(w[0], w[1], w[2], w[3]);
+      }
     }
   }
 }
