@@ -161,16 +161,34 @@ __global__ void k_slice_density(const int2* __restrict__ tiles, const GroupDev* 
   dexp[G.dexp_off + i] = (int16_t)e;
   const int nks = G.m32 / 32;
   int8_t* dst = dslices + G.ds_off + (long long)t.y * nks * kTcStepD;
-  for (int j = 0; j < G.m32; j++) {
-    double x = 0.0;
-    if (i < G.m && j < G.m) {
-      const int gj = fg[j];
-      double v = P[packed_index(gi, gj, M)];
-      if (gi != gj) v *= 0.5;
-      x = ldexp(v, -e);
+  // 16 consecutive functions j at a time: per slice one 16-byte row segment
+  for (int j0 = 0; j0 < G.m32; j0 += 16) {
+    double x[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+      const int j = j0 + k;
+      x[k] = 0.0;
+      if (i < G.m && j < G.m) {
+        const int gj = fg[j];
+        double v = P[packed_index(gi, gj, M)];
+        if (gi != gj) v *= 0.5;
+        x[k] = ldexp(v, -e);
+      }
     }
-    int8_t* blk = dst + (j >> 5) * kTcStepD;
-    for (int s = 0; s < kSlices; s++) blk[lio::umma::kmajor_offset(s * kTcFuncs + r, j & 31, kTcTall)] = next_digit(x);
+    int8_t* blk = dst + (j0 >> 5) * kTcStepD;
+#pragma unroll
+    for (int s = 0; s < kSlices; s++) {
+      uint32_t w[4];
+#pragma unroll
+      for (int k4 = 0; k4 < 4; k4++) {
+        uint32_t packed = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) packed |= ((uint32_t)(uint8_t)next_digit(x[k4 * 4 + k])) << (8 * k);
+        w[k4] = packed;
+      }
+      *reinterpret_cast<uint4*>(blk + lio::umma::kmajor_offset(s * kTcFuncs + r, j0 & 31, kTcTall)) =
+          make_uint4(w[0], w[1], w[2], w[3]);
+    }
   }
 }
 
