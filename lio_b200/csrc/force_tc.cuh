@@ -116,6 +116,11 @@ __global__ void __launch_bounds__(FtCfg::kThreads, 2)
         const int nks = G.m32 / 32;
         const int8_t* A = aslices + G.sl_off + (long long)t.y * NA * nks * kTcStepA;  // kind F: the first of NA
         const int8_t* D = (t.w == 0 ? dsl_a : dsl_b) + G.ds_off + (long long)t.z * nks * kTcStepD;
+        {  // the unit's gradient chunks (its existing function rows) into L2 for the epilogue's loads
+          const double* gch = bblk + G.bb_off + ((long long)(t.y * G.nftc + t.z) * nkb + 1) * kTcChunk;
+          const uint32_t bytes = (uint32_t)min(kTcFuncs, G.m - t.z * kTcFuncs) * kTcPoints * 8;
+          for (int a = 0; a < 3; a++) lio::umma::bulk_prefetch_l2(gch + (long long)a * kTcChunk, bytes);
+        }
         for (int kk = 0; kk < nks; kk++, cnt++) {
           const int buf = cnt % kFtStages, use = cnt / kFtStages;
           if (use > 0 && (*vfail || !lio::umma::mbar_wait(&empty[buf], (use - 1) & 1))) {

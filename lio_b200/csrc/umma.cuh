@@ -177,6 +177,11 @@ __device__ __forceinline__ void bulk_copy_g2s_hint(void* smem_dst, const void* g
       : "memory");
 }
 
+// L2 prefetch of a contiguous global range (16-byte aligned, size a multiple of 16)
+__device__ __forceinline__ void bulk_prefetch_l2(const void* gmem_src, uint32_t size) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(gmem_src), "r"(size) : "memory");
+}
+
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 }  // namespace umma
