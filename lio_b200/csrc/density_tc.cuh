@@ -5,11 +5,13 @@
 // with D the group's dense density, computed with int8 tensor-core products
 // (tcgen05 kind::i8, exact int32 accumulation in TMEM) on Ozaki-style slices:
 //   A^a_pj = 2^(e_p) * sum_s a_s[p][j] 128^-(s+1),   |a_s| <= 64  (per point p)
-//   D_ji   = 2^(f_i) * sum_t d_t[i][j] 128^-(t+1),   |d_t| <= 64  (per function i)
-// and G_pi = 2^(e_p + f_i - 7(S+1)) * sum_l acc_l[p][i] 128^(S-1-l), where the
+//   D_ji   = 2^(f_T) * sum_t d_t[i][j] 128^-(t+1),   |d_t| <= 64  (per 32-function tile T of i)
+// and G_pi = 2^(e_p + f_T - 7(S+1)) * sum_l acc_l[p][i] 128^(S-1-l), where the
 // level accumulator acc_l holds every slice pair s + t = l (pairs with
 // s + t >= S are dropped). With S = 6 the dropped terms are ~2^-42 of
-// max_j|A_pj| * max_j|D_ji| per term, far inside the 1e-7 / 1e-6 Ha tolerances.
+// max_j|A_pj| * max_(j, i in T)|D_ji| per term, far inside the 1e-7 / 1e-6 Ha
+// absolute tolerances. One exponent per tile lets the epilogue scale a whole
+// row dot once instead of every G_pi.
 //
 // Slice pairs in few, wide MMAs: the S slices of a 32-function D tile are
 // stacked along N ("tall" B operand, row t * 32 + i holds d_t[i]). For A slice s
@@ -135,11 +137,13 @@ __global__ void k_slice_basis(const int2* __restrict__ tiles, const GroupDev* __
 }
 
 // --------------------------------------------------------------- D slices
-// Per solve and spin: one thread per (group, function i) of a 32-function tile;
-// gathers column i of the group's density from the packed matrix (off-diagonal
-// packed values halved), writes its exponent and its S slices into the stacked
-// operand: per tile and 32-function K step kk a 192-row x 32-byte block
-// (kTcStepD bytes, one bulk copy) whose row t * 32 + i holds d_t[i].
+// Per solve and spin: one thread per (group, function i) of a 32-function tile
+// (one warp per tile); gathers column i of the group's density from the packed
+// matrix (off-diagonal packed values halved), writes the tile's exponent (one
+// per 32 columns, from the largest |D_ji| of the tile, stored for each of its
+// functions) and its S slices into the stacked operand: per tile and
+// 32-function K step kk a 192-row x 32-byte block (kTcStepD bytes, one bulk
+// copy) whose row t * 32 + i holds d_t[i].
 __global__ void k_slice_density(const int2* __restrict__ tiles, const GroupDev* __restrict__ groups,
                                 const int* __restrict__ fn_glob, const double* __restrict__ P, int M,
                                 int8_t* __restrict__ dslices, int16_t* __restrict__ dexp) {
@@ -157,6 +161,8 @@ __global__ void k_slice_density(const int2* __restrict__ tiles, const GroupDev* 
       if (gi != gj) v *= 0.5;
       amax = fmax(amax, fabs(v));
     }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
   const int e = slice_exponent(amax);
   dexp[G.dexp_off + i] = (int16_t)e;
   const int nks = G.m32 / 32;
@@ -482,7 +488,7 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
     const uint32_t lane_base = tbase + ((uint32_t)(quad * 32) << 16);
     const double* bring = reinterpret_cast<const double*>(tc_smem + Cfg::kBRing);
     double* red = reinterpret_cast<double*>(tc_smem + Cfg::kRed);
-    double* tsa = reinterpret_cast<double*>(tc_smem + Cfg::kTab);  // 2^f_i, spin a
+    double* tsa = reinterpret_cast<double*>(tc_smem + Cfg::kTab);  // 2^f_T per function, spin a
     double* tsb = tsa + fcap;                                        // spin b (NS = 2 only)
     bool lfail = false;
     int ucnt = 0, bcnt = 0;
@@ -510,7 +516,13 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
       for (int tt = 0; tt < ntt; tt++, ucnt++) {
         const int ft = tt / NP, pass = tt - ft * NP, first = pass * KP;
         const int cb = ft * kTcFuncs + colg * CPW;  // first function of this warp's columns
-        // ---- the unit's accumulators -> G (FP64, scaled by 2^(e_p + f_i - 7(S+1))) in registers
+        // ---- the unit's accumulators -> G / 2^(e_p + f_T - 7(S+1)) (FP64) in registers; the
+        // scale is applied to each row dot
+        double sc[NS][KP];
+#pragma unroll
+        for (int sp = 0; sp < NS; sp++)
+#pragma unroll
+          for (int kp = 0; kp < KP; kp++) sc[sp][kp] = spx[first + kp] * (sp == 0 ? tsa : tsb)[ft * kTcFuncs];
         bool ok = !lfail && !*vfail && lio::umma::mbar_wait(&tfull, ucnt & 1);
         ok = __all_sync(0xffffffffu, ok);
         lio::umma::fence_after_sync();
@@ -528,11 +540,8 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
                   lio::umma::tmem_ld8(
                       lane_base + (uint32_t)(((sp * KP + kp) * kSlices + l) * kTcFuncs + colg * CPW + h * 8), lv[l]);
                 lio::umma::tmem_wait_ld();
-                const double sa = spx[first + kp];
 #pragma unroll
-                for (int c = 0; c < 8; c++)
-                  g[h * 8 + c][sp][kp] =
-                      level_sum(lv, c, narrow) * sa * (sp == 0 ? tsa[cb + h * 8 + c] : tsb[cb + h * 8 + c]);
+                for (int c = 0; c < 8; c++) g[h * 8 + c][sp][kp] = level_sum(lv, c, narrow);
               }
         } else {
           lfail = true;
@@ -573,7 +582,8 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
 #pragma unroll
             for (int sp = 0; sp < NS; sp++)
 #pragma unroll
-              for (int kp = 0; kp < KP; kp++) d[sp][kp] = (d4[0][sp][kp] + d4[1][sp][kp]) + (d4[2][sp][kp] + d4[3][sp][kp]);
+              for (int kp = 0; kp < KP; kp++)
+                d[sp][kp] = ((d4[0][sp][kp] + d4[1][sp][kp]) + (d4[2][sp][kp] + d4[3][sp][kp])) * sc[sp][kp];
             apply_chunk<GGA, NS, NQ, KP>(first, k, d, q);
           }
           __syncwarp();

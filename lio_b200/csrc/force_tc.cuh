@@ -191,10 +191,13 @@ __global__ void __launch_bounds__(FtCfg::kThreads, 2)
         break;
       }
       lio::umma::fence_after_sync();
-      // G_i(p) = acc * 2^(e_p + f_i - 7(S+1)); the factor f_p joins the point scale
+      // G_i(p) = acc * 2^(e_p + f_T - 7(S+1)), f_T the exponent of the density
+      // tile (one per 32 functions; columns past m have no slices, acc = 0); the
+      // factor f_p joins the point scale
       const int16_t* dexp = sp == 0 ? dexp_a : dexp_b;
       const double fp = (sp == 0 ? fac_a : fac_b)[G.pt_off + p];
-      const double spx = fp * pow2(aexp[G.aexp_off + p] - 7 * (kSlices + 1));
+      const double spx =
+          fp * pow2(aexp[G.aexp_off + p] - 7 * (kSlices + 1)) * pow2(dexp[G.dexp_off + ft * kTcFuncs]);
       const bool narrow = G.m32 <= kTcNarrowK;
       double g[kTcFuncs];
 #pragma unroll
@@ -204,11 +207,7 @@ __global__ void __launch_bounds__(FtCfg::kThreads, 2)
         for (int l = 0; l < kSlices; l++) lio::umma::tmem_ld8(lane_base + (uint32_t)(l * kTcFuncs + h * 8), lv[l]);
         lio::umma::tmem_wait_ld();
 #pragma unroll
-        for (int c = 0; c < 8; c++) {
-          const int i = ft * kTcFuncs + h * 8 + c;
-          const double ts = i < G.m ? pow2(dexp[G.dexp_off + i]) : 0.0;
-          g[h * 8 + c] = level_sum(lv, c, narrow) * spx * ts;
-        }
+        for (int c = 0; c < 8; c++) g[h * 8 + c] = level_sum(lv, c, narrow) * spx;
       }
       // levels read: the next unit's MMAs may overwrite TMEM
       lio::umma::fence_before_sync();
