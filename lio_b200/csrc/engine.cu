@@ -68,11 +68,10 @@ struct GroupDev {
   long long sl_off;    // int8 slices of the density A operands (bytes)
   long long aexp_off;  // their per-point exponents (elements): NA x ldp
   long long ds_off;    // int8 slices of the density matrix (bytes, one spin)
-  long long dexp_off;  // their per-function exponents (elements): nftc x 32
+  long long dexp_off;  // their exponents (elements): nftc x 32, one value per 32-function tile
   long long fa_off;    // int8 slices of F by function row for the Kohn-Sham contraction (bytes)
   long long fae_off;   // their per-row exponents (elements): nI x 128
-  long long fb_off;    // int8 slices of f*F by row (bytes, one spin)
-  long long fbe_off;   // their per-row exponents (elements): nJ x 32
+  long long fbe_off;   // per-row exponents of f*F (elements): nJ x 32
 };
 
 // device bytes held by every DevBuf of the process (footprint accounting)
@@ -747,9 +746,9 @@ struct DeviceEngine::Impl {
   DevBuf<int> tc_err;
   long long tc_sizes[5] = {0, 0, 0, 0, 0};
   // tensor-core Kohn-Sham contraction
-  DevBuf<int2> fa_rows, fb_rows, fa_tiles32, fb_tiles32;  // rows, and 32-row pieces, of the Fock slice blocks
+  DevBuf<int2> fa_rows, fb_rows, fa_tiles32;  // rows of the Kohn-Sham operands, 32-row pieces of the A slices
   DevBuf<int4> fk_tiles, force_tc_tiles;
-  DevBuf<int8_t> fa_slices, fb_slices_a, fb_slices_b;
+  DevBuf<int8_t> fa_slices;
   DevBuf<int16_t> fa_exp, fb_exp_a, fb_exp_b;
   long long fk_sizes[4] = {0, 0, 0, 0};
   bool tc_ready = false;
@@ -989,8 +988,8 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
   std::vector<int4> dtiles, ktiles, tctiles;
   long long pt_off = 0, fn_off = 0, sf_off = 0, bas_off = 0, part_off = 0;
   long long bb_off = 0, sl_off = 0, aexp_off = 0, ds_off = 0, dexp_off = 0;
-  long long fa_off = 0, fae_off = 0, fb_off = 0, fbe_off = 0;
-  std::vector<int2> farows, fbrows, fat32, fbt32;
+  long long fa_off = 0, fae_off = 0, fbe_off = 0;
+  std::vector<int2> farows, fbrows, fat32;
   std::vector<int4> fktiles, frtiles;
   long long npts_total = 0;
   int maxm = 0;
@@ -1020,13 +1019,11 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
     G.dexp_off = dexp_off;
     G.fa_off = fa_off;
     G.fae_off = fae_off;
-    G.fb_off = fb_off;
     G.fbe_off = fbe_off;
     const int nI = (G.m + kFkRows - 1) / kFkRows, nJ = (G.m + kFkCols - 1) / kFkCols;
     for (int i = 0; i < nI * kFkRows; i++) farows.push_back({gdev, i});
     for (int j = 0; j < nJ * kFkCols; j++) fbrows.push_back({gdev, j});
     for (int i = 0; i < nI * kFkRows; i += 32) fat32.push_back({gdev, i});
-    for (int j = 0; j < nJ * kFkCols; j += 32) fbt32.push_back({gdev, j});
     for (int I = 0; I < nI; I++)
       for (int J = 0; J < nJ; J++)
         if (J * kFkCols + kFkCols - 1 >= I * kFkRows) fktiles.push_back({gdev, I, J, 0});
@@ -1071,7 +1068,6 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
     dexp_off += (long long)G.nftc * kTcFuncs;
     fa_off += (long long)nI * kSlices * kFkRows * G.ldp;
     fae_off += (long long)nI * kFkRows;
-    fb_off += (long long)nJ * kSlices * kFkCols * G.ldp;
     fbe_off += (long long)nJ * kFkCols;
     npts_total += G.npts;
     gd.push_back(G);
@@ -1104,12 +1100,10 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
   d->tc_ready = false;
   d->fk_sizes[0] = fa_off;
   d->fk_sizes[1] = fae_off;
-  d->fk_sizes[2] = fb_off;
   d->fk_sizes[3] = fbe_off;
   d->fa_rows.upload(farows);
   d->fb_rows.upload(fbrows);
   d->fa_tiles32.upload(fat32);
-  d->fb_tiles32.upload(fbt32);
   d->fk_tiles.upload(fktiles);
   d->force_tc_tiles.upload(frtiles);
   d->hgroups = gd;
@@ -1227,10 +1221,8 @@ void DeviceEngine::prepare_tensor_core() {
   LIO_CUDA(cudaGetLastError());
   d->fa_slices.alloc(d->fk_sizes[0]);
   d->fa_exp.alloc(d->fk_sizes[1]);
-  d->fb_slices_a.alloc(d->fk_sizes[2]);
   d->fb_exp_a.alloc(d->fk_sizes[3]);
   if (d->open) {
-    d->fb_slices_b.alloc(d->fk_sizes[2]);
     d->fb_exp_b.alloc(d->fk_sizes[3]);
   }
   {
@@ -1238,9 +1230,8 @@ void DeviceEngine::prepare_tensor_core() {
     k_fock_rowexp<1><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(d->fa_rows.p, nrows, d->groups.p, d->bblk.p,
                                                                   nullptr, nullptr, d->fa_exp.p, nullptr, 0, d->nk);
     LIO_CUDA(cudaGetLastError());
-    k_fock_slices<kFkRows, false, 1><<<(unsigned)d->fa_tiles32.n, 256, 0, st>>>(
-        d->fa_tiles32.p, d->groups.p, d->bblk.p, nullptr, nullptr, d->fa_exp.p, nullptr, d->fa_slices.p, nullptr, 0,
-        d->nk);
+    k_fock_aslices<<<(unsigned)d->fa_tiles32.n, 256, 0, st>>>(d->fa_tiles32.p, d->groups.p, d->bblk.p,
+                                                                d->fa_exp.p, d->fa_slices.p, d->nk);
     LIO_CUDA(cudaGetLastError());
   }
   LIO_CUDA(cudaFuncSetAttribute(k_fock_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FkCfg<1>::kSmem));
@@ -1342,36 +1333,28 @@ int DeviceEngine::run_kernels(bool compute_rmm, bool ext) {
       if (d->open) LIO_CUDA(cudaMemsetAsync(d->K_b.p, 0, npacked * sizeof(double), st));
     }
     if (tc) {
-      // f * F slices of both spins: row exponents, then the slices (one pass over F each)
+      // row exponents of f * F (both spins, one pass over F); the contraction
+      // kernel cuts the f * F slices itself
       const int nrows = (int)d->fb_rows.n;
-      if (d->open) {
+      if (d->open)
         k_fock_rowexp<2><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(d->fb_rows.p, nrows, d->groups.p, d->bblk.p,
                                                                       d->fac_a.p, d->fac_b.p, d->fb_exp_a.p,
                                                                       d->fb_exp_b.p, 1, d->nk);
-        LIO_CUDA(cudaGetLastError());
-        k_fock_slices<kFkCols, true, 2><<<(unsigned)d->fb_tiles32.n, 256, 0, st>>>(
-            d->fb_tiles32.p, d->groups.p, d->bblk.p, d->fac_a.p, d->fac_b.p, d->fb_exp_a.p, d->fb_exp_b.p,
-            d->fb_slices_a.p, d->fb_slices_b.p, 1, d->nk);
-      } else {
+      else
         k_fock_rowexp<1><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(d->fb_rows.p, nrows, d->groups.p, d->bblk.p,
                                                                       d->fac_a.p, nullptr, d->fb_exp_a.p, nullptr, 1,
                                                                       d->nk);
-        LIO_CUDA(cudaGetLastError());
-        k_fock_slices<kFkCols, true, 1><<<(unsigned)d->fb_tiles32.n, 256, 0, st>>>(
-            d->fb_tiles32.p, d->groups.p, d->bblk.p, d->fac_a.p, nullptr, d->fb_exp_a.p, nullptr, d->fb_slices_a.p,
-            nullptr, 1, d->nk);
-      }
       LIO_CUDA(cudaGetLastError());
-      launches += 2;
+      launches++;
       d->mark(4);
       if (d->open)
         k_fock_tc<2><<<(unsigned)d->fk_tiles.n, FkCfg<2>::kThreads, FkCfg<2>::kSmem, st>>>(
-            d->fk_tiles.p, d->groups.p, d->fn_glob.p, d->fa_slices.p, d->fa_exp.p, d->fb_slices_a.p, d->fb_exp_a.p,
-            d->fb_slices_b.p, d->fb_exp_b.p, d->M, Ka, Kb, d->tc_err.p);
+            d->fk_tiles.p, d->groups.p, d->fn_glob.p, d->fa_slices.p, d->fa_exp.p, d->bblk.p, d->nk, d->fac_a.p,
+            d->fac_b.p, d->fb_exp_a.p, d->fb_exp_b.p, d->M, Ka, Kb, d->tc_err.p);
       else
         k_fock_tc<1><<<(unsigned)d->fk_tiles.n, FkCfg<1>::kThreads, FkCfg<1>::kSmem, st>>>(
-            d->fk_tiles.p, d->groups.p, d->fn_glob.p, d->fa_slices.p, d->fa_exp.p, d->fb_slices_a.p, d->fb_exp_a.p,
-            nullptr, nullptr, d->M, Ka, nullptr, d->tc_err.p);
+            d->fk_tiles.p, d->groups.p, d->fn_glob.p, d->fa_slices.p, d->fa_exp.p, d->bblk.p, d->nk, d->fac_a.p,
+            nullptr, d->fb_exp_a.p, nullptr, d->M, Ka, nullptr, d->tc_err.p);
     } else if (d->open) {
       d->mark(4);  // no operand preparation in the FP64 form
       k_fock_fp64<2><<<nk, 256, 0, st>>>(d->fock_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, d->fac_a.p,
@@ -1420,7 +1403,7 @@ void DeviceEngine::prepare() {
 size_t DeviceEngine::cache_bytes() const {
   const Impl* d = impl_.get();
   size_t b = (d->basis.cap + d->bblk.cap) * sizeof(double);
-  for (const auto* x : {&d->aslices, &d->dslices_a, &d->dslices_b, &d->fa_slices, &d->fb_slices_a, &d->fb_slices_b})
+  for (const auto* x : {&d->aslices, &d->dslices_a, &d->dslices_b, &d->fa_slices})
     b += x->cap;
   for (const auto* x : {&d->aexp, &d->dexp_a, &d->dexp_b, &d->fa_exp, &d->fb_exp_a, &d->fb_exp_b})
     b += x->cap * sizeof(int16_t);
@@ -1439,7 +1422,7 @@ long long DeviceEngine::process_device_bytes() { return g_devbuf_bytes.load(); }
 
 void DeviceEngine::drop_tensor_core() {
   Impl* d = impl_.get();
-  for (auto* b : {&d->aslices, &d->dslices_a, &d->dslices_b, &d->fa_slices, &d->fb_slices_a, &d->fb_slices_b})
+  for (auto* b : {&d->aslices, &d->dslices_a, &d->dslices_b, &d->fa_slices})
     b->free();
   for (auto* b : {&d->aexp, &d->dexp_a, &d->dexp_b, &d->fa_exp, &d->fb_exp_a, &d->fb_exp_b}) b->free();
   d->bblk.free();
@@ -1526,12 +1509,12 @@ size_t DeviceEngine::estimate_device_bytes(const System& sys, const Partition& p
     const double ldp = (double)(((long long)pg.points.size() + kPointPad - 1) / kPointPad * kPointPad);
     const int m = pg.total_functions(), m32 = (m + 31) / 32 * 32;
     const int nft = (m + kTile - 1) / kTile, nftc = (m + kTcFuncs - 1) / kTcFuncs;
-    const int nI = (m + kFkRows - 1) / kFkRows, nJ = (m + kFkCols - 1) / kFkCols;
+    const int nI = (m + kFkRows - 1) / kFkRows;
     b += ldp * (6 * 8 + nspin * (nq * (double)nft * 8 + 8));  // points, partials, factors
     if (prec == Precision::FP64) b += ldp * nk * (double)m * 8;  // function-major basis cache
     if (prec == Precision::TensorCore)
       b += ldp * ((double)nftc * kTcFuncs * nk * 8 + (double)na * m32 * kSlices + na * 2 +
-                  (double)nI * kFkRows * kSlices + (double)nspin * nJ * kFkCols * kSlices) +
+                  (double)nI * kFkRows * kSlices) +
            (double)nspin * nftc * m32 * kTcTall;
   }
   return (size_t)(b * 1.05) + (16u << 20);

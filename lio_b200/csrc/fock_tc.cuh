@@ -9,7 +9,9 @@
 // contraction. A tile is 128 functions (i) x 32 functions (j); the S slices
 // of a B tile are stacked along N (row t * 32 + j holds b_t[j]), so one MMA per
 // A slice s (N = (S - s) * 32) lands every product (s, t) on level s + t.
-// Both spins share the A slices and keep 2 x S level blocks in TMEM.
+// Both spins share the A slices and keep 2 x S level blocks in TMEM. The A
+// slices are built once per geometry; the B slices are cut inside the
+// contraction kernel, a K step at a time, so they never go through HBM.
 #pragma once
 
 constexpr int kFkRows = 128;  // UMMA M: functions i per tile
@@ -23,14 +25,28 @@ template <int NS>
 struct FkCfg {
   static constexpr int kStageA = kFkStepA;
   static constexpr int kStage = kStageA + NS * kFkStepB;
-  static constexpr size_t kSmem = (size_t)kFkStages * kStage;
+  // ring slot: the 32 F rows of a 128-point tile, each padded to 1040 bytes so
+  // that 32 lanes reading 16 bytes of 32 different rows hit distinct banks,
+  // then each spin's 128 factors
+  static constexpr int kRowBytes = kTcPoints * 8 + 16;
+  static constexpr int kSlot = kFkCols * kRowBytes + NS * kTcPoints * 8;
+  static constexpr size_t kSmem = (size_t)kFkStages * kStage + 2 * (size_t)kSlot;
   static constexpr uint32_t kCols = NS * kSlices * kFkCols;
   static constexpr uint32_t kTmem = kCols <= 256 ? 256 : 512;
-  static constexpr int kThreads = 32 * 6;  // 4 epilogue warps, producer, MMA issuer
+  // B slicers (4 per spin; the first four are also the epilogue), producer, MMA issuer
+  static constexpr int kSlicers = 4 * NS;
+  static constexpr int kProd = kSlicers, kMma = kSlicers + 1;
+  static constexpr int kThreads = 32 * (kSlicers + 2);
 };
+static_assert(FkCfg<2>::kSmem <= 227 * 1024, "shared memory of the Kohn-Sham kernel");
+static_assert(FkCfg<1>::kSlot % 128 == 0 && FkCfg<2>::kSlot % 128 == 0 && FkCfg<2>::kStage % 128 == 0,
+              "ring slots and stages stay 128-byte aligned");
 
 // Slices of the rows of v = F (A operand, per geometry) or v = f_s F (B
-// operand, per solve, both spins at once), in two passes over the FP64 basis.
+// operand, per solve, both spins at once), in two passes over the FP64 basis:
+// pass 1 (row exponents) runs for both operands; pass 2 writes the A slices to
+// HBM, while the B slices are cut by the Kohn-Sham kernel itself (in the TALL
+// layout below, in shared memory).
 //
 // F(i, p) of a group and the values after it up to the end of its 128-point
 // tile: from the function-major basis cache (nkb = 0) or from the blocked copy
@@ -89,93 +105,97 @@ __global__ void k_fock_rowexp(const int2* __restrict__ rows, int nrows, const Gr
   }
 }
 
-// Pass 2, a CTA per 32-row piece of a row tile (lane = row), each warp taking
-// 16-point blocks: per spin and slice one 16-byte store. Layout per row tile
-// (R rows) and 32-point K step: A (TALL = false): the S slices one after the
-// other, each an R-row x 32-byte K-major block; B (TALL = true): one
-// (S * R)-row x 32-byte block whose row t * R + r holds slice t of row r.
-template <int R, bool TALL, int NS>
-__global__ void __launch_bounds__(256) k_fock_slices(const int2* __restrict__ rtiles, const GroupDev* __restrict__ groups,
-                                                     const double* __restrict__ basis,
-                                                     const double* __restrict__ fac_a,
-                                                     const double* __restrict__ fac_b,
-                                                     const int16_t* __restrict__ expo_a,
-                                                     const int16_t* __restrict__ expo_b, int8_t* __restrict__ sl_a,
-                                                     int8_t* __restrict__ sl_b, int use_sl_b, int nkb) {
-  constexpr int kStep = kSlices * 32 * R;  // bytes of one K step of a row tile (either layout)
+// Pass 2 for the A operand (per geometry): a CTA per 32-row piece of a
+// 128-row tile (lane = row), each warp taking 16-point blocks, one 16-byte store
+// per slice. Layout per row tile and 32-point K step: the S slices one after
+// the other, each a 128-row x 32-byte K-major block (kFkStepA bytes, one bulk
+// copy). The B operand's layout, per 32-row tile and K step one
+// (S * 32)-row x 32-byte block whose row t * 32 + r holds slice t of row r, is
+// written by the Kohn-Sham kernel's slicers in shared memory.
+__global__ void __launch_bounds__(256) k_fock_aslices(const int2* __restrict__ rtiles,
+                                                      const GroupDev* __restrict__ groups,
+                                                      const double* __restrict__ basis,
+                                                      const int16_t* __restrict__ expo, int8_t* __restrict__ sl,
+                                                      int nkb) {
   const int2 t = rtiles[blockIdx.x];
   const GroupDev& G = groups[t.x];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i = t.y + lane, ldp = G.ldp, nkp = ldp / 32;
   const bool valid = i < G.m;
-  const long long base = use_sl_b ? G.fb_off : G.fa_off;
-  const long long ebase = use_sl_b ? G.fbe_off : G.fae_off;
-  double sc[NS];
-#pragma unroll
-  for (int sp = 0; sp < NS; sp++) sc[sp] = pow2(-(int)(sp == 0 ? expo_a : expo_b)[ebase + i]);
-  const int tile = i / R, r = i % R;
+  const double sc = pow2(-(int)expo[G.fae_off + i]);
+  const int tile = i / kFkRows, r = i % kFkRows;
   for (int b = warp; b < ldp / 16; b += blockDim.x / 32) {
     const int p0 = b * 16;
     const double* Fi = f_row(G, basis, valid ? i : 0, p0, nkb);  // 16 values within one 128-point tile
-    double F[16];
+    double x[16];
 #pragma unroll
     for (int k = 0; k < 16; k += 2) {
       const double2 v = valid ? *reinterpret_cast<const double2*>(Fi + k) : make_double2(0.0, 0.0);
-      F[k] = v.x;
-      F[k + 1] = v.y;
+      x[k] = v.x * sc;
+      x[k + 1] = v.y * sc;
     }
+    int8_t* blk = sl + G.fa_off + ((long long)tile * nkp + (p0 >> 5)) * kFkStepA;
 #pragma unroll
-    for (int sp = 0; sp < NS; sp++) {
-      const double* fac = sp == 0 ? fac_a : fac_b;
-      int8_t* blk = (sp == 0 ? sl_a : sl_b) + base + ((long long)tile * nkp + (p0 >> 5)) * kStep;
-      double x[16];
+    for (int s = 0; s < kSlices; s++) {
+      uint32_t w[4];
 #pragma unroll
-      for (int k = 0; k < 16; k++) x[k] = (fac ? F[k] * fac[G.pt_off + p0 + k] : F[k]) * sc[sp];
+      for (int k4 = 0; k4 < 4; k4++) {
+        uint32_t packed = 0;
 #pragma unroll
-      for (int s = 0; s < kSlices; s++) {
-        uint32_t w[4];
-#pragma unroll
-        for (int k4 = 0; k4 < 4; k4++) {
-          uint32_t packed = 0;
-#pragma unroll
-          for (int k = 0; k < 4; k++) packed |= ((uint32_t)(uint8_t)next_digit(x[k4 * 4 + k])) << (8 * k);
-          w[k4] = packed;
-        }
-        const uint32_t off = TALL ? lio::umma::kmajor_offset(s * R + r, p0 & 31, kSlices * R)
-                                  : s * 32 * R + lio::umma::kmajor_offset(r, p0 & 31, R);
-        *reinterpret_cast<uint4*>(blk + off) = make_uint4(w[0], w[1], w[2], w[3]);
+        for (int k = 0; k < 4; k++) packed |= ((uint32_t)(uint8_t)next_digit(x[k4 * 4 + k])) << (8 * k);
+        w[k4] = packed;
       }
+      *reinterpret_cast<uint4*>(blk + s * kFkSliceA + lio::umma::kmajor_offset(r, p0 & 31, kFkRows)) =
+          make_uint4(w[0], w[1], w[2], w[3]);
     }
   }
 }
 
 // CTA = (group, 128-row tile I, 32-column tile J) with some j >= some i.
-// Warps 0-3: epilogue (TMEM lane = row i); warp 4: producer (bulk copies of
-// one 32-point K step per stage, four-stage ring); warp 5: MMA issuer. After
-// the last K step the epilogue combines the levels of each (i, j <= ...) and
-// adds K_ij into the packed accumulator(s) with FP64 atomics.
+// Warp roles:
+//   warps 0 .. 4 NS - 1  B slicers: lane = row j of J, warp = (spin, 8 of the
+//                        K step's 32 points); per stage each cuts its 32 x 8
+//                        values f_p F_jp 2^-b_j into S digits and stores them
+//                        in the stage's stacked B block. Warps 0-3 are also
+//                        the epilogue.
+//   warp 4 NS            producer: per K step the A slices (one bulk copy); per
+//                        128-point tile the F rows of J (kind 0 of the blocked
+//                        basis, one bulk copy per existing row) and each spin's
+//                        factors, into a two-slot ring
+//   warp 4 NS + 1        MMA issuer: per stage NS x S MMAs
+// A stage is ready when its A copy has landed (afull) and every slicer has
+// stored and fenced its part (bready). After the last K step the epilogue
+// combines the levels of each (i, j) with i <= j and adds K_ij into the packed
+// accumulator(s) with FP64 atomics. Every wait is bounded; a timeout sets the
+// error flag, and the producer lets its copies in flight land before exiting.
 template <int NS>
 __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
     k_fock_tc(const int4* __restrict__ tiles, const GroupDev* __restrict__ groups, const int* __restrict__ fn_glob,
-              const int8_t* __restrict__ aslices, const int16_t* __restrict__ aexp,
-              const int8_t* __restrict__ bslices_a, const int16_t* __restrict__ bexp_a,
-              const int8_t* __restrict__ bslices_b, const int16_t* __restrict__ bexp_b, int M,
+              const int8_t* __restrict__ aslices, const int16_t* __restrict__ aexp, const double* __restrict__ bblk,
+              int nkb, const double* __restrict__ fac_a, const double* __restrict__ fac_b,
+              const int16_t* __restrict__ bexp_a, const int16_t* __restrict__ bexp_b, int M,
               double* __restrict__ K_a, double* __restrict__ K_b, int* __restrict__ err) {
   using Cfg = FkCfg<NS>;
   extern __shared__ __align__(128) uint8_t fk_smem[];
-  __shared__ uint64_t full[kFkStages], empty[kFkStages], done;
+  __shared__ uint64_t afull[kFkStages], bready[kFkStages], empty[kFkStages], cfull[2], cempty[2], done;
   __shared__ uint32_t tmem_base;
   __shared__ int fail;
   const int4 t = tiles[blockIdx.x];
   const GroupDev G = groups[t.x];
   const int I = t.y, J = t.z;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int nsteps = G.ldp / 32;
+  const int nsteps = G.ldp / 32;  // a multiple of 4: groups are padded to whole 128-point tiles
+  uint8_t* ring = fk_smem + (size_t)kFkStages * Cfg::kStage;
   if (warp == 0) lio::umma::tmem_alloc(&tmem_base, Cfg::kTmem);
   if (tid == 0) {
     for (int s = 0; s < kFkStages; s++) {
-      lio::umma::mbar_init(&full[s], 1);
+      lio::umma::mbar_init(&afull[s], 1);
+      lio::umma::mbar_init(&bready[s], Cfg::kSlicers);
       lio::umma::mbar_init(&empty[s], 1);
+    }
+    for (int c = 0; c < 2; c++) {
+      lio::umma::mbar_init(&cfull[c], 1);
+      lio::umma::mbar_init(&cempty[c], Cfg::kSlicers);
     }
     lio::umma::mbar_init(&done, 1);
     lio::umma::fence_mbar_init();
@@ -185,32 +205,52 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
   __syncthreads();
   lio::umma::fence_after_sync();
   const uint32_t tbase = tmem_base;
-  if (warp == 4) {
+  volatile int* vfail = &fail;
+  if (warp == Cfg::kProd) {
     if (lane == 0) {
       const int8_t* A = aslices + G.fa_off + (long long)I * nsteps * kFkStepA;
-      const int8_t* Ba = bslices_a + G.fb_off + (long long)J * nsteps * kFkStepB;
-      const int8_t* Bb = NS == 2 ? bslices_b + G.fb_off + (long long)J * nsteps * kFkStepB : nullptr;
-      for (int st = 0; st < nsteps; st++) {
+      const int rows = min(kFkCols, G.m - J * kFkCols);  // rows of J that exist (from row 0 of the chunk)
+      int na = 0, nc = 0;  // A stages and F tiles issued
+      for (int st = 0; st < nsteps && !*vfail; st++) {
+        const int T = st >> 2;
+        if ((st & 3) == 0) {
+          const int c = T & 1;
+          if (T >= 2 && !lio::umma::mbar_wait(&cempty[c], ((T >> 1) - 1) & 1)) {
+            *vfail = 1;
+            break;
+          }
+          uint8_t* slot = ring + c * Cfg::kSlot;
+          const double* F = bblk + G.bb_off + (long long)(T * G.nftc + J) * nkb * kTcChunk;
+          lio::umma::mbar_expect_tx(&cfull[c], (uint32_t)((rows + NS) * kTcPoints * 8));
+          for (int r = 0; r < rows; r++)
+            lio::umma::bulk_copy_g2s(slot + r * Cfg::kRowBytes, F + r * kTcPoints, kTcPoints * 8, &cfull[c]);
+          for (int sp = 0; sp < NS; sp++)
+            lio::umma::bulk_copy_g2s(slot + kFkCols * Cfg::kRowBytes + sp * kTcPoints * 8,
+                                     (sp == 0 ? fac_a : fac_b) + G.pt_off + T * kTcPoints, kTcPoints * 8, &cfull[c]);
+          nc = T + 1;
+        }
         const int buf = st % kFkStages, use = st / kFkStages;
         if (use > 0 && !lio::umma::mbar_wait(&empty[buf], (use - 1) & 1)) {
-          fail = 1;
+          *vfail = 1;
           break;
         }
-        uint8_t* stage = fk_smem + buf * Cfg::kStage;
-        lio::umma::mbar_expect_tx(&full[buf], (uint32_t)Cfg::kStage);
-        lio::umma::bulk_copy_g2s(stage, A + (long long)st * kFkStepA, kFkStepA, &full[buf]);
-        for (int sp = 0; sp < NS; sp++)
-          lio::umma::bulk_copy_g2s(stage + Cfg::kStageA + sp * kFkStepB, (sp == 0 ? Ba : Bb) + (long long)st * kFkStepB,
-                                   kFkStepB, &full[buf]);
+        lio::umma::mbar_expect_tx(&afull[buf], (uint32_t)kFkStepA);
+        lio::umma::bulk_copy_g2s(fk_smem + buf * Cfg::kStage, A + (long long)st * kFkStepA, kFkStepA, &afull[buf]);
+        na = st + 1;
       }
+      // copies in flight land before the CTA exits (each is the latest phase of its barrier)
+      for (int k = max(0, na - kFkStages); k < na; k++)
+        if (!lio::umma::mbar_wait(&afull[k % kFkStages], (k / kFkStages) & 1)) break;
+      for (int T = max(0, nc - 2); T < nc; T++)
+        if (!lio::umma::mbar_wait(&cfull[T & 1], (T >> 1) & 1)) break;
     }
-  } else if (warp == 5) {
+  } else if (warp == Cfg::kMma) {
     if (lane == 0) {
       const uint32_t smem0 = lio::umma::smem_u32(fk_smem);
       for (int st = 0; st < nsteps; st++) {
         const int buf = st % kFkStages, use = st / kFkStages;
-        if (!lio::umma::mbar_wait(&full[buf], use & 1)) {
-          fail = 1;
+        if (*vfail || !lio::umma::mbar_wait(&afull[buf], use & 1) || !lio::umma::mbar_wait(&bready[buf], use & 1)) {
+          *vfail = 1;
           break;
         }
         lio::umma::fence_after_sync();
@@ -230,11 +270,65 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
       lio::umma::commit(&done);
     }
   } else {
+    // ---- B slicers: stage st holds points 32 st .. 32 st + 31 of the group
+    {
+      const int sp = warp >> 2, k0 = (warp & 3) * 8;
+      const int j = J * kFkCols + lane;
+      const bool valid = j < G.m;  // rows past m are zeros (the ring holds stale rows there)
+      const double sc = valid ? pow2(-(int)(sp == 0 ? bexp_a : bexp_b)[G.fbe_off + j]) : 0.0;
+      for (int st = 0; st < nsteps; st++) {
+        const int T = st >> 2, sub = st & 3, c = T & 1;
+        const int buf = st % kFkStages, use = st / kFkStages;
+        bool ok = !*vfail;
+        if (ok && sub == 0) ok = lio::umma::mbar_wait(&cfull[c], (T >> 1) & 1);
+        if (ok && use > 0) ok = lio::umma::mbar_wait(&empty[buf], (use - 1) & 1);
+        if (!__all_sync(0xffffffffu, ok)) {
+          *vfail = 1;
+          break;
+        }
+        const uint8_t* slot = ring + c * Cfg::kSlot;
+        const double* Fr = reinterpret_cast<const double*>(slot + lane * Cfg::kRowBytes) + sub * 32 + k0;
+        const double* fr =
+            reinterpret_cast<const double*>(slot + kFkCols * Cfg::kRowBytes) + sp * kTcPoints + sub * 32 + k0;
+        double x[8];
+#pragma unroll
+        for (int k = 0; k < 8; k += 2) {
+          const double2 v = *reinterpret_cast<const double2*>(Fr + k);
+          const double2 f = *reinterpret_cast<const double2*>(fr + k);
+          x[k] = valid ? v.x * f.x * sc : 0.0;
+          x[k + 1] = valid ? v.y * f.y * sc : 0.0;
+        }
+        uint8_t* bst = fk_smem + buf * Cfg::kStage + Cfg::kStageA + sp * kFkStepB;
+#pragma unroll
+        for (int s = 0; s < kSlices; s++) {
+          uint32_t w[2];
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            uint32_t packed = 0;
+#pragma unroll
+            for (int k = 0; k < 4; k++) packed |= ((uint32_t)(uint8_t)next_digit(x[h * 4 + k])) << (8 * k);
+            w[h] = packed;
+          }
+          *reinterpret_cast<uint2*>(bst + lio::umma::kmajor_offset(s * kFkCols + lane, k0, kFkTall)) =
+              make_uint2(w[0], w[1]);
+        }
+        // generic-proxy stores -> visible to the MMAs (async proxy) once bready completes
+        lio::umma::fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+          lio::umma::mbar_arrive(&bready[buf]);
+          if (sub == 3) lio::umma::mbar_arrive(&cempty[c]);
+        }
+      }
+    }
+  }
+  if (warp < 4) {
+    // ---- epilogue
     const int rrow = warp * 32 + lane;  // TMEM lane
     const int i = I * kFkRows + rrow;
-    const bool ok = lio::umma::mbar_wait(&done, 0);
+    const bool ok = lio::umma::mbar_wait(&done, 0) && !*vfail;
     lio::umma::fence_after_sync();
-    if (!ok) fail = 1;
+    if (!ok) *vfail = 1;
     if (ok) {
       const int gi = i < G.m ? fn_glob[G.fn_off + i] : 0;
       const int ea = i < G.m ? aexp[G.fae_off + i] : 0;
