@@ -88,6 +88,42 @@ __device__ __forceinline__ int8_t next_digit(double& x) {
   return (int8_t)__double2loint(t);
 }
 
+// All S = 6 digits at once, from one rounding on the FP64 adder instead of one
+// per digit: t = 2^52 + B + x 2^42 with B = 64 (128^6 - 1) / 127 (even) rounds
+// x 2^42 (|x| < 1/2) to the nearest integer N, ties to even, and the low
+// mantissa bits of t hold M = N + B >= 0. The base-128 digits m_k of M less 64
+// are balanced digits of N (|m_k - 64| <= 64), so
+//   x = sum_s (m_(5-s) - 64) 128^-(s+1) + r,  |r| <= 2^-43,
+// the same bound as the digit-by-digit form (whose digits may differ from these
+// where a remainder ties). `s42` is 2^42 times the row's power-of-two scale.
+// Returns t's two 32-bit halves (M = bits 0..42).
+__device__ __forceinline__ void digits_m(double x, double s42, uint32_t& lo, uint32_t& hi) {
+  const double t = fma(x, s42, 4505815965769792.0);  // 2^52 + B
+  lo = (uint32_t)__double2loint(t);
+  hi = (uint32_t)__double2hiint(t);
+}
+// m_(5-s), the field of slice s (0 = most significant), in the low byte; for
+// s >= 1 bit 7 of that byte belongs to the next field and is masked by
+// pack_digits. t's exponent bits (from bit 20 of hi) never reach a low byte.
+__device__ __forceinline__ uint32_t digit_field(uint32_t lo, uint32_t hi, int s) {
+  switch (s) {
+    case 0: return hi >> 3;                        // bits 35..42 (m_5 <= 128)
+    case 1: return __funnelshift_r(lo, hi, 28);    // bits 28..34
+    case 2: return lo >> 21;
+    case 3: return lo >> 14;
+    case 4: return lo >> 7;
+    default: return lo;
+  }
+}
+// four fields (low bytes, first point lowest) -> four int8 digits m - 64,
+// byte-wise without carries between bytes; slice 0 keeps its bit 7 (m_5 = 128
+// gives digit 64)
+__device__ __forceinline__ uint32_t pack_digits(uint32_t f0, uint32_t f1, uint32_t f2, uint32_t f3, bool top) {
+  const uint32_t w = __byte_perm(__byte_perm(f0, f1, 0x0040), __byte_perm(f2, f3, 0x0040), 0x5410);
+  const uint32_t low = (w & 0x7F7F7F7Fu) + 0x40404040u;
+  return top ? low ^ ((w ^ 0xC0C0C0C0u) & 0x80808080u) : low ^ 0x80808080u;
+}
+
 // ---------------------------------------------------------------- A slices
 // Per geometry: one thread per (group, point) and kind; reads the blocked FP64
 // basis (NK kinds per block), writes the per-point exponent and the int8

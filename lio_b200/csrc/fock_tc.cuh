@@ -155,7 +155,8 @@ __global__ void __launch_bounds__(256) k_fock_aslices(const int2* __restrict__ r
 // Warp roles:
 //   warps 0 .. 4 NS - 1  B slicers: lane = row j of J, warp = (spin, 8 of the
 //                        K step's 32 points); per stage each cuts its 32 x 8
-//                        values f_p F_jp 2^-b_j into S digits and stores them
+//                        values f_p F_jp 2^-b_j into S digits (digits_m: one
+//                        FP64 rounding, then integer fields) and stores them
 //                        in the stage's stacked B block. Warps 0-3 are also
 //                        the epilogue.
 //   warp 4 NS            producer: per K step the A slices (one bulk copy); per
@@ -275,7 +276,7 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
       const int sp = warp >> 2, k0 = (warp & 3) * 8;
       const int j = J * kFkCols + lane;
       const bool valid = j < G.m;  // rows past m are zeros (the ring holds stale rows there)
-      const double sc = valid ? pow2(-(int)(sp == 0 ? bexp_a : bexp_b)[G.fbe_off + j]) : 0.0;
+      const double s42 = valid ? pow2(42 - (int)(sp == 0 ? bexp_a : bexp_b)[G.fbe_off + j]) : 1.0;
       for (int st = 0; st < nsteps; st++) {
         const int T = st >> 2, sub = st & 3, c = T & 1;
         const int buf = st % kFkStages, use = st / kFkStages;
@@ -290,25 +291,23 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
         const double* Fr = reinterpret_cast<const double*>(slot + lane * Cfg::kRowBytes) + sub * 32 + k0;
         const double* fr =
             reinterpret_cast<const double*>(slot + kFkCols * Cfg::kRowBytes) + sp * kTcPoints + sub * 32 + k0;
-        double x[8];
+        uint32_t lo[8], hi[8];
 #pragma unroll
         for (int k = 0; k < 8; k += 2) {
           const double2 v = *reinterpret_cast<const double2*>(Fr + k);
           const double2 f = *reinterpret_cast<const double2*>(fr + k);
-          x[k] = valid ? v.x * f.x * sc : 0.0;
-          x[k + 1] = valid ? v.y * f.y * sc : 0.0;
+          digits_m(valid ? v.x * f.x : 0.0, s42, lo[k], hi[k]);
+          digits_m(valid ? v.y * f.y : 0.0, s42, lo[k + 1], hi[k + 1]);
         }
         uint8_t* bst = fk_smem + buf * Cfg::kStage + Cfg::kStageA + sp * kFkStepB;
 #pragma unroll
         for (int s = 0; s < kSlices; s++) {
           uint32_t w[2];
 #pragma unroll
-          for (int h = 0; h < 2; h++) {
-            uint32_t packed = 0;
-#pragma unroll
-            for (int k = 0; k < 4; k++) packed |= ((uint32_t)(uint8_t)next_digit(x[h * 4 + k])) << (8 * k);
-            w[h] = packed;
-          }
+          for (int h = 0; h < 2; h++)
+            w[h] = pack_digits(digit_field(lo[4 * h], hi[4 * h], s), digit_field(lo[4 * h + 1], hi[4 * h + 1], s),
+                               digit_field(lo[4 * h + 2], hi[4 * h + 2], s),
+                               digit_field(lo[4 * h + 3], hi[4 * h + 3], s), s == 0);
           *reinterpret_cast<uint2*>(bst + lio::umma::kmajor_offset(s * kFkCols + lane, k0, kFkTall)) =
               make_uint2(w[0], w[1]);
         }
