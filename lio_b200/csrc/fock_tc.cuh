@@ -7,16 +7,20 @@
 //   B_jp = f_p F_jp      = 2^(b_j) sum_t b_t[j][p] 128^-(t+1)  (per solve and spin, per row)
 // with the same int8 slices, level accumulators and level sum as the density
 // contraction. A tile is 128 functions (i) x 32 functions (j); the S slices
-// of a B tile are stacked along N (row t * 32 + j holds b_t[j]), so one MMA per
-// A slice s (N = (S - s) * 32) lands every product (s, t) on level s + t.
-// Both spins share the A slices and keep 2 x S level blocks in TMEM. The A
-// slices are built once per geometry; the B slices are cut inside the
-// contraction kernel, a K step at a time, so they never go through HBM.
+// of a B tile are stacked along N, level-major with the spins interleaved (row
+// (t * NS + spin) * 32 + j holds b_t[j] of that spin), so the MMAs of A slice s
+// over rows [0, (S - s) * NS * 32) (at most 256 per MMA) land every product
+// (s, t) of every spin on level s + t: TMEM column (l * NS + spin) * 32 + j.
+// The spins share each read of the A slices: 8 MMAs per K step for two spins
+// instead of 12, and a third less operand traffic from shared memory, which
+// bounds this kernel. The A slices are built once per geometry; the B slices
+// are cut inside the contraction kernel, a K step at a time, so they never go
+// through HBM.
 #pragma once
 
 constexpr int kFkRows = 128;  // UMMA M: functions i per tile
 constexpr int kFkCols = 32;   // functions j per tile (output columns per level)
-constexpr int kFkTall = kSlices * kFkCols;  // rows of the stacked B operand
+constexpr int kFkTall = kSlices * kFkCols;  // rows of one spin's stacked B operand
 constexpr int kFkStages = 4;
 constexpr int kFkSliceA = 32 * kFkRows;       // bytes of one A slice per 32-point K step
 constexpr int kFkStepA = kSlices * kFkSliceA;  // all A slices of a K step (contiguous)
@@ -25,6 +29,9 @@ template <int NS>
 struct FkCfg {
   static constexpr int kStageA = kFkStepA;
   static constexpr int kStage = kStageA + NS * kFkStepB;
+  static constexpr int kLevelRows = NS * kFkCols;           // B rows (and TMEM columns) per level
+  static constexpr int kTallRows = kSlices * kLevelRows;    // rows of the stacked B operand
+  static constexpr int kMaxLevels = 256 / kLevelRows;       // levels per MMA (N <= 256)
   // ring slot: the 32 F rows of a 128-point tile, each padded to 1040 bytes so
   // that 32 lanes reading 16 bytes of 32 different rows hit distinct banks,
   // then each spin's 128 factors
@@ -256,15 +263,20 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
         }
         lio::umma::fence_after_sync();
         const uint32_t sa = smem0 + buf * Cfg::kStage;
+        // stacked B: K-major, kTallRows rows (LBO = 16 * kTallRows bytes between K halves); the
+        // rows of levels t0 .. start (t0 * kLevelRows / 8) core matrices in. At st = 0 the
+        // MMAs of slice 0 (levels 0 .. S-1, disjoint columns) write every column first.
 #pragma unroll
-        for (int sp = 0; sp < NS; sp++) {
-          // stacked B of this spin: K-major, 192 rows (LBO = 16 * 192 bytes between K halves)
-          const uint64_t bd = lio::umma::smem_desc(sa + Cfg::kStageA + sp * kFkStepB, 16u * kFkTall, 128u);
+        for (int s = 0; s < kSlices; s++) {
+          const uint64_t ad = lio::umma::smem_desc(sa + s * kFkSliceA, 16u * kFkRows, 128u);
 #pragma unroll
-          for (int s = 0; s < kSlices; s++)
-            lio::umma::mma_i8(tbase + (uint32_t)((sp * kSlices + s) * kFkCols),
-                              lio::umma::smem_desc(sa + s * kFkSliceA, 16u * kFkRows, 128u), bd,
-                              lio::umma::idesc_i8(kFkRows, (kSlices - s) * kFkCols), (st > 0 || s > 0) ? 1u : 0u);
+          for (int t0 = 0; t0 < kSlices - s; t0 += Cfg::kMaxLevels) {
+            const int nl = min(Cfg::kMaxLevels, kSlices - s - t0);
+            const uint64_t bd = lio::umma::smem_desc(sa + Cfg::kStageA + (t0 * Cfg::kLevelRows / 8) * 128,
+                                                     16u * Cfg::kTallRows, 128u);
+            lio::umma::mma_i8(tbase + (uint32_t)((s + t0) * Cfg::kLevelRows), ad, bd,
+                              lio::umma::idesc_i8(kFkRows, nl * Cfg::kLevelRows), (st > 0 || s > 0) ? 1u : 0u);
+          }
         }
         lio::umma::commit(&empty[buf]);
       }
@@ -299,7 +311,7 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
           digits_m(valid ? v.x * f.x : 0.0, s42, lo[k], hi[k]);
           digits_m(valid ? v.y * f.y : 0.0, s42, lo[k + 1], hi[k + 1]);
         }
-        uint8_t* bst = fk_smem + buf * Cfg::kStage + Cfg::kStageA + sp * kFkStepB;
+        uint8_t* bst = fk_smem + buf * Cfg::kStage + Cfg::kStageA;
 #pragma unroll
         for (int s = 0; s < kSlices; s++) {
           uint32_t w[2];
@@ -308,7 +320,8 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
             w[h] = pack_digits(digit_field(lo[4 * h], hi[4 * h], s), digit_field(lo[4 * h + 1], hi[4 * h + 1], s),
                                digit_field(lo[4 * h + 2], hi[4 * h + 2], s),
                                digit_field(lo[4 * h + 3], hi[4 * h + 3], s), s == 0);
-          *reinterpret_cast<uint2*>(bst + lio::umma::kmajor_offset(s * kFkCols + lane, k0, kFkTall)) =
+          *reinterpret_cast<uint2*>(
+              bst + lio::umma::kmajor_offset(s * Cfg::kLevelRows + sp * kFkCols + lane, k0, Cfg::kTallRows)) =
               make_uint2(w[0], w[1]);
         }
         // generic-proxy stores -> visible to the MMAs (async proxy) once bready completes
@@ -339,7 +352,7 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
           int32_t lv[kSlices][8];
 #pragma unroll
           for (int l = 0; l < kSlices; l++)
-            lio::umma::tmem_ld8(lane_base + (uint32_t)((sp * kSlices + l) * kFkCols + c0), lv[l]);
+            lio::umma::tmem_ld8(lane_base + (uint32_t)((l * NS + sp) * kFkCols + c0), lv[l]);
           lio::umma::tmem_wait_ld();
 #pragma unroll
           for (int c = 0; c < 8; c++) {
