@@ -102,6 +102,11 @@ __device__ __forceinline__ void digits_m(double x, double s42, uint32_t& lo, uin
   lo = (uint32_t)__double2loint(t);
   hi = (uint32_t)__double2hiint(t);
 }
+// `s42` for a row with exponent e: 2^(42 - e), or 0 (every digit zero) for a
+// row whose values are all below 2^-981, where 2^(42 - e) would leave the
+// double range; the dropped values are far below any tolerance
+__device__ __forceinline__ double digit_scale(int e) { return e > -980 ? pow2(42 - e) : 0.0; }
+
 // m_(5-s), the field of slice s (0 = most significant), in the low byte; for
 // s >= 1 bit 7 of that byte belongs to the next field and is masked by
 // pack_digits. t's exponent bits (from bit 20 of hi) never reach a low byte.

@@ -160,12 +160,11 @@ __global__ void __launch_bounds__(256) k_fock_aslices(const int2* __restrict__ r
 
 // CTA = (group, 128-row tile I, 32-column tile J) with some j >= some i.
 // Warp roles:
-//   warps 0 .. 4 NS - 1  B slicers: lane = row j of J, warp = (spin, 8 of the
-//                        K step's 32 points); per stage each cuts its 32 x 8
-//                        values f_p F_jp 2^-b_j into S digits (digits_m: one
-//                        FP64 rounding, then integer fields) and stores them
-//                        in the stage's stacked B block. Warps 0-3 are also
-//                        the epilogue.
+//   warps 0 .. 4 NS - 1  B slicers: per stage each cuts the values f_p F_jp 2^-b_j
+//                        of 8 rows j and 32 / NS points, every spin, into S
+//                        digits (digits_m: one FP64 rounding, then integer
+//                        fields) and stores them in the stage's stacked B
+//                        block. Warps 0-3 are also the epilogue.
 //   warp 4 NS            producer: per K step the A slices (one bulk copy); per
 //                        128-point tile the F rows of J (kind 0 of the blocked
 //                        basis, one bulk copy per existing row) and each spin's
@@ -285,10 +284,20 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
   } else {
     // ---- B slicers: stage st holds points 32 st .. 32 st + 31 of the group
     {
-      const int sp = warp >> 2, k0 = (warp & 3) * 8;
-      const int j = J * kFkCols + lane;
+      // lane = (row r8 of the warp's 8 rows, point group q): warp w takes rows 8 (w % 4) .. + 7
+      // and PPT points per lane (pb ..), every spin from one read of F. Reads of F (16 bytes
+      // per lane, rows 1040 bytes apart) and the digit stores (8 rows x 16 bytes of one core
+      // matrix per instruction) are free of bank conflicts.
+      constexpr int PPT = 8 / NS;
+      const int r8 = lane & 7, q = lane >> 3;
+      const int row = 8 * (warp & 3) + r8;
+      const int pb = 4 * PPT * (warp >> 2) + PPT * q;  // first point of the lane within a K step
+      const int j = J * kFkCols + row;
       const bool valid = j < G.m;  // rows past m are zeros (the ring holds stale rows there)
-      const double s42 = valid ? pow2(42 - (int)(sp == 0 ? bexp_a : bexp_b)[G.fbe_off + j]) : 1.0;
+      double s42[NS];
+#pragma unroll
+      for (int sp = 0; sp < NS; sp++)
+        s42[sp] = valid ? digit_scale((sp == 0 ? bexp_a : bexp_b)[G.fbe_off + j]) : 1.0;
       for (int st = 0; st < nsteps; st++) {
         const int T = st >> 2, sub = st & 3, c = T & 1;
         const int buf = st % kFkStages, use = st / kFkStages;
@@ -300,30 +309,38 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
           break;
         }
         const uint8_t* slot = ring + c * Cfg::kSlot;
-        const double* Fr = reinterpret_cast<const double*>(slot + lane * Cfg::kRowBytes) + sub * 32 + k0;
-        const double* fr =
-            reinterpret_cast<const double*>(slot + kFkCols * Cfg::kRowBytes) + sp * kTcPoints + sub * 32 + k0;
-        uint32_t lo[8], hi[8];
+        const double* Fr = reinterpret_cast<const double*>(slot + row * Cfg::kRowBytes) + sub * 32 + pb;
+        const double* fr = reinterpret_cast<const double*>(slot + kFkCols * Cfg::kRowBytes) + sub * 32 + pb;
+        uint32_t lo[NS][PPT], hi[NS][PPT];
 #pragma unroll
-        for (int k = 0; k < 8; k += 2) {
+        for (int k = 0; k < PPT; k += 2) {
           const double2 v = *reinterpret_cast<const double2*>(Fr + k);
-          const double2 f = *reinterpret_cast<const double2*>(fr + k);
-          digits_m(valid ? v.x * f.x : 0.0, s42, lo[k], hi[k]);
-          digits_m(valid ? v.y * f.y : 0.0, s42, lo[k + 1], hi[k + 1]);
+#pragma unroll
+          for (int sp = 0; sp < NS; sp++) {
+            const double2 f = *reinterpret_cast<const double2*>(fr + sp * kTcPoints + k);
+            digits_m(valid ? v.x * f.x : 0.0, s42[sp], lo[sp][k], hi[sp][k]);
+            digits_m(valid ? v.y * f.y : 0.0, s42[sp], lo[sp][k + 1], hi[sp][k + 1]);
+          }
         }
         uint8_t* bst = fk_smem + buf * Cfg::kStage + Cfg::kStageA;
 #pragma unroll
-        for (int s = 0; s < kSlices; s++) {
-          uint32_t w[2];
+        for (int sp = 0; sp < NS; sp++)
 #pragma unroll
-          for (int h = 0; h < 2; h++)
-            w[h] = pack_digits(digit_field(lo[4 * h], hi[4 * h], s), digit_field(lo[4 * h + 1], hi[4 * h + 1], s),
-                               digit_field(lo[4 * h + 2], hi[4 * h + 2], s),
-                               digit_field(lo[4 * h + 3], hi[4 * h + 3], s), s == 0);
-          *reinterpret_cast<uint2*>(
-              bst + lio::umma::kmajor_offset(s * Cfg::kLevelRows + sp * kFkCols + lane, k0, Cfg::kTallRows)) =
-              make_uint2(w[0], w[1]);
-        }
+          for (int s = 0; s < kSlices; s++) {
+            uint32_t w[PPT / 4];
+#pragma unroll
+            for (int h = 0; h < PPT / 4; h++)
+              w[h] = pack_digits(digit_field(lo[sp][4 * h], hi[sp][4 * h], s),
+                                 digit_field(lo[sp][4 * h + 1], hi[sp][4 * h + 1], s),
+                                 digit_field(lo[sp][4 * h + 2], hi[sp][4 * h + 2], s),
+                                 digit_field(lo[sp][4 * h + 3], hi[sp][4 * h + 3], s), s == 0);
+            uint8_t* dst =
+                bst + lio::umma::kmajor_offset(s * Cfg::kLevelRows + sp * kFkCols + row, pb, Cfg::kTallRows);
+            if (PPT == 8)
+              *reinterpret_cast<uint2*>(dst) = make_uint2(w[0], w[PPT / 4 - 1]);
+            else
+              *reinterpret_cast<uint32_t*>(dst) = w[0];
+          }
         // generic-proxy stores -> visible to the MMAs (async proxy) once bready completes
         lio::umma::fence_proxy_async_smem();
         __syncwarp();
