@@ -76,27 +76,15 @@ __device__ __forceinline__ double pow2(int k) {
   return (k > -1022 && k < 1024) ? __longlong_as_double((long long)(k + 1023) << 52) : ldexp(1.0, k);
 }
 
-// Next base-128 digit of x (|x| <= 1/2): returns rint(128 x) as an integer and
-// leaves the remainder 128 x - rint(128 x) (|.| <= 1/2) in x, all exactly. The
-// rounding is done by the FP64 adder: 128 x + 1.5 * 2^52 rounds to the nearest
-// integer (ties to even, as rint), whose value sits in the low mantissa bits.
-__device__ __forceinline__ int8_t next_digit(double& x) {
-  constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52
-  const double t = fma(x, 128.0, kRound);
-  const double d = t - kRound;
-  x = fma(x, 128.0, -d);
-  return (int8_t)__double2loint(t);
-}
-
-// All S = 6 digits at once, from one rounding on the FP64 adder instead of one
-// per digit: t = 2^52 + B + x 2^42 with B = 64 (128^6 - 1) / 127 (even) rounds
-// x 2^42 (|x| < 1/2) to the nearest integer N, ties to even, and the low
-// mantissa bits of t hold M = N + B >= 0. The base-128 digits m_k of M less 64
-// are balanced digits of N (|m_k - 64| <= 64), so
+// The S = 6 base-128 digits of x (|x| < 1/2), all from one rounding on the
+// FP64 adder: t = 2^52 + B + x 2^42 with B = 64 (128^6 - 1) / 127 (even) rounds
+// x 2^42 to the nearest integer N, ties to even, and the low mantissa bits of
+// t hold M = N + B >= 0. The base-128 digits m_k of M less 64 are balanced
+// digits of N (|m_k - 64| <= 64), so
 //   x = sum_s (m_(5-s) - 64) 128^-(s+1) + r,  |r| <= 2^-43,
-// the same bound as the digit-by-digit form (whose digits may differ from these
-// where a remainder ties). `s42` is 2^42 times the row's power-of-two scale.
-// Returns t's two 32-bit halves (M = bits 0..42).
+// with two FP64 operations per value instead of three per digit for a
+// digit-by-digit extraction. `s42` is 2^42 times the row's power-of-two scale
+// (digit_scale). Returns t's two 32-bit halves (M = bits 0..42).
 __device__ __forceinline__ void digits_m(double x, double s42, uint32_t& lo, uint32_t& hi) {
   const double t = fma(x, s42, 4505815965769792.0);  // 2^52 + B
   lo = (uint32_t)__double2loint(t);
@@ -152,25 +140,24 @@ __global__ void k_slice_basis(const int2* __restrict__ tiles, const GroupDev* __
     double amax = 0.0;
     for (int j = 0; j < G.m; j++) amax = fmax(amax, fabs(val(a, j)));
     const int e = slice_exponent(amax);
+    const double s42 = digit_scale(e);
     aexp[G.aexp_off + (long long)a * G.ldp + p] = (int16_t)e;
     int8_t* dst = aslices + G.sl_off + (long long)(t.y * NA + a) * nks * kTcStepA;
     // 16 consecutive functions at a time: per slice their 16 digits are one
     // contiguous 16-byte row segment of the K-major block, one store
     for (int j0 = 0; j0 < G.m32; j0 += 16) {
-      double x[16];
+      uint32_t lo[16], hi[16];
 #pragma unroll
-      for (int k = 0; k < 16; k++) x[k] = j0 + k < G.m ? ldexp(val(a, j0 + k), -e) : 0.0;
+      for (int k = 0; k < 16; k++) digits_m(j0 + k < G.m ? val(a, j0 + k) : 0.0, s42, lo[k], hi[k]);
       int8_t* blk = dst + (j0 >> 5) * kTcStepA + lio::umma::kmajor_offset(r, j0 & 31, kTcPoints);
 #pragma unroll
       for (int s = 0; s < kSlices; s++) {
         uint32_t w[4];
 #pragma unroll
-        for (int k4 = 0; k4 < 4; k4++) {
-          uint32_t packed = 0;
-#pragma unroll
-          for (int k = 0; k < 4; k++) packed |= ((uint32_t)(uint8_t)next_digit(x[k4 * 4 + k])) << (8 * k);
-          w[k4] = packed;
-        }
+        for (int k4 = 0; k4 < 4; k4++)
+          w[k4] = pack_digits(digit_field(lo[4 * k4], hi[4 * k4], s), digit_field(lo[4 * k4 + 1], hi[4 * k4 + 1], s),
+                              digit_field(lo[4 * k4 + 2], hi[4 * k4 + 2], s),
+                              digit_field(lo[4 * k4 + 3], hi[4 * k4 + 3], s), s == 0);
         *reinterpret_cast<uint4*>(blk + s * kTcSliceA) = make_uint4(w[0], w[1], w[2], w[3]);
       }
     }
@@ -205,34 +192,33 @@ __global__ void k_slice_density(const int2* __restrict__ tiles, const GroupDev* 
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
   const int e = slice_exponent(amax);
+  const double s42 = digit_scale(e);
   dexp[G.dexp_off + i] = (int16_t)e;
   const int nks = G.m32 / 32;
   int8_t* dst = dslices + G.ds_off + (long long)t.y * nks * kTcStepD;
   // 16 consecutive functions j at a time: per slice one 16-byte row segment
   for (int j0 = 0; j0 < G.m32; j0 += 16) {
-    double x[16];
+    uint32_t lo[16], hi[16];
 #pragma unroll
     for (int k = 0; k < 16; k++) {
       const int j = j0 + k;
-      x[k] = 0.0;
+      double v = 0.0;
       if (i < G.m && j < G.m) {
         const int gj = fg[j];
-        double v = P[packed_index(gi, gj, M)];
+        v = P[packed_index(gi, gj, M)];
         if (gi != gj) v *= 0.5;
-        x[k] = ldexp(v, -e);
       }
+      digits_m(v, s42, lo[k], hi[k]);
     }
     int8_t* blk = dst + (j0 >> 5) * kTcStepD;
 #pragma unroll
     for (int s = 0; s < kSlices; s++) {
       uint32_t w[4];
 #pragma unroll
-      for (int k4 = 0; k4 < 4; k4++) {
-        uint32_t packed = 0;
-#pragma unroll
-        for (int k = 0; k < 4; k++) packed |= ((uint32_t)(uint8_t)next_digit(x[k4 * 4 + k])) << (8 * k);
-        w[k4] = packed;
-      }
+      for (int k4 = 0; k4 < 4; k4++)
+        w[k4] = pack_digits(digit_field(lo[4 * k4], hi[4 * k4], s), digit_field(lo[4 * k4 + 1], hi[4 * k4 + 1], s),
+                            digit_field(lo[4 * k4 + 2], hi[4 * k4 + 2], s),
+                            digit_field(lo[4 * k4 + 3], hi[4 * k4 + 3], s), s == 0);
       *reinterpret_cast<uint4*>(blk + lio::umma::kmajor_offset(s * kTcFuncs + r, j0 & 31, kTcTall)) =
           make_uint4(w[0], w[1], w[2], w[3]);
     }

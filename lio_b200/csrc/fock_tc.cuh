@@ -129,29 +129,27 @@ __global__ void __launch_bounds__(256) k_fock_aslices(const int2* __restrict__ r
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i = t.y + lane, ldp = G.ldp, nkp = ldp / 32;
   const bool valid = i < G.m;
-  const double sc = pow2(-(int)expo[G.fae_off + i]);
+  const double s42 = digit_scale(expo[G.fae_off + i]);
   const int tile = i / kFkRows, r = i % kFkRows;
   for (int b = warp; b < ldp / 16; b += blockDim.x / 32) {
     const int p0 = b * 16;
     const double* Fi = f_row(G, basis, valid ? i : 0, p0, nkb);  // 16 values within one 128-point tile
-    double x[16];
+    uint32_t lo[16], hi[16];
 #pragma unroll
     for (int k = 0; k < 16; k += 2) {
       const double2 v = valid ? *reinterpret_cast<const double2*>(Fi + k) : make_double2(0.0, 0.0);
-      x[k] = v.x * sc;
-      x[k + 1] = v.y * sc;
+      digits_m(v.x, s42, lo[k], hi[k]);
+      digits_m(v.y, s42, lo[k + 1], hi[k + 1]);
     }
     int8_t* blk = sl + G.fa_off + ((long long)tile * nkp + (p0 >> 5)) * kFkStepA;
 #pragma unroll
     for (int s = 0; s < kSlices; s++) {
       uint32_t w[4];
 #pragma unroll
-      for (int k4 = 0; k4 < 4; k4++) {
-        uint32_t packed = 0;
-#pragma unroll
-        for (int k = 0; k < 4; k++) packed |= ((uint32_t)(uint8_t)next_digit(x[k4 * 4 + k])) << (8 * k);
-        w[k4] = packed;
-      }
+      for (int k4 = 0; k4 < 4; k4++)
+        w[k4] = pack_digits(digit_field(lo[4 * k4], hi[4 * k4], s), digit_field(lo[4 * k4 + 1], hi[4 * k4 + 1], s),
+                            digit_field(lo[4 * k4 + 2], hi[4 * k4 + 2], s),
+                            digit_field(lo[4 * k4 + 3], hi[4 * k4 + 3], s), s == 0);
       *reinterpret_cast<uint4*>(blk + s * kFkSliceA + lio::umma::kmajor_offset(r, p0 & 31, kFkRows)) =
           make_uint4(w[0], w[1], w[2], w[3]);
     }
