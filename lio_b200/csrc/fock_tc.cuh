@@ -296,55 +296,70 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
 #pragma unroll
       for (int sp = 0; sp < NS; sp++)
         s42[sp] = valid ? digit_scale((sp == 0 ? bexp_a : bexp_b)[G.fbe_off + j]) : 1.0;
-      for (int st = 0; st < nsteps; st++) {
+      // two K steps per iteration (nsteps is a multiple of 4, so both lie in one 128-point
+      // tile): their independent digit work interleaves, which a warp needs to keep up with
+      // the MMAs
+      constexpr int SU = 2;
+      for (int st = 0; st < nsteps; st += SU) {
         const int T = st >> 2, sub = st & 3, c = T & 1;
-        const int buf = st % kFkStages, use = st / kFkStages;
         bool ok = !*vfail;
         if (ok && sub == 0) ok = lio::umma::mbar_wait(&cfull[c], (T >> 1) & 1);
-        if (ok && use > 0) ok = lio::umma::mbar_wait(&empty[buf], (use - 1) & 1);
+#pragma unroll
+        for (int u = 0; u < SU; u++) {
+          const int use = (st + u) / kFkStages;
+          if (ok && use > 0) ok = lio::umma::mbar_wait(&empty[(st + u) % kFkStages], (use - 1) & 1);
+        }
         if (!__all_sync(0xffffffffu, ok)) {
           *vfail = 1;
           break;
         }
         const uint8_t* slot = ring + c * Cfg::kSlot;
-        const double* Fr = reinterpret_cast<const double*>(slot + row * Cfg::kRowBytes) + sub * 32 + pb;
-        const double* fr = reinterpret_cast<const double*>(slot + kFkCols * Cfg::kRowBytes) + sub * 32 + pb;
-        uint32_t lo[NS][PPT], hi[NS][PPT];
+        uint32_t lo[SU][NS][PPT], hi[SU][NS][PPT];
 #pragma unroll
-        for (int k = 0; k < PPT; k += 2) {
-          const double2 v = *reinterpret_cast<const double2*>(Fr + k);
+        for (int u = 0; u < SU; u++) {
+          const double* Fr = reinterpret_cast<const double*>(slot + row * Cfg::kRowBytes) + (sub + u) * 32 + pb;
+          const double* fr =
+              reinterpret_cast<const double*>(slot + kFkCols * Cfg::kRowBytes) + (sub + u) * 32 + pb;
 #pragma unroll
-          for (int sp = 0; sp < NS; sp++) {
-            const double2 f = *reinterpret_cast<const double2*>(fr + sp * kTcPoints + k);
-            digits_m(valid ? v.x * f.x : 0.0, s42[sp], lo[sp][k], hi[sp][k]);
-            digits_m(valid ? v.y * f.y : 0.0, s42[sp], lo[sp][k + 1], hi[sp][k + 1]);
+          for (int k = 0; k < PPT; k += 2) {
+            const double2 v = *reinterpret_cast<const double2*>(Fr + k);
+#pragma unroll
+            for (int sp = 0; sp < NS; sp++) {
+              const double2 f = *reinterpret_cast<const double2*>(fr + sp * kTcPoints + k);
+              digits_m(valid ? v.x * f.x : 0.0, s42[sp], lo[u][sp][k], hi[u][sp][k]);
+              digits_m(valid ? v.y * f.y : 0.0, s42[sp], lo[u][sp][k + 1], hi[u][sp][k + 1]);
+            }
           }
         }
-        uint8_t* bst = fk_smem + buf * Cfg::kStage + Cfg::kStageA;
 #pragma unroll
-        for (int sp = 0; sp < NS; sp++)
+        for (int u = 0; u < SU; u++) {
+          uint8_t* bst = fk_smem + ((st + u) % kFkStages) * Cfg::kStage + Cfg::kStageA;
 #pragma unroll
-          for (int s = 0; s < kSlices; s++) {
-            uint32_t w[PPT / 4];
+          for (int sp = 0; sp < NS; sp++)
 #pragma unroll
-            for (int h = 0; h < PPT / 4; h++)
-              w[h] = pack_digits(digit_field(lo[sp][4 * h], hi[sp][4 * h], s),
-                                 digit_field(lo[sp][4 * h + 1], hi[sp][4 * h + 1], s),
-                                 digit_field(lo[sp][4 * h + 2], hi[sp][4 * h + 2], s),
-                                 digit_field(lo[sp][4 * h + 3], hi[sp][4 * h + 3], s), s == 0);
-            uint8_t* dst =
-                bst + lio::umma::kmajor_offset(s * Cfg::kLevelRows + sp * kFkCols + row, pb, Cfg::kTallRows);
-            if (PPT == 8)
-              *reinterpret_cast<uint2*>(dst) = make_uint2(w[0], w[PPT / 4 - 1]);
-            else
-              *reinterpret_cast<uint32_t*>(dst) = w[0];
-          }
+            for (int s = 0; s < kSlices; s++) {
+              uint32_t w[PPT / 4];
+#pragma unroll
+              for (int h = 0; h < PPT / 4; h++)
+                w[h] = pack_digits(digit_field(lo[u][sp][4 * h], hi[u][sp][4 * h], s),
+                                   digit_field(lo[u][sp][4 * h + 1], hi[u][sp][4 * h + 1], s),
+                                   digit_field(lo[u][sp][4 * h + 2], hi[u][sp][4 * h + 2], s),
+                                   digit_field(lo[u][sp][4 * h + 3], hi[u][sp][4 * h + 3], s), s == 0);
+              uint8_t* dst =
+                  bst + lio::umma::kmajor_offset(s * Cfg::kLevelRows + sp * kFkCols + row, pb, Cfg::kTallRows);
+              if (PPT == 8)
+                *reinterpret_cast<uint2*>(dst) = make_uint2(w[0], w[PPT / 4 - 1]);
+              else
+                *reinterpret_cast<uint32_t*>(dst) = w[0];
+            }
+        }
         // generic-proxy stores -> visible to the MMAs (async proxy) once bready completes
         lio::umma::fence_proxy_async_smem();
         __syncwarp();
         if (lane == 0) {
-          lio::umma::mbar_arrive(&bready[buf]);
-          if (sub == 3) lio::umma::mbar_arrive(&cempty[c]);
+#pragma unroll
+          for (int u = 0; u < SU; u++) lio::umma::mbar_arrive(&bready[(st + u) % kFkStages]);
+          if (sub + SU - 1 == 3) lio::umma::mbar_arrive(&cempty[c]);
         }
       }
     }
