@@ -74,6 +74,39 @@ struct GroupDev {
   long long fbe_off;   // per-row exponents of f*F (elements): nJ x 32
 };
 
+// Process-wide pinned host staging of the grid build (grow-only, one buffer per
+// use, never returned until exit): a new geometry (every MD step) would
+// otherwise fault in tens of bytes per point of fresh host memory and copy it
+// pageable. Engines of many resident molecules share one buffer rather than
+// each pinning its own; users hold the mutex while they fill and copy it.
+struct PinnedStaging {
+  std::mutex m;
+  void* host = nullptr;
+  size_t bytes = 0;
+  void reserve(size_t need) {
+    if (bytes >= need) return;
+    if (host) cudaFreeHost(host);
+    host = nullptr;
+    bytes = 0;
+    const cudaError_t e = cudaMallocHost(&host, need);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      host = nullptr;
+      throw std::runtime_error(std::string("CUDA error ") + cudaGetErrorString(e) + " pinning " +
+                               std::to_string(need) + " bytes of host staging");
+    }
+    bytes = need;
+  }
+};
+PinnedStaging& weights_staging() {  // Becke weights: points in, factors out
+  static PinnedStaging* w = new PinnedStaging;  // never destroyed: no cudaFreeHost after the runtime's exit
+  return *w;
+}
+PinnedStaging& point_staging() {  // the point arrays of an engine's upload
+  static PinnedStaging* w = new PinnedStaging;
+  return *w;
+}
+
 // device bytes held by every DevBuf of the process (footprint accounting)
 std::atomic<long long> g_devbuf_bytes{0};
 
@@ -887,18 +920,41 @@ void DeviceEngine::release() {
 
 long long DeviceEngine::points() const { return impl_->npoints; }
 
+namespace {
+size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+}  // namespace
+
 void DeviceEngine::becke_weights(const System& sys, const std::vector<PointGroup*>& groups) {
   const long long ng = (long long)groups.size();
   std::vector<long long> first(ng + 1, 0);  // first point of each group in the flat arrays
   for (long long gi = 0; gi < ng; gi++) first[gi + 1] = first[gi] + (long long)groups[gi]->points.size();
   const long long n = first[ng];
   if (n == 0) return;
-  std::vector<double> hx((size_t)n), hy((size_t)n), hz((size_t)n);
-  std::vector<int> hatom((size_t)n), hgroup((size_t)n), hoff(groups.size() + 1, 0), hnucs;
+  std::vector<int> hoff(groups.size() + 1, 0), hnucs;
   for (size_t gi = 0; gi < groups.size(); gi++) {
     hnucs.insert(hnucs.end(), groups[gi]->nucs.begin(), groups[gi]->nucs.end());
     hoff[gi + 1] = (int)hnucs.size();
   }
+  const size_t na = (size_t)sys.natoms;
+  // one layout for the pinned staging and the device block: per point x, y, z,
+  // factor (FP64), atom, group (int); then the group offsets, their nuclei and
+  // the atom tables
+  const size_t o_x = 0, o_y = o_x + align256(n * 8), o_z = o_y + align256(n * 8), o_f = o_z + align256(n * 8);
+  const size_t o_atom = o_f + align256(n * 8), o_group = o_atom + align256(n * 4);
+  const size_t o_off = o_group + align256(n * 4), o_nucs = o_off + align256(hoff.size() * 4);
+  const size_t o_ax = o_nucs + align256(std::max<size_t>(hnucs.size(), 1) * 4);
+  const size_t o_ay = o_ax + align256(na * 8), o_az = o_ay + align256(na * 8), o_rm = o_az + align256(na * 8);
+  const size_t o_dist = o_rm + align256(na * 8), total = o_dist + align256(na * na * 8);
+  PinnedStaging& ws = weights_staging();
+  std::lock_guard<std::mutex> lock(ws.m);  // one grid build at a time uses the staging
+  ws.reserve(total);
+  char* h = static_cast<char*>(ws.host);
+  double* hx = reinterpret_cast<double*>(h + o_x);
+  double* hy = reinterpret_cast<double*>(h + o_y);
+  double* hz = reinterpret_cast<double*>(h + o_z);
+  double* hf = reinterpret_cast<double*>(h + o_f);
+  int* hatom = reinterpret_cast<int*>(h + o_atom);
+  int* hgroup = reinterpret_cast<int*>(h + o_group);
 #pragma omp parallel for schedule(dynamic, 4)
   for (long long gi = 0; gi < ng; gi++) {
     long long k = first[gi];
@@ -911,26 +967,29 @@ void DeviceEngine::becke_weights(const System& sys, const std::vector<PointGroup
       k++;
     }
   }
-  DevBuf<double> dx, dy, dz, dax, day, daz, drm, dist, fac;
-  DevBuf<int> datom, dgroup, doff, dnucs;
-  dx.upload(hx);
-  dy.upload(hy);
-  dz.upload(hz);
-  datom.upload(hatom);
-  dgroup.upload(hgroup);
-  doff.upload(hoff);
-  dnucs.upload(hnucs);
-  dax.upload(sys.ax);
-  day.upload(sys.ay);
-  daz.upload(sys.az);
-  drm.upload(sys.rm);
-  dist.upload(sys.atom_dist);
-  fac.alloc((size_t)n);
-  k_becke_weights<<<(unsigned)((n + 127) / 128), 128>>>(dx.p, dy.p, dz.p, datom.p, dgroup.p, n, doff.p, dnucs.p,
-                                                        dax.p, day.p, daz.p, drm.p, dist.p, sys.natoms, fac.p);
+  std::memcpy(h + o_off, hoff.data(), hoff.size() * 4);
+  if (!hnucs.empty()) std::memcpy(h + o_nucs, hnucs.data(), hnucs.size() * 4);
+  std::memcpy(h + o_ax, sys.ax.data(), na * 8);
+  std::memcpy(h + o_ay, sys.ay.data(), na * 8);
+  std::memcpy(h + o_az, sys.az.data(), na * 8);
+  std::memcpy(h + o_rm, sys.rm.data(), na * 8);
+  std::memcpy(h + o_dist, sys.atom_dist.data(), na * na * 8);
+  DevBuf<char> blk;
+  blk.alloc(total);
+  char* d = blk.p;
+  // inputs: the points (up to the factor slot), then the small tables
+  LIO_CUDA(cudaMemcpy(d, h, o_f, cudaMemcpyHostToDevice));
+  LIO_CUDA(cudaMemcpy(d + o_atom, h + o_atom, total - o_atom, cudaMemcpyHostToDevice));
+  k_becke_weights<<<(unsigned)((n + 127) / 128), 128>>>(
+      reinterpret_cast<const double*>(d + o_x), reinterpret_cast<const double*>(d + o_y),
+      reinterpret_cast<const double*>(d + o_z), reinterpret_cast<const int*>(d + o_atom),
+      reinterpret_cast<const int*>(d + o_group), n, reinterpret_cast<const int*>(d + o_off),
+      reinterpret_cast<const int*>(d + o_nucs), reinterpret_cast<const double*>(d + o_ax),
+      reinterpret_cast<const double*>(d + o_ay), reinterpret_cast<const double*>(d + o_az),
+      reinterpret_cast<const double*>(d + o_rm), reinterpret_cast<const double*>(d + o_dist), sys.natoms,
+      reinterpret_cast<double*>(d + o_f));
   LIO_CUDA(cudaGetLastError());
-  std::vector<double> hf((size_t)n);
-  LIO_CUDA(cudaMemcpy(hf.data(), fac.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+  LIO_CUDA(cudaMemcpy(hf, d + o_f, (size_t)n * 8, cudaMemcpyDeviceToHost));
 #pragma omp parallel for schedule(dynamic, 4)
   for (long long gi = 0; gi < ng; gi++) {
     long long k = first[gi];
@@ -980,7 +1039,6 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
   const int NQ = sys.lda ? 1 : kNQ;
 
   std::vector<GroupDev> gd;
-  std::vector<double> hx, hy, hz, hw;
   std::vector<int> src_group;  // partition group of each device group
   std::vector<int> hfn, hsf, hst, hfsh, hfat;
   std::vector<int8_t> hfcp;
@@ -1072,12 +1130,16 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
     npts_total += G.npts;
     gd.push_back(G);
   }
-  // points of every device group in parallel, SoA at the group's pt_off;
-  // padded slots hold a copy of the first point with zero weight
-  hx.resize(pt_off);
-  hy.resize(pt_off);
-  hz.resize(pt_off);
-  hw.resize(pt_off);
+  // points of every device group in parallel, SoA at the group's pt_off, into
+  // the pinned staging (x, y, z, w one after the other); padded slots hold a
+  // copy of the first point with zero weight
+  PinnedStaging& ps = point_staging();
+  std::lock_guard<std::mutex> ps_lock(ps.m);  // one upload at a time fills it; held until the copies
+  ps.reserve(4 * (size_t)pt_off * sizeof(double));
+  double* hx = static_cast<double*>(ps.host);
+  double* hy = hx + pt_off;
+  double* hz = hy + pt_off;
+  double* hw = hz + pt_off;
 #pragma omp parallel for schedule(dynamic, 4)
   for (long long gi = 0; gi < (long long)gd.size(); gi++) {
     const GroupDev& G = gd[gi];
@@ -1117,10 +1179,11 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
     hnc[i] = sys.ncont[i];
   }
   d->groups.upload(gd);
-  d->px.upload(hx);
-  d->py.upload(hy);
-  d->pz.upload(hz);
-  d->pw.upload(hw);
+  for (auto [buf, src] : {std::pair<DevBuf<double>*, const double*>{&d->px, hx}, {&d->py, hy}, {&d->pz, hz},
+                          {&d->pw, hw}}) {
+    buf->alloc((size_t)pt_off);
+    LIO_CUDA(cudaMemcpy(buf->p, src, (size_t)pt_off * sizeof(double), cudaMemcpyHostToDevice));
+  }
   d->fn_glob.upload(hfn);
   d->fn_sh.upload(hfsh);
   d->fn_atom.upload(hfat);

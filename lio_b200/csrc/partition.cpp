@@ -174,6 +174,16 @@ void host_becke_weights(const System& sys, const std::vector<PointGroup*>& group
   for (PointGroup* g : groups) compute_weights(sys, *g);
 }
 
+// Per-atom point buffers of the grid build, kept by each calling thread from one
+// geometry to the next: allocating them afresh (a few hundred KB per atom) on
+// every call costs page faults that the threads filling them in parallel take
+// one at a time.
+struct PointScratch {
+  std::vector<std::vector<GridPoint>> pts;
+  std::vector<std::vector<long long>> dst;
+};
+static thread_local PointScratch tl_point_scratch;
+
 void build_partition(const System& sys, const Options& opt, const AngularGrid& ang,
                      int grid_type, Partition& out, WeightsFn weights) {
   out.cubes.clear();
@@ -236,8 +246,13 @@ void build_partition(const System& sys, const Options& opt, const AngularGrid& a
   const size_t ncubes_all = (size_t)psize[0] * psize[1] * psize[2];
   std::vector<std::vector<GridPoint>> prism(ncubes_all);
   std::vector<std::vector<GridPoint>> sph(opt.sphere_radius > 0 ? natoms : 0);
-  std::vector<std::vector<GridPoint>> apts(natoms);
-  std::vector<std::vector<long long>> adst(natoms);
+  PointScratch& scratch = tl_point_scratch;  // the calling thread's (the workers fill it)
+  if ((int)scratch.pts.size() < natoms) {
+    scratch.pts.resize(natoms);
+    scratch.dst.resize(natoms);
+  }
+  std::vector<std::vector<GridPoint>>& apts = scratch.pts;
+  std::vector<std::vector<long long>>& adst = scratch.dst;
   bool outside = false;
 #pragma omp parallel for schedule(dynamic, 1) reduction(|| : outside)
   for (int atom = 0; atom < natoms; atom++) {
@@ -245,8 +260,15 @@ void build_partition(const System& sys, const Options& opt, const AngularGrid& a
     const double t0 = M_PI / (ns + 1);
     const double rm = sys.rm[atom];
     const unsigned inc = (unsigned)std::ceil(opt.sphere_radius * ns);
-    std::vector<GridPoint>& P = apts[atom];
-    std::vector<long long>& D = adst[atom];
+    // filled through vectors on this thread's stack (swapped in and out of the
+    // atom's slot): the slots' headers share cache lines between atoms, and a
+    // push_back on them from several threads would bounce those lines
+    std::vector<GridPoint> P;
+    std::vector<long long> D;
+    P.swap(apts[atom]);
+    D.swap(adst[atom]);
+    P.clear();
+    D.clear();
     P.reserve((size_t)ns * ang.size());
     D.reserve((size_t)ns * ang.size());
     for (unsigned shell = 0; shell < ns; shell++) {
@@ -274,6 +296,8 @@ void build_partition(const System& sys, const Options& opt, const AngularGrid& a
         }
       }
     }
+    P.swap(apts[atom]);
+    D.swap(adst[atom]);
   }
   if (outside) throw std::runtime_error("grid point outside the cube prism");
 #pragma omp parallel
@@ -291,8 +315,6 @@ void build_partition(const System& sys, const Options& opt, const AngularGrid& a
       for (size_t q = 0; q < apts[atom].size(); q++)
         if (adst[atom][q] < 0) sph[atom].push_back(apts[atom][q]);
   }
-  apts.clear();
-  adst.clear();
 
   const Screen screen = make_screen(sys, opt, min_exps_func);
 
