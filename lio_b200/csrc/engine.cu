@@ -1134,7 +1134,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
   // the pinned staging (x, y, z, w one after the other); padded slots hold a
   // copy of the first point with zero weight
   PinnedStaging& ps = point_staging();
-  std::lock_guard<std::mutex> ps_lock(ps.m);  // one upload at a time fills it; held until the copies
+  std::lock_guard<std::mutex> ps_lock(ps.m);  // one upload at a time: held to the end of this upload
   ps.reserve(4 * (size_t)pt_off * sizeof(double));
   double* hx = static_cast<double*>(ps.host);
   double* hy = hx + pt_off;
