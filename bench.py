@@ -292,6 +292,15 @@ def ours(args, rank, world):
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / args.steps
+    # the bytes the library moved in the last step (only the packed entries the
+    # groups touch, when that is at most half of the matrix), plus the exchange
+    xh2d, xd2h = C.c_longlong(0), C.c_longlong(0)
+    L.g2g_last_transfer_bytes_(C.byref(xh2d), C.byref(xd2h))
+    lib.check("g2g_last_transfer_bytes_")
+    h2d_b, d2h_b = xh2d.value, xd2h.value
+    if world > 1:
+        h2d_b += (1 + nspin * npacked) * 8
+        d2h_b += 8
 
     # device-resident throughput
     L.g2g_solve_resident_.restype = C.c_int
@@ -373,7 +382,7 @@ def ours(args, rank, world):
                    "l2": "inputs larger than L2 (resident basis cache of %.1f GB)" % (nk * pm * 8 / 1e9),
                    "grid_build_s": round(grid_s, 3), "E_xc": E},
         "e2e": {"value": total_pts / (e2e_ms * 1e-3), "unit": UNIT,
-                "h2d_bytes_per_step": npacked * 8 * nspin, "d2h_bytes_per_step": npacked * 8 * nspin + 8},
+                "h2d_bytes_per_step": h2d_b, "d2h_bytes_per_step": d2h_b},
         "gpu_launches": int(launches) * args.steps,
         "stage_ms": dict(zip(STAGES, stage_ms)),
         "roofline": {"bound": "hbm", "achieved": dens_bytes / t_dens / 1e9, "peak": hbm,
@@ -434,6 +443,9 @@ def forces_mode(args):
     with ClockSampler(0) as clk:
         f_ms, (E, F) = timed(force_call)
     k_ms = float(np.mean(kernel_ms[-args.steps:]))
+    xh2d = C.c_longlong(0)
+    lib.lib.g2g_last_transfer_bytes_(C.byref(xh2d), None)
+    lib.check("g2g_last_transfer_bytes_")
     e_ms, _ = timed(lambda: lib.solve_groups(1))
     tc = args.precision == 1 and wl.iexch > 3
     hbm, _, src = load_peaks()
@@ -459,7 +471,7 @@ def forces_mode(args):
            "config": {"workload": wl.name, "points": npts, "atoms": wl.mol.natom,
                       "precision_of_build": args.precision, "max_abs_force": float(np.max(np.abs(F))), "E_xc": E},
            "e2e": {"value": npts / (f_ms * 1e-3), "unit": UNIT,
-                   "h2d_bytes_per_step": nspin * 8 * (wl.basis.M * (wl.basis.M + 1) // 2),
+                   "h2d_bytes_per_step": xh2d.value,
                    "d2h_bytes_per_step": 3 * 8 * wl.mol.natom + 8},
            "energy_only_ms": e_ms, "force_kernel_ms": k_ms, "roofline": roof,
            "clocks": clk.summary()}

@@ -210,6 +210,15 @@ void g2g_set_device_weights_(const unsigned int* on);
  * it is not included), or -1 without a device engine. */
 double g2g_last_force_ms_(void);
 
+/* No counterpart in the reference: bytes the last g2g_solve_groups_ moved
+ * between the caller's arrays and the device (h2d: density values; d2h:
+ * Kohn-Sham values and the energy). When the point groups touch at most half
+ * of the packed matrix, only those entries travel: the density's are gathered
+ * from the caller's vector and scattered on the device, the Kohn-Sham
+ * contributions gathered on the device and added into the caller's vector
+ * (every other entry's XC contribution is zero). */
+void g2g_last_transfer_bytes_(long long* h2d, long long* d2h);
+
 /* No counterpart in the reference: an XC build that allocates no device
  * memory, for callers that cannot call cudaMalloc (a host program whose
  * allocator already owns all of the GPU's memory, or code that must not

@@ -161,6 +161,24 @@ void host_accumulate(double* dst, const double* src, size_t n) {
   for (long long i = 0; i < (long long)n; i++) dst[i] += src[i];
 }
 
+// Compact transfers of a host-array solve: only the packed entries some group
+// touches (sorted, unique `idx`, n per spin) cross PCIe. The density's are
+// scattered into the full device matrices (the kernels read no other entry);
+// the Kohn-Sham matrices' are gathered before the download (no other entry
+// receives an XC contribution).
+__global__ void k_scatter_packed(const double* __restrict__ src, const long long* __restrict__ idx, long long n,
+                                 int nspin, double* __restrict__ a, double* __restrict__ b) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n * nspin;
+       k += (long long)gridDim.x * blockDim.x)
+    (k < n ? a : b)[idx[k < n ? k : k - n]] = src[k];
+}
+__global__ void k_gather_packed(const double* __restrict__ a, const double* __restrict__ b,
+                                const long long* __restrict__ idx, long long n, int nspin, double* __restrict__ dst) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n * nspin;
+       k += (long long)gridDim.x * blockDim.x)
+    dst[k] = (k < n ? a : b)[idx[k < n ? k : k - n]];
+}
+
 __device__ __forceinline__ long long packed_index(int gi, int gj, int M) {
   const long long lo = gi < gj ? gi : gj, hi = gi < gj ? gj : gi;
   return lo * M - (lo * (lo - 1)) / 2 + (hi - lo);
@@ -791,6 +809,13 @@ struct DeviceEngine::Impl {
   DevBuf<int2> basis_tiles, func_tiles;
   DevBuf<int4> dens_tiles, fock_tiles;
   DevBuf<double> P_a, P_b, K_a, K_b, part_a, part_b, fac_a, fac_b, eblocks, energy;
+  // packed entries the groups touch (sorted); when they are at most half of the
+  // packed matrix, host-array solves move only these (Pc, Kc: nspin x npairs)
+  std::vector<long long> hpidx;
+  DevBuf<long long> pidx;
+  DevBuf<double> Pc, Kc;
+  bool compact = false;
+  long long last_h2d = 0, last_d2h = 0;  // bytes of the last host-array solve
   double* hK = nullptr;  // pinned: Kohn-Sham result of the last solve (nspin x npacked)
   double* hP = nullptr;  // pinned: staging of the caller's densities (nspin x npacked)
   size_t pinned_elems = 0;
@@ -998,6 +1023,10 @@ void DeviceEngine::becke_weights(const System& sys, const std::vector<PointGroup
 }
 
 double DeviceEngine::last_force_kernel_ms() const { return impl_->last_force_ms; }
+void DeviceEngine::last_transfer_bytes(long long* h2d, long long* d2h) const {
+  if (h2d) *h2d = impl_->last_h2d;
+  if (d2h) *d2h = impl_->last_d2h;
+}
 
 void DeviceEngine::set_accumulators(double* d_fock_a, double* d_fock_b, double* d_energy) {
   Impl* d = impl_.get();
@@ -1213,6 +1242,32 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
   d->fock_tiles.upload(ktiles);
 
   const size_t npacked = (size_t)sys.M * (sys.M + 1) / 2;
+  {
+    // the packed entries this engine's groups touch (fn_glob is increasing within a group)
+    std::vector<unsigned char> touched(npacked, 0);
+    const long long Ml = sys.M;
+    for (const GroupDev& G : gd) {
+      const int* f = hfn.data() + G.fn_off;
+      for (int a = 0; a < G.m; a++) {
+        const long long lo = f[a], row = lo * Ml - (lo * (lo - 1)) / 2 - lo;
+        for (int b = a; b < G.m; b++) touched[(size_t)(row + f[b])] = 1;
+      }
+    }
+    d->hpidx.clear();
+    for (size_t e = 0; e < npacked; e++)
+      if (touched[e]) d->hpidx.push_back((long long)e);
+    d->compact = !d->hpidx.empty() && 2 * d->hpidx.size() <= npacked;
+    const size_t nsp = sys.open ? 2 : 1;
+    if (d->compact) {
+      d->pidx.upload(d->hpidx);
+      d->Pc.alloc(nsp * d->hpidx.size());
+      d->Kc.alloc(nsp * d->hpidx.size());
+    } else {
+      d->pidx.free();
+      d->Pc.free();
+      d->Kc.free();
+    }
+  }
   d->P_a.alloc(npacked);
   LIO_CUDA(cudaMemset(d->P_a.p, 0, npacked * sizeof(double)));
   d->K_a.alloc(npacked);
@@ -1604,16 +1659,37 @@ void DeviceEngine::enqueue(const SolveRequest& req) {
     // the caller's (pageable) densities through pinned staging: a threaded host
     // copy, then one full-speed copy per spin
     const int nspin = d->open ? 2 : 1;
-    // in pieces, so that the host copy of one piece overlaps the transfer of the last
-    const size_t piece = std::max<size_t>(npacked / 8, 1 << 16);
-    for (int s = 0; s < nspin; s++) {
-      const double* src = d->open ? (s == 0 ? req.rho_a : req.rho_b) : req.rho;
-      double* dst = s == 0 ? d->P_a.p : d->P_b.p;
-      for (size_t o = 0; o < npacked; o += piece) {
-        const size_t n = std::min(piece, npacked - o);
-        host_copy(d->hP + s * npacked + o, src + o, n);
-        LIO_CUDA(cudaMemcpyAsync(dst + o, d->hP + s * npacked + o, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (d->compact) {
+      // the touched entries only: gathered per spin by all host threads, each
+      // spin sent while the next is gathered, then scattered on the device
+      const long long np = (long long)d->hpidx.size();
+      const long long* ix = d->hpidx.data();
+      for (int s = 0; s < nspin; s++) {
+        const double* src = d->open ? (s == 0 ? req.rho_a : req.rho_b) : req.rho;
+        double* h = d->hP + (size_t)s * np;
+#pragma omp parallel for schedule(static) if (np > (1 << 16))
+        for (long long k = 0; k < np; k++) h[k] = src[ix[k]];
+        LIO_CUDA(cudaMemcpyAsync(d->Pc.p + (size_t)s * np, h, (size_t)np * sizeof(double), cudaMemcpyHostToDevice,
+                                 st));
       }
+      k_scatter_packed<<<(unsigned)std::min<long long>((nspin * np + 255) / 256, 4096), 256, 0, st>>>(
+          d->Pc.p, d->pidx.p, np, nspin, d->P_a.p, d->open ? d->P_b.p : nullptr);
+      LIO_CUDA(cudaGetLastError());
+      d->last_h2d = (long long)nspin * np * (long long)sizeof(double);
+    } else {
+      // in pieces, so that the host copy of one piece overlaps the transfer of the last
+      const size_t piece = std::max<size_t>(npacked / 8, 1 << 16);
+      for (int s = 0; s < nspin; s++) {
+        const double* src = d->open ? (s == 0 ? req.rho_a : req.rho_b) : req.rho;
+        double* dst = s == 0 ? d->P_a.p : d->P_b.p;
+        for (size_t o = 0; o < npacked; o += piece) {
+          const size_t n = std::min(piece, npacked - o);
+          host_copy(d->hP + s * npacked + o, src + o, n);
+          LIO_CUDA(
+              cudaMemcpyAsync(dst + o, d->hP + s * npacked + o, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        }
+      }
+      d->last_h2d = (long long)nspin * (long long)npacked * (long long)sizeof(double);
     }
   }
   // graph replay when on (not while profiling: the stage events are recorded eagerly)
@@ -1649,8 +1725,23 @@ void DeviceEngine::enqueue(const SolveRequest& req) {
     LIO_CUDA(cudaMemcpyAsync(d->hE, d->energy.p, sizeof(double), cudaMemcpyDeviceToHost, st));
     if (tc) LIO_CUDA(cudaMemcpyAsync(d->hErr, d->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     d->nchunks = 0;
-    if (req.compute_rmm) {  // nspin x npacked values in up to kMaxChunks pieces, an event after each
+    d->last_d2h = (long long)sizeof(double);  // the energy
+    if (req.compute_rmm && d->compact) {  // the touched entries, gathered, in pieces with an event after each
+      const long long np = (long long)d->hpidx.size();
+      k_gather_packed<<<(unsigned)std::min<long long>((nspin * np + 255) / 256, 4096), 256, 0, st>>>(
+          d->K_a.p, d->open ? d->K_b.p : nullptr, d->pidx.p, np, nspin, d->Kc.p);
+      LIO_CUDA(cudaGetLastError());
+      const size_t total = (size_t)nspin * np;
+      const size_t piece = std::max<size_t>((total + Impl::kMaxChunks - 1) / Impl::kMaxChunks, 1 << 16);
+      for (size_t o = 0; o < total; o += piece, d->nchunks++) {
+        LIO_CUDA(cudaMemcpyAsync(d->hK + o, d->Kc.p + o, std::min(piece, total - o) * sizeof(double),
+                                 cudaMemcpyDeviceToHost, st));
+        LIO_CUDA(cudaEventRecord(d->kev[d->nchunks], st));
+      }
+      d->last_d2h += (long long)total * (long long)sizeof(double);
+    } else if (req.compute_rmm) {  // nspin x npacked values in up to kMaxChunks pieces, an event after each
       const size_t total = (size_t)nspin * npacked;
+      d->last_d2h += (long long)total * (long long)sizeof(double);
       const size_t piece = std::max<size_t>((total + Impl::kMaxChunks - 1) / Impl::kMaxChunks, 1 << 16);
       for (size_t o = 0; o < total; o += piece, d->nchunks++) {
         const size_t n = std::min(piece, total - o);
@@ -1691,7 +1782,23 @@ SolveResult DeviceEngine::finish(const SolveRequest& req) {
     LIO_CUDA(cudaEventSynchronize(d->ev1));
     throw std::runtime_error("tensor-core density: an MMA completion wait timed out");
   }
-  if (req.compute_rmm) {  // chunk by chunk as they arrive (the same pieces enqueue downloaded)
+  if (req.compute_rmm && d->compact) {  // scatter-added chunk by chunk as they arrive
+    const int nspin = d->open ? 2 : 1;
+    const long long np = (long long)d->hpidx.size();
+    const long long* ix = d->hpidx.data();
+    const size_t total = (size_t)nspin * np;
+    const size_t piece = std::max<size_t>((total + Impl::kMaxChunks - 1) / Impl::kMaxChunks, 1 << 16);
+    int c = 0;
+    for (size_t o = 0; o < total; o += piece, c++) {
+      LIO_CUDA(cudaEventSynchronize(d->kev[c]));
+      const long long k1 = (long long)std::min(o + piece, total);
+#pragma omp parallel for schedule(static) if (k1 - (long long)o > (1 << 16))
+      for (long long k = (long long)o; k < k1; k++) {
+        double* f = k < np ? req.fock : req.fock_b;  // indices are unique: no two threads add to one entry
+        f[ix[k < np ? k : k - np]] += d->hK[k];
+      }
+    }
+  } else if (req.compute_rmm) {  // chunk by chunk as they arrive (the same pieces enqueue downloaded)
     const int nspin = d->open ? 2 : 1;
     const size_t total = (size_t)nspin * npacked;
     const size_t piece = std::max<size_t>((total + Impl::kMaxChunks - 1) / Impl::kMaxChunks, 1 << 16);

@@ -64,6 +64,10 @@ class DeviceEngine {
   SolveResult solve_forces(const SolveRequest& req, double* forces, int ld);
   // device ms of the last solve_forces' force kernel (CUDA events around it)
   double last_force_kernel_ms() const;
+  // bytes the last host-array solve moved: densities in, Kohn-Sham values (and
+  // the energy) out; only the packed entries the groups touch when those are at
+  // most half of the matrix
+  void last_transfer_bytes(long long* h2d, long long* d2h) const;
   // External accumulators for resident solves (nullptr: off): the Kohn-Sham
   // contraction's FP64 atomics and the energy sum add (+=) into these device
   // buffers, which the caller zeroes, instead of the engine's own. Shards of a

@@ -455,6 +455,14 @@ double g2g_last_force_ms_(void) {
   return ms;
 }
 
+void g2g_last_transfer_bytes_(long long* h2d, long long* d2h) {
+  guarded("g2g_last_transfer_bytes_", [&] {
+    State& s = st();
+    if (!s.engine) throw std::runtime_error("no device engine");
+    s.engine->last_transfer_bytes(h2d, d2h);
+  });
+}
+
 int g2g_stage_times_(double* ms, int* solves) {
   int n = 0;
   guarded("g2g_stage_times_", [&] {
