@@ -300,20 +300,62 @@ void build_partition(const System& sys, const Options& opt, const AngularGrid& a
     D.swap(adst[atom]);
   }
   if (outside) throw std::runtime_error("grid point outside the cube prism");
-#pragma omp parallel
-  {
-    const int nt = omp_get_num_threads(), t = omp_get_thread_num();
-    const long long c0 = (long long)(ncubes_all * t / nt), c1 = (long long)(ncubes_all * (t + 1) / nt);
+  const size_t ncount = (size_t)natoms * ncubes_all;
+  if (ncount <= ((size_t)1 << 26)) {
+    // counting sort: points per (atom, cube), start offsets by a prefix over the
+    // atoms within each cube, then every atom's points written in parallel to
+    // their places (atom-major, each atom's order: the serial loop's order)
+    std::vector<int> at((size_t)ncount, 0);  // [atom][cube]: count, then start offset
+#pragma omp parallel for schedule(dynamic, 1)
     for (int atom = 0; atom < natoms; atom++) {
+      int* row = at.data() + (size_t)atom * ncubes_all;
+      for (long long c : adst[atom])
+        if (c >= 0) row[c]++;
+    }
+#pragma omp parallel for schedule(dynamic, 16)
+    for (long long c = 0; c < (long long)ncubes_all; c++) {
+      int run = 0;
+      for (int atom = 0; atom < natoms; atom++) {
+        int& v = at[(size_t)atom * ncubes_all + (size_t)c];
+        const int n = v;
+        v = run;
+        run += n;
+      }
+      prism[(size_t)c].resize((size_t)run);
+    }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int atom = 0; atom < natoms; atom++) {
+      int* row = at.data() + (size_t)atom * ncubes_all;
       const std::vector<GridPoint>& P = apts[atom];
       const std::vector<long long>& D = adst[atom];
-      for (size_t q = 0; q < P.size(); q++)
-        if (D[q] >= c0 && D[q] < c1) prism[(size_t)D[q]].push_back(P[q]);
+      std::vector<GridPoint> mine;  // the atom's sphere points (filled on this thread's stack)
+      for (size_t q = 0; q < P.size(); q++) {
+        if (D[q] >= 0)
+          prism[(size_t)D[q]][(size_t)row[D[q]]++] = P[q];
+        else if (atom < (int)sph.size())
+          mine.push_back(P[q]);
+      }
+      if (atom < (int)sph.size()) sph[atom].swap(mine);
     }
+  } else {
+#pragma omp parallel
+    {
+      const int nt = omp_get_num_threads(), t = omp_get_thread_num();
+      const long long c0 = (long long)(ncubes_all * t / nt), c1 = (long long)(ncubes_all * (t + 1) / nt);
+      for (int atom = 0; atom < natoms; atom++) {
+        const std::vector<GridPoint>& P = apts[atom];
+        const std::vector<long long>& D = adst[atom];
+        for (size_t q = 0; q < P.size(); q++)
+          if (D[q] >= c0 && D[q] < c1) prism[(size_t)D[q]].push_back(P[q]);
+      }
 #pragma omp for schedule(dynamic, 8)
-    for (int atom = 0; atom < (int)sph.size(); atom++)
-      for (size_t q = 0; q < apts[atom].size(); q++)
-        if (adst[atom][q] < 0) sph[atom].push_back(apts[atom][q]);
+      for (int atom = 0; atom < (int)sph.size(); atom++) {
+        std::vector<GridPoint> mine;
+        for (size_t q = 0; q < apts[atom].size(); q++)
+          if (adst[atom][q] < 0) mine.push_back(apts[atom][q]);
+        sph[atom].swap(mine);
+      }
+    }
   }
 
   const Screen screen = make_screen(sys, opt, min_exps_func);
