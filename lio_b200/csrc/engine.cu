@@ -1314,6 +1314,15 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
 // gradient) and of the Kohn-Sham A operand (F).
 void DeviceEngine::prepare_tensor_core() {
   Impl* d = impl_.get();
+  // The Kohn-Sham contraction sums over a group's points: its int32 level
+  // accumulators hold (l + 1) * 64 * 64 * K at most, below 2^31 for K up to
+  // 87,381 (the density and force contractions sum over functions, far fewer).
+  constexpr int kTcMaxGroupPoints = 87296;  // a multiple of the 128-point padding
+  for (const GroupDev& G : d->hgroups)
+    if (G.ldp > kTcMaxGroupPoints)
+      throw std::runtime_error("tensor-core form: a point group of " + std::to_string(G.ldp) +
+                               " padded points exceeds its limit of " + std::to_string(kTcMaxGroupPoints) +
+                               " (int32 level accumulators); use the FP64 form or a smaller little_cube_size");
   cudaStream_t st = d->stream;
   // the FP64 form's function-major cache is not needed (and not kept): every
   // tensor-core operand is built from the blocked copy, computed directly
