@@ -361,35 +361,47 @@ void build_partition(const System& sys, const Options& opt, const AngularGrid& a
   const Screen screen = make_screen(sys, opt, min_exps_func);
 
   // cubes (:331-399): screening against the cube box, then weights
+  // every cube screened in parallel into its own slot, then the kept ones taken
+  // in the serial loop's (i, j, k) order
   std::vector<PointGroup> cand_cubes, cand_spheres;
-  std::vector<double> dists(natoms);
-  for (unsigned i = 0; i < psize[0]; i++)
-    for (unsigned j = 0; j < psize[1]; j++)
-      for (unsigned k = 0; k < psize[2]; k++) {
-        std::vector<GridPoint>& pts = prism[((size_t)i * psize[1] + j) * psize[2] + k];
-        // an empty cube never becomes a group (it has fewer than min_points_per_cube >= 1 points)
-        if (pts.empty() && opt.min_points_per_cube > 0) continue;
-        const double cc[3] = {x0[0] + i * lcs, x0[1] + j * lcs, x0[2] + k * lcs};
-        for (int a = 0; a < natoms; a++) {
-          const double pos[3] = {sys.ax[a], sys.ay[a], sys.az[a]};
-          double dv[3];
-          for (int d = 0; d < 3; d++) {
-            if (pos[d] < cc[d])
-              dv[d] = cc[d] - pos[d];
-            else if (pos[d] > (cc[d] + lcs))
-              dv[d] = pos[d] - (cc[d] + lcs);
-            else
-              dv[d] = 0;
-          }
-          dists[a] = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
+  std::vector<PointGroup> cube_slot(ncubes_all);
+  std::vector<char> cube_kept(ncubes_all, 0);
+#pragma omp parallel
+  {
+    std::vector<double> dists(natoms);
+#pragma omp for schedule(dynamic, 4)
+    for (long long c = 0; c < (long long)ncubes_all; c++) {
+      const unsigned i = (unsigned)(c / ((long long)psize[1] * psize[2]));
+      const unsigned j = (unsigned)((c / psize[2]) % psize[1]);
+      const unsigned k = (unsigned)(c % psize[2]);
+      std::vector<GridPoint>& pts = prism[(size_t)c];
+      // an empty cube never becomes a group (it has fewer than min_points_per_cube >= 1 points)
+      if (pts.empty() && opt.min_points_per_cube > 0) continue;
+      const double cc[3] = {x0[0] + i * lcs, x0[1] + j * lcs, x0[2] + k * lcs};
+      for (int a = 0; a < natoms; a++) {
+        const double pos[3] = {sys.ax[a], sys.ay[a], sys.az[a]};
+        double dv[3];
+        for (int d = 0; d < 3; d++) {
+          if (pos[d] < cc[d])
+            dv[d] = cc[d] - pos[d];
+          else if (pos[d] > (cc[d] + lcs))
+            dv[d] = pos[d] - (cc[d] + lcs);
+          else
+            dv[d] = 0;
         }
-        PointGroup g;
-        g.sphere = false;
-        assign_functions(sys, opt, dists, min_exps_func, screen, g);
-        if (g.funcs.empty() || pts.size() < opt.min_points_per_cube) continue;
-        g.points.swap(pts);
-        cand_cubes.push_back(std::move(g));
+        dists[a] = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
       }
+      PointGroup& g = cube_slot[(size_t)c];
+      g.sphere = false;
+      assign_functions(sys, opt, dists, min_exps_func, screen, g);
+      if (g.funcs.empty() || pts.size() < opt.min_points_per_cube) continue;
+      g.points.swap(pts);
+      cube_kept[(size_t)c] = 1;
+    }
+  }
+  for (size_t c = 0; c < ncubes_all; c++)
+    if (cube_kept[c]) cand_cubes.push_back(std::move(cube_slot[c]));
+  std::vector<double> dists(natoms);
 
   // spheres (:402-462)
   if (opt.sphere_radius > 0) {
