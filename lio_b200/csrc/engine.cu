@@ -124,15 +124,20 @@ struct DevBuf {
       n = count;
       return;
     }
+    // a buffer that must grow (a new geometry with a few more points) gets
+    // 1/16 headroom, so that the next small growth reuses it; first
+    // allocations are exact
+    const size_t want = p ? count + count / 16 : count;
     free();
-    const cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    const cudaError_t e = cudaMalloc(&p, want * sizeof(T));
     if (e != cudaSuccess) {  // clear the thread's last error: later launch checks must not see it
       cudaGetLastError();
       p = nullptr;
       throw std::runtime_error(std::string("CUDA error ") + cudaGetErrorString(e) + " allocating " +
                                std::to_string(count * sizeof(T)) + " bytes");
     }
-    n = cap = count;
+    n = count;
+    cap = want;
     g_devbuf_bytes += (long long)(cap * sizeof(T));
   }
   void upload(const std::vector<T>& v) {
@@ -999,9 +1004,15 @@ void DeviceEngine::becke_weights(const System& sys, const std::vector<PointGroup
   std::memcpy(h + o_az, sys.az.data(), na * 8);
   std::memcpy(h + o_rm, sys.rm.data(), na * 8);
   std::memcpy(h + o_dist, sys.atom_dist.data(), na * na * 8);
-  DevBuf<char> blk;
-  blk.alloc(total);
-  char* d = blk.p;
+  // the device block is kept per device too (grow-only, never freed): no
+  // cudaMalloc / cudaFree of ~50 bytes per point on every geometry
+  static DevBuf<char>* blocks[64] = {};
+  int dev = 0;
+  LIO_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) throw std::runtime_error("device ordinal out of range for the weights block");
+  if (!blocks[dev]) blocks[dev] = new DevBuf<char>;
+  blocks[dev]->alloc(total);
+  char* d = blocks[dev]->p;
   // inputs: the points (up to the factor slot), then the small tables
   LIO_CUDA(cudaMemcpy(d, h, o_f, cudaMemcpyHostToDevice));
   LIO_CUDA(cudaMemcpy(d + o_atom, h + o_atom, total - o_atom, cudaMemcpyHostToDevice));
