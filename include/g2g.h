@@ -113,10 +113,14 @@ void g2g_set_angular_grid_(const unsigned int* grid_type, const unsigned int* np
                            const double* e, const double* wang);
 
 /* Arithmetic of the two contractions (density and Kohn-Sham update):
- * 0 = FP64 on the CUDA cores (the plain form), 1 = tensor-core form,
- * 2 = autotuned: after each grid upload one build of each form is timed and
- * the faster kept (both meet the accuracy bar; small molecules, whose
- * function tiles are mostly padding, often run faster in FP64). */
+ * 0 = FP64 on the CUDA cores (the plain form), 1 = tensor-core form (a grid it
+ * cannot run is refused with an error), 2 = autotuned: after each grid upload
+ * one build of each form is timed and the faster kept (both meet the accuracy
+ * bar; small molecules, whose function tiles are mostly padding, often run
+ * faster in FP64), 3 = the default for a caller that never calls this: the
+ * tensor-core form, with the FP64 form for a grid the tensor-core form cannot
+ * run (a point group above 87,296 padded points, or more significant
+ * functions in one group than a block's shared memory holds). */
 void g2g_set_precision_(const unsigned int* mode);
 
 /* Partition statistics of the current grid: out[0] = groups, out[1] = cubes,
@@ -236,10 +240,26 @@ void g2g_last_transfer_bytes_(long long* h2d, long long* d2h);
  * capture. All calls share the array: calls that overlap on the GPU (on
  * different streams or from different threads) race and corrupt each other.
  * The grid itself (points, basis values) must already be resident, built by
- * g2g_reload_atom_positions_. stream: a cudaStream_t, or NULL for the
- * library's own stream. Returns 0 on success. */
+ * g2g_reload_atom_positions_ in the FP64 form (g2g_set_precision_(0) before
+ * the grid build): the tensor-core form, the default, does not keep the FP64
+ * basis values this path reads, and since building them would allocate, the
+ * call is then refused with an error rather than run. stream: a cudaStream_t,
+ * or NULL for the library's own stream. Returns 0 on success. */
 int g2g_solve_device_noalloc_(const double* d_rho_a, const double* d_rho_b, double* d_fock_a,
                               double* d_fock_b, double* d_energy, void* stream);
+
+/* Failure-path self-test (no counterpart in the reference, which aborts with
+ * exit(1) on a failed build, g2g/partition.cpp:584-590). Every wait of the
+ * pipelined tensor-core kernels on an mbarrier is bounded; when one runs out,
+ * the kernel records the failure, lets its copies in flight land, frees its
+ * TMEM and returns, and the host reports an error instead of hanging. This
+ * runs that path on purpose: a one-CTA kernel whose producer arms and sends
+ * the first of two ring stages and then stops, while the consumer waits for
+ * both with a limit of *polls polls. Returns 1 when the second wait ran out
+ * as intended (then the sticky status is 3 and g2g_last_error_ carries the
+ * message), 0 if it did not run out, -1 on an error; *ms gets the kernel's
+ * device time. The GPU context stays usable for the next build. */
+int g2g_selftest_bounded_wait_(const unsigned int* polls, double* ms);
 
 /* Diagnostic (no counterpart in the reference): runs one tcgen05 int8 tensor-
  * core product D[128 x N] = A[128 x K] * B[N x K]^T (row-major host arrays,

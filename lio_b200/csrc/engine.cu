@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(256) k_density_fp64(const int4* __restrict__ t
                                                       const int* __restrict__ fn_glob,
                                                       const double* __restrict__ basis,
                                                       const double* __restrict__ P, int M,
-                                                      double* __restrict__ partial) {
+                                                      double* __restrict__ partial, long long part_base) {
   constexpr int NQ = NA == 1 ? 1 : kNQ;
   __shared__ double As[NA][kKStep][kTile];
   __shared__ double Bs[kKStep][kTile + 1];
@@ -397,7 +397,7 @@ __global__ void __launch_bounds__(256) k_density_fp64(const int4* __restrict__ t
       q[k] = v;
     }
     if (tx == 0) {
-      double* dst = partial + G.part_off;
+      double* dst = partial + (G.part_off - part_base);
 #pragma unroll
       for (int k = 0; k < NQ; k++) dst[((long long)ft * NQ + k) * G.ldp + p] = q[k];
     }
@@ -624,7 +624,8 @@ __global__ void __launch_bounds__(kFuncBlock, 8) k_functional(const int2* __rest
                                                            const double* __restrict__ part_b, int part_tile,
                                                            int iexch, double* __restrict__ fac_a,
                                                            double* __restrict__ fac_b,
-                                                           double* __restrict__ energy_blocks) {
+                                                           double* __restrict__ energy_blocks, long long part_base,
+                                                           long long pt_base) {
   constexpr bool kLda = MODE == 0 || MODE == 3, kOpen = MODE >= 2;
   constexpr int NQ = kLda ? 1 : kNQ;
   __shared__ double sh[32];
@@ -642,7 +643,7 @@ __global__ void __launch_bounds__(kFuncBlock, 8) k_functional(const int2* __rest
     for (int f = 0; f < nparts; f++)
 #pragma unroll
       for (int k = 0; k < NQ; k++) {
-        const long long o = G.part_off + ((long long)f * NQ + k) * ldp + p;
+        const long long o = G.part_off - part_base + ((long long)f * NQ + k) * ldp + p;
         qa[k] += part_a[o];
         if (kOpen) qb[k] += part_b[o];
       }
@@ -664,28 +665,33 @@ __global__ void __launch_bounds__(kFuncBlock, 8) k_functional(const int2* __rest
         va = w * o.v;
       }
     }
-    fac_a[G.pt_off + p] = va;
-    if (kOpen) fac_b[G.pt_off + p] = vb;
+    fac_a[G.pt_off - pt_base + p] = va;
+    if (kOpen) fac_b[G.pt_off - pt_base + p] = vb;
   }
   const double s = block_sum(e, sh);
   if (threadIdx.x == 0) energy_blocks[blockIdx.x] = s;
 }
 
+// part_base / pt_base: offsets (elements) subtracted from every group's
+// part_off / pt_off when indexing the partials and the factors, for callers
+// whose arrays hold only a batch of groups (the weights pw are always indexed
+// by the group's own pt_off)
 void launch_functional(bool lda, bool open, unsigned nblocks, cudaStream_t st, const int2* tiles,
                        const GroupDev* groups, const double* pw, const double* part_a, const double* part_b,
-                       int part_tile, int iexch, double* fac_a, double* fac_b, double* eblocks) {
+                       int part_tile, int iexch, double* fac_a, double* fac_b, double* eblocks,
+                       long long part_base = 0, long long pt_base = 0) {
+#define LIO_FUNCTIONAL(MODE)                                                                                \
+  k_functional<MODE><<<nblocks, kFuncBlock, 0, st>>>(tiles, groups, pw, part_a, part_b, part_tile, iexch, fac_a, \
+                                                     fac_b, eblocks, part_base, pt_base)
   if (!open && lda)
-    k_functional<0><<<nblocks, kFuncBlock, 0, st>>>(tiles, groups, pw, part_a, part_b, part_tile, iexch, fac_a, fac_b,
-                                                    eblocks);
+    LIO_FUNCTIONAL(0);
   else if (!open)
-    k_functional<1><<<nblocks, kFuncBlock, 0, st>>>(tiles, groups, pw, part_a, part_b, part_tile, iexch, fac_a, fac_b,
-                                                    eblocks);
+    LIO_FUNCTIONAL(1);
   else if (!lda)
-    k_functional<2><<<nblocks, kFuncBlock, 0, st>>>(tiles, groups, pw, part_a, part_b, part_tile, iexch, fac_a, fac_b,
-                                                    eblocks);
+    LIO_FUNCTIONAL(2);
   else
-    k_functional<3><<<nblocks, kFuncBlock, 0, st>>>(tiles, groups, pw, part_a, part_b, part_tile, iexch, fac_a, fac_b,
-                                                    eblocks);
+    LIO_FUNCTIONAL(3);
+#undef LIO_FUNCTIONAL
 }
 
 // E_xc of the build from the per-block partials: written, or (accumulate) added
@@ -713,7 +719,8 @@ __global__ void __launch_bounds__(256) k_fock_fp64(const int4* __restrict__ tile
                                                    const double* __restrict__ basis,
                                                    const double* __restrict__ fac_a,
                                                    const double* __restrict__ fac_b, int M,
-                                                   double* __restrict__ K_a, double* __restrict__ K_b) {
+                                                   double* __restrict__ K_a, double* __restrict__ K_b,
+                                                   long long pt_base) {
   __shared__ double As[kKStep][kTile + 1];
   __shared__ double Bs[NS][kKStep][kTile + 1];
   const int4 t = tiles[blockIdx.x];
@@ -735,8 +742,8 @@ __global__ void __launch_bounds__(256) k_fock_fp64(const int4* __restrict__ tile
       const int i = i0 + row, j = j0 + row, p = p0 + kk;
       As[kk][row] = i < G.m ? F[(long long)i * G.ldp + p] : 0.0;
       const double fj = j < G.m ? F[(long long)j * G.ldp + p] : 0.0;
-      Bs[0][kk][row] = fj * fac_a[G.pt_off + p];
-      if (NS == 2) Bs[NS - 1][kk][row] = fj * fac_b[G.pt_off + p];
+      Bs[0][kk][row] = fj * fac_a[G.pt_off - pt_base + p];
+      if (NS == 2) Bs[NS - 1][kk][row] = fj * fac_b[G.pt_off - pt_base + p];
     }
     __syncthreads();
 #pragma unroll
@@ -1448,9 +1455,11 @@ int DeviceEngine::run_kernels(bool compute_rmm, bool ext) {
       const double* P = s == 0 ? d->P_a.p : d->P_b.p;
       double* part = s == 0 ? d->part_a.p : d->part_b.p;
       if (d->lda)
-        k_density_fp64<1><<<nd, 256, 0, st>>>(d->dens_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, P, d->M, part);
+        k_density_fp64<1><<<nd, 256, 0, st>>>(d->dens_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, P, d->M, part,
+                                              0);
       else
-        k_density_fp64<4><<<nd, 256, 0, st>>>(d->dens_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, P, d->M, part);
+        k_density_fp64<4><<<nd, 256, 0, st>>>(d->dens_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, P, d->M, part,
+                                              0);
       LIO_CUDA(cudaGetLastError());
       launches++;
     }
@@ -1496,11 +1505,11 @@ int DeviceEngine::run_kernels(bool compute_rmm, bool ext) {
     } else if (d->open) {
       d->mark(4);  // no operand preparation in the FP64 form
       k_fock_fp64<2><<<nk, 256, 0, st>>>(d->fock_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, d->fac_a.p,
-                                         d->fac_b.p, d->M, Ka, Kb);
+                                         d->fac_b.p, d->M, Ka, Kb, 0);
     } else {
       d->mark(4);
       k_fock_fp64<1><<<nk, 256, 0, st>>>(d->fock_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, d->fac_a.p,
-                                         nullptr, d->M, Ka, nullptr);
+                                         nullptr, d->M, Ka, nullptr, 0);
     }
     LIO_CUDA(cudaGetLastError());
     launches++;
@@ -1528,6 +1537,7 @@ void DeviceEngine::copy_results(double* d_fock_a, double* d_fock_b, double* d_en
 
 void DeviceEngine::prepare() {
   Impl* d = impl_.get();
+  if (d->ngroups == 0) return;  // nothing to build (e.g. a shard that owns no group)
   if (precision_ == Precision::TensorCore && !d->tc_ready) {
     prepare_tensor_core();
     d->drop_graph();
@@ -1937,11 +1947,6 @@ double* noalloc_scratch_address() {
   }
   return g_noalloc_ptr[dev];
 }
-
-template <class T>
-T* shift_base(T* region, long long offset) {  // base such that base + offset == region
-  return reinterpret_cast<T*>(reinterpret_cast<uintptr_t>(region) - (uintptr_t)offset * sizeof(T));
-}
 }  // namespace
 
 size_t DeviceEngine::noalloc_scratch_bytes() { return kNoAllocScratchBytes; }
@@ -1952,7 +1957,14 @@ void DeviceEngine::solve_noalloc(const double* rho_a, const double* rho_b, doubl
   if (d->ngroups == 0) throw std::runtime_error("no grid uploaded");
   if (!rho_a || !fock_a || !energy || (d->open && (!rho_b || !fock_b)))
     throw std::runtime_error("null device pointer");
-  if (!d->basis_valid) d->compute_basis();  // allocates: only after a tensor-core solve dropped the cache
+  // The FP64 form's basis cache must be resident: building it would allocate
+  // (gigabytes at a few hundred atoms), which is what this entry point's callers
+  // cannot do. A grid built or autotuned into the tensor-core form does not keep it.
+  if (!d->basis_valid)
+    throw std::runtime_error(
+        "the no-allocation entry point needs the FP64 form's resident basis values, which this grid does not hold "
+        "(it was built or autotuned in the tensor-core form): call g2g_set_precision_(0) before "
+        "g2g_reload_atom_positions_");
   double* scratch = noalloc_scratch_address();
   cudaStream_t st = cuda_stream ? (cudaStream_t)cuda_stream : d->stream;
   const int nspin = d->open ? 2 : 1;
@@ -2000,31 +2012,31 @@ void DeviceEngine::solve_noalloc(const double* rho_a, const double* rho_b, doubl
     double* fac_a = part_b + (nspin == 2 ? part_len : 0);
     double* fac_b = fac_a + fac_len;
     double* eblk = fac_b + (nspin == 2 ? fac_len : 0);
-    double* pa = shift_base(part_a, first.part_off);
-    double* pb = shift_base(part_b, first.part_off);
-    double* fa = shift_base(fac_a, first.pt_off);
-    double* fb = shift_base(fac_b, first.pt_off);
+    // the batch's partials and factors start at the region: the kernels index
+    // them by each group's offset less the batch's first group's
+    const long long part_base = first.part_off, pt_base = first.pt_off;
     for (int s = 0; s < nspin; s++) {
       const double* P = s == 0 ? rho_a : rho_b;
       if (d->lda)
         k_density_fp64<1><<<(unsigned)nd, 256, 0, st>>>(d->dens_tiles.p + dt0, d->groups.p, d->fn_glob.p, d->basis.p,
-                                                          P, d->M, s == 0 ? pa : pb);
+                                                          P, d->M, s == 0 ? part_a : part_b, part_base);
       else
         k_density_fp64<4><<<(unsigned)nd, 256, 0, st>>>(d->dens_tiles.p + dt0, d->groups.p, d->fn_glob.p, d->basis.p,
-                                                          P, d->M, s == 0 ? pa : pb);
+                                                          P, d->M, s == 0 ? part_a : part_b, part_base);
       LIO_CUDA(cudaGetLastError());
     }
-    launch_functional(d->lda, d->open, (unsigned)nf, st, d->func_tiles.p + ft0, d->groups.p, d->pw.p, pa,
-                      d->open ? pb : nullptr, kTile, d->iexch, fa, d->open ? fb : nullptr, eblk);
+    launch_functional(d->lda, d->open, (unsigned)nf, st, d->func_tiles.p + ft0, d->groups.p, d->pw.p, part_a,
+                      d->open ? part_b : nullptr, kTile, d->iexch, fac_a, d->open ? fac_b : nullptr, eblk, part_base,
+                      pt_base);
     LIO_CUDA(cudaGetLastError());
     k_sum_blocks<<<1, 1024, 0, st>>>(eblk, (int)nf, eparts + nbatch, 0);
     LIO_CUDA(cudaGetLastError());
     if (d->open)
       k_fock_fp64<2><<<(unsigned)nk, 256, 0, st>>>(d->fock_tiles.p + kt0, d->groups.p, d->fn_glob.p, d->basis.p,
-                                                    fa, fb, d->M, fock_a, fock_b);
+                                                    fac_a, fac_b, d->M, fock_a, fock_b, pt_base);
     else
       k_fock_fp64<1><<<(unsigned)nk, 256, 0, st>>>(d->fock_tiles.p + kt0, d->groups.p, d->fn_glob.p, d->basis.p,
-                                                    fa, nullptr, d->M, fock_a, nullptr);
+                                                    fac_a, nullptr, d->M, fock_a, nullptr, pt_base);
     LIO_CUDA(cudaGetLastError());
     dt0 += nd;
     ft0 += nf;

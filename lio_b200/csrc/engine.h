@@ -98,7 +98,9 @@ class DeviceEngine {
   // (engine.cu); groups are processed in batches that fit it. Inputs: packed
   // densities in device memory (rho_b only for open shell). Outputs: packed
   // Kohn-Sham vectors in device memory, accumulated (+=); the energy (one
-  // double in device memory) is overwritten. Throws on sizes beyond the array.
+  // double in device memory) is overwritten. Throws on sizes beyond the array,
+  // and when the FP64 form's basis cache is not resident (a grid built or
+  // autotuned in the tensor-core form): rebuilding it would allocate.
   void solve_noalloc(const double* rho_a, const double* rho_b, double* fock_a, double* fock_b,
                      double* energy, void* cuda_stream);
   static size_t noalloc_scratch_bytes();
@@ -150,5 +152,12 @@ class DeviceEngine {
   std::unique_ptr<Impl> impl_;
   Precision precision_ = Precision::FP64;
 };
+
+// Self-test of the bounded waits of the pipelined tensor-core kernels (a
+// producer that stops early, one consumer wait of `polls` polls that runs out);
+// returns 1 when that wait timed out and the kernel returned (0 would mean both
+// stages arrived, 2 that even the armed stage did not), the device ms in *ms
+// and a checksum of the stage that did land (32640 for its 256 values 0..255)
+int bounded_wait_selftest(unsigned polls, double* ms, unsigned* checksum);
 
 }  // namespace lio

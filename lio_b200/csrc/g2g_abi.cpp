@@ -50,7 +50,10 @@ struct State {
   int grid_type = -1;
   Partition part;
   std::unique_ptr<lio::DeviceEngine> engine;
-  lio::Precision precision = lio::Precision::FP64;
+  // precision mode (g2g_set_precision_): 0 FP64, 1 tensor core, 2 autotuned,
+  // 3 (the default) tensor core where the grid can run it, else FP64
+  unsigned mode = 3;
+  lio::Precision precision = lio::Precision::TensorCore;  // the form of the current grid
   int status = 0;
   std::string message;
   double last_solve_ms = 0.0, last_grid_ms = 0.0;
@@ -58,7 +61,6 @@ struct State {
   bool device_ready = false;
   void* stream = nullptr;
   bool graphs = true;
-  bool auto_precision = false;
   bool device_weights = true;  // Becke weights of the grid build on the GPU when one is present
   int shard_rank = 0, shard_world = 1;  // this process's share of the groups (multi-GPU)
 };
@@ -180,6 +182,7 @@ void build_grid(unsigned grid_type) {
   if (!s.engine) s.engine.reset(new lio::DeviceEngine());
   s.engine->set_stream(s.stream);
   s.engine->set_graphs(s.graphs);
+  s.precision = s.mode == 0 ? lio::Precision::FP64 : lio::Precision::TensorCore;
   s.engine->set_precision(s.precision);
   if (s.shard_world > 1) {
     const std::vector<int> owner = shard_owners(s.part, s.shard_world);
@@ -191,7 +194,21 @@ void build_grid(unsigned grid_type) {
   }
   const double t_up = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   s.grid_phase_ms[1] = t_up - s.grid_phase_ms[0];
-  if (s.auto_precision) s.precision = s.engine->autotune();
+  if (s.mode == 2) {
+    s.precision = s.engine->autotune();
+  } else if (s.mode == 3) {
+    // the tensor-core operands are built now; a grid the form cannot run (a
+    // point group beyond the Kohn-Sham accumulators' limit, or more functions
+    // than a block's shared memory holds) gets the FP64 form instead
+    try {
+      s.engine->prepare();
+    } catch (const std::exception&) {
+      s.engine->drop_tensor_core();
+      s.precision = lio::Precision::FP64;
+      s.engine->set_precision(s.precision);
+      s.engine->prepare();
+    }
+  }
   s.device_ready = true;
   s.last_grid_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   s.grid_phase_ms[2] = s.last_grid_ms - t_up;
@@ -485,6 +502,24 @@ int g2g_solve_device_noalloc_(const double* d_rho_a, const double* d_rho_b, doub
   return rc;
 }
 
+int g2g_selftest_bounded_wait_(const unsigned* polls, double* ms) {
+  int rc = -1;
+  guarded("g2g_selftest_bounded_wait_", [&] {
+    if (!lio::DeviceEngine::available()) throw std::runtime_error("no CUDA device visible");
+    unsigned checksum = 0;
+    rc = lio::bounded_wait_selftest(*polls, ms, &checksum);
+    if (rc == 1) {
+      if (checksum != 32640u) throw std::runtime_error("bounded-wait self-test: the armed stage held wrong data");
+      fail("bounded wait timed out after " + std::to_string(*polls) +
+               " polls (self-test: the producer stopped early); the kernel returned and freed its TMEM",
+           3);
+    } else if (rc != 0) {
+      throw std::runtime_error("bounded-wait self-test: status " + std::to_string(rc));
+    }
+  });
+  return rc;
+}
+
 void g2g_deinit_(void) {
   guarded("g2g_deinit_", [] {
     State& s = st();
@@ -510,10 +545,28 @@ int g2g_last_error_(char* msg, const unsigned* len) {
 void g2g_set_precision_(const unsigned* mode) {
   guarded("g2g_set_precision_", [&] {
     State& s = st();
-    if (*mode > 2) throw std::runtime_error("precision mode must be 0 (FP64), 1 (tensor core) or 2 (autotuned)");
-    s.auto_precision = *mode == 2;
-    if (!s.auto_precision) s.precision = *mode == 1 ? lio::Precision::TensorCore : lio::Precision::FP64;
-    if (s.auto_precision && s.engine && s.device_ready) s.precision = s.engine->autotune();
+    if (*mode > 3)
+      throw std::runtime_error(
+          "precision mode must be 0 (FP64), 1 (tensor core), 2 (autotuned) or 3 (tensor core, FP64 where it cannot run)");
+    s.mode = *mode;
+    // a change applies to the current grid at once when the device holds one
+    if (s.mode == 0 || s.mode == 1) s.precision = s.mode == 1 ? lio::Precision::TensorCore : lio::Precision::FP64;
+    if (s.engine && s.device_ready) {
+      if (s.mode == 2) {
+        s.precision = s.engine->autotune();
+      } else if (s.mode == 3) {
+        s.precision = lio::Precision::TensorCore;
+        s.engine->set_precision(s.precision);
+        try {
+          s.engine->prepare();
+        } catch (const std::exception&) {
+          s.engine->drop_tensor_core();
+          s.precision = lio::Precision::FP64;
+          s.engine->set_precision(s.precision);
+          s.engine->prepare();
+        }
+      }
+    }
   });
 }
 

@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <stdexcept>
+#include <string>
 
 #include "umma.cuh"
 
@@ -66,7 +68,98 @@ __global__ void __launch_bounds__(128) k_tc_selftest(const int8_t* __restrict__ 
   if (warp == 0) umma::tmem_dealloc(tbase, ncols);
 }
 
+// The failure path of the pipelined kernels, exercised on purpose: a producer
+// that stops early. It arms stage 0 of a two-stage ring and sends that stage's
+// bulk copy, then stops without ever arming stage 1. The consumer waits for
+// both stages with the caller's poll limit: stage 0 lands, stage 1's wait runs
+// out. The consumer then does what the production kernels do after a timeout
+// (records the failure, lets every copy it issued land, frees its TMEM) and
+// the kernel returns, leaving the context usable. status: 0 both stages
+// arrived, 1 a wait ran out, 2 stage 0 itself did not arrive.
+__global__ void __launch_bounds__(64) k_wait_selftest(const uint4* __restrict__ src, uint32_t polls,
+                                                      int* __restrict__ status, uint32_t* __restrict__ checksum) {
+  __shared__ __align__(128) uint4 ring[2][64];  // two 1 KB stages
+  __shared__ uint64_t full[2];
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (warp == 0) umma::tmem_alloc(&tmem_base, 32);
+  if (tid == 0) {
+    umma::mbar_init(&full[0], 1);
+    umma::mbar_init(&full[1], 1);
+    umma::fence_mbar_init();
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tbase = tmem_base;
+  if (tid == 32) {  // producer: stage 0 only
+    umma::mbar_expect_tx(&full[0], (uint32_t)sizeof(ring[0]));
+    umma::bulk_copy_g2s(ring[0], src, (uint32_t)sizeof(ring[0]), &full[0]);
+  }
+  if (tid == 0) {  // consumer
+    int st = 0;
+    if (!umma::mbar_wait(&full[0], 0, polls)) {
+      st = 2;
+    } else {
+      uint32_t sum = 0;
+      for (int i = 0; i < 64; i++) sum += ring[0][i].x + ring[0][i].y + ring[0][i].z + ring[0][i].w;
+      *checksum = sum;
+      if (!umma::mbar_wait(&full[1], 0, polls)) st = 1;  // never armed: runs out
+    }
+    // the one copy issued lands before the CTA exits (the production limit,
+    // not the caller's: a 1 KB copy takes microseconds)
+    if (st == 2) umma::mbar_wait(&full[0], 0);
+    *status = st;
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tbase, 32);
+}
+
 }  // namespace
+
+// Runs k_wait_selftest (one CTA) and returns its status; `ms` gets the
+// kernel's device time (CUDA events). Throws on a CUDA error.
+int bounded_wait_selftest(unsigned polls, double* ms, unsigned* checksum) {
+  uint4* src = nullptr;
+  int* dst = nullptr;
+  int status = -1;
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaError_t e = cudaMalloc(&src, 64 * sizeof(uint4));
+  if (e == cudaSuccess) e = cudaMalloc(&dst, 2 * sizeof(int));
+  if (e == cudaSuccess) {
+    uint4 h[64];
+    for (int i = 0; i < 64; i++) h[i] = make_uint4(4 * i, 4 * i + 1, 4 * i + 2, 4 * i + 3);
+    e = cudaMemcpy(src, h, sizeof(h), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess) e = cudaMemset(dst, 0xff, 2 * sizeof(int));
+  if (e == cudaSuccess) e = cudaEventCreate(&a);
+  if (e == cudaSuccess) e = cudaEventCreate(&b);
+  if (e == cudaSuccess) {
+    cudaEventRecord(a);
+    k_wait_selftest<<<1, 64>>>(src, polls, dst, reinterpret_cast<uint32_t*>(dst + 1));
+    e = cudaGetLastError();
+    cudaEventRecord(b);
+  }
+  if (e == cudaSuccess) e = cudaEventSynchronize(b);
+  int h[2] = {-1, 0};
+  if (e == cudaSuccess) e = cudaMemcpy(h, dst, sizeof(h), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) {
+    float f = 0.f;
+    cudaEventElapsedTime(&f, a, b);
+    if (ms) *ms = f;
+    if (checksum) *checksum = (unsigned)h[1];
+    status = h[0];
+  }
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  cudaFree(src);
+  cudaFree(dst);
+  if (e != cudaSuccess) throw std::runtime_error(std::string("CUDA error in the bounded-wait self-test: ") +
+                                                 cudaGetErrorString(e));
+  return status;
+}
+
 }  // namespace lio
 
 extern "C" __attribute__((visibility("default"))) int lio_tc_selftest_(int N, int K, const int8_t* hA,

@@ -66,10 +66,11 @@ __device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
 }
 
-// bounded wait for the phase with the given parity; returns false on timeout
-__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity) {
+// bounded wait for the phase with the given parity; returns false once
+// `limit` polls have not seen it
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint32_t limit = kSpinLimit) {
   const uint32_t a = smem_u32(mbar);
-  for (uint32_t i = 0; i < kSpinLimit; i++) {
+  for (uint32_t i = 0; i < limit; i++) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred P;\n\t"

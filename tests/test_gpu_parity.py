@@ -98,3 +98,36 @@ def test_grid_types_0_1_match_reference(grid_type, precision):
     assert abs(E - E_ref) <= H.E_TOL, (E, E_ref)
     assert np.max(np.abs(K - K_ref)) <= H.K_TOL
     assert np.max(np.abs(Kb - Kb_ref)) <= H.K_TOL
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("grid_type", [0, 1, 2])
+def test_lio_tables_match_reference(grid_type, precision):
+    """Builds on lioamber's own angular tables (lioamber/grid.f90:39-476, as
+    tests/golden/make_lio_tables.py evaluates them), grid types 0, 1, 2."""
+    from .test_partition import lio_tables
+
+    wl = W.small_workload(12, 29, 9, True)
+    tables = lio_tables()
+
+    def build(path, product):
+        L = H.lib(path, product)
+        if not product:
+            L.init()
+        L.set_options(eai=True)
+        L.bind_workload(wl, tables)
+        if product:
+            L.set_precision(precision)
+        msg = L.reload_atom_positions(grid_type)
+        assert not msg, msg
+        E = L.solve_groups(0)
+        out = (E, L.fock.copy(), L.fockb.copy())
+        if not product:
+            L.deinit()
+        return out
+
+    E_ref, K_ref, Kb_ref = build(H.REF_LIB, False)
+    E, K, Kb = build(H.os.path.join(H.ROOT, "lio_b200", "libg2g_b200.so"), True)
+    assert abs(E - E_ref) <= H.E_TOL, (E, E_ref)
+    assert np.max(np.abs(K - K_ref)) <= H.K_TOL
+    assert np.max(np.abs(Kb - Kb_ref)) <= H.K_TOL

@@ -101,3 +101,39 @@ def test_partition_bit_exact_vs_reference_grid_types_0_1(grid_type):
     prod, ref = groups(PROD, True), groups(H.REF_LIB, False)
     assert_same(prod, ref)
     assert len(prod) > 0
+
+
+def lio_tables():
+    """lioamber's own angular tables for grid types 0, 1, 2 (50, 116, 194
+    directions), evaluated from lioamber/grid.f90:39-476 by
+    tests/golden/make_lio_tables.py."""
+    g = np.load(os.path.join(GOLD, "lio_angular_tables.npz"))
+    return {t: (np.asfortranarray(g[f"e{t}"]), np.ascontiguousarray(g[f"w{t}"])) for t in (0, 1, 2)}
+
+
+@pytest.mark.skipif(not os.path.exists(H.REF_LIB), reason="reference build absent")
+@pytest.mark.parametrize("grid_type", [0, 1, 2])
+def test_partition_bit_exact_vs_reference_lio_tables(grid_type):
+    """The tables lioamber actually passes (not this project's solved Lebedev
+    grids), through g2g_parameter_init_ to both libraries."""
+    wl = W.small_workload(12, 29, 9, True)
+    tables = lio_tables()
+
+    def groups(path, product):
+        L = H.lib(path, product)
+        if not product:
+            L.init()
+        L.set_options(eai=True)
+        L.bind_workload(wl, tables)
+        L.reload_atom_positions(grid_type)
+        out = {}
+        for g in range(L.num_groups(ref=not product)):
+            d = L.partition_group(g, ref=not product)
+            out[tuple(sorted(map(tuple, d["ids"].tolist())))] = d
+        if not product:
+            L.deinit()
+        return out
+
+    prod, ref = groups(PROD, True), groups(H.REF_LIB, False)
+    assert len(prod) > 0
+    assert_same(prod, ref)
