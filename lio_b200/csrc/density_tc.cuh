@@ -20,11 +20,23 @@
 // lands on level s + t: S MMAs per K step and kind instead of S(S+1)/2 narrow
 // ones (an MMA costs about the same for every N up to 64 on this part).
 //
-// The row-dot epilogue needs F, dF and d2F at (p, i) in FP64. They come from a
-// blocked copy of the basis cache (per 128-point tile, 32-function tile and
-// kind one contiguous 32 KB chunk) that a dedicated warp streams into a
-// shared-memory ring with bulk copies, so the epilogue does no global loads.
+// The row-dot epilogue needs F, dF and d2F at (p, i) in FP64. They are not
+// streamed from HBM (80 bytes per point and function, three quarters of the
+// kernel's traffic before). Each value is P(r) R(r): a Cartesian monomial of the
+// point's displacement from the function's atom times the shell's contracted
+// radial part, whose sums t, tg, th (the only exponentials) are computed once per
+// geometry (k_radial, 24 bytes per point and shell). The epilogue contracts G
+// shell by shell in factored form: with S0 = sum_c P_c G_c, S1_a = sum_c
+// dP_c/da G_c and S2_ab = sum_c d2P_c/da db G_c over the shell's components,
+//   sum_c F_c G_c        = t S0
+//   sum_c dF_c/da G_c    = t S1_a + r_a tg2 S0
+//   sum_c d2F_c/dadb G_c = t S2_ab + tg2 (r_b S1_a + r_a S1_b + delta_ab S0) + th4 r_a r_b S0
+// (tg2 = -2 tg, th4 = 4 th; the closed forms of g2g/cpu/functions.cpp:81-352
+// summed over a shell): a few FP64 operations per function instead of ten
+// values and their row dots.
 #pragma once
+#include <type_traits>
+
 #include "umma.cuh"
 
 constexpr int kSlices = 6;       // Ozaki slices per operand
@@ -41,30 +53,42 @@ constexpr int kTcChunk = kTcFuncs * kTcPoints;  // doubles of one blocked basis 
 // KP = kinds per unit: all NS x KP x S x 32 level columns of a unit fit in 384
 // TMEM columns. Open shell: one kind per unit (F, x, y, z); closed shell GGA:
 // {F, dF/dx} then {dF/dy, dF/dz}; LDA: {F}.
+constexpr int kTcMaxWarpShells = 16;  // shells an epilogue warp's 16 columns touch, at most
 template <bool GGA, int NS>
 struct TcCfg {
   static constexpr int KP = (GGA && NS == 1) ? 2 : 1;
   static constexpr int NA = GGA ? 4 : 1;   // kinds of the contraction
-  static constexpr int NK = GGA ? 10 : 1;  // kinds of the FP64 basis (F; dF; d2F)
   static constexpr int NP = NA / KP;       // units per function tile
   static constexpr int NQ = GGA ? 10 : 1;
+  static constexpr int NR = GGA ? 3 : 1;   // radial sums per (shell, point): t (LDA); t, -2 tg, 4 th (GGA)
   static constexpr int kStageA = KP * kTcStepA;
   static constexpr int kStage = kStageA + NS * kTcStepD;
   static constexpr uint32_t kCols = NS * KP * kSlices * kTcFuncs;
-  static constexpr uint32_t kTmem = kCols <= 256 ? 256 : 512;
-  // epilogue warps, operand producer, MMA issuer, basis producer
-  static constexpr int kWarps = kTcEpiWarps + 3;
+  // after the level columns, the unit's G in FP64: per function column c the
+  // NS x KP values, two 32-bit TMEM columns each (column kCols + c * kGPer + ...)
+  static constexpr uint32_t kGPer = 2 * NS * KP;
+  static constexpr uint32_t kTmemUsed = kCols + kTcFuncs * kGPer;
+  static constexpr uint32_t kTmem = kTmemUsed <= 256 ? 256 : 512;
+  static_assert(kTmemUsed <= 512, "levels and G fit the 512 TMEM columns");
+  // epilogue warps, operand producer, MMA issuer
+  static constexpr int kWarps = kTcEpiWarps + 2;
   static constexpr int kThreads = 32 * kWarps;
-  static constexpr int kProd = kTcEpiWarps, kMma = kTcEpiWarps + 1, kBasisProd = kTcEpiWarps + 2;
-  // dynamic shared memory: operand ring | basis ring | column-group reduction | function table
+  static constexpr int kProd = kTcEpiWarps, kMma = kTcEpiWarps + 1;
+  // dynamic shared memory: operand ring | radial sums (per epilogue warp: up to
+  // 16 shells x NR values x 32 points, each thread's own) | per-group
+  // density-tile scales. At the end of a tile each warp of column group 1 hands
+  // its points' sums to column group 0 through its own radial area, which it
+  // no longer reads by then. Two operand stages: a third (room for it only in
+  // the open-shell form) measured slower at 256 atoms, 7.23 against 7.01 ms.
+  static constexpr size_t kWarpRad = (size_t)kTcMaxWarpShells * NR * 32 * 8;
+  static constexpr size_t kRadBytes = (size_t)kTcEpiWarps * kWarpRad;
+  static constexpr size_t kRedBytes = (size_t)NS * 32 * NQ * 8;  // per warp: [spin][lane][NQ] FP64
+  static_assert(kRedBytes <= kWarpRad, "a warp's sums fit its radial area");
   static constexpr int kStages = 2;
-  static constexpr int kBStages = 3;
   static constexpr size_t kRing = (size_t)kStages * kStage;
-  static constexpr size_t kBRing = kRing;
-  static constexpr size_t kRed = kBRing + (size_t)kBStages * kTcChunk * 8;
-  static constexpr size_t kRedBytes = (size_t)NS * kTcPoints * NQ * 8;  // [spin][point][NQ] FP64
-  static constexpr size_t kTab = kRed + kRedBytes;
-  static constexpr size_t kTabEntry = NS * 8;  // 2^f_i per spin
+  static constexpr size_t kRad = kRing;
+  static constexpr size_t kTab = kRad + kRadBytes;
+  static constexpr size_t kTabEntry = NS * 8;  // 2^f_T per function, per spin
   static size_t smem(int cap) { return kTab + (size_t)cap * kTabEntry; }
 };
 
@@ -262,65 +286,188 @@ __device__ __forceinline__ bool epi_sync_or(bool pred) {
   return out != 0;
 }
 
-// Whether a later unit of the same function tile reads chunk k again (the dF/dy,
-// dF/dz chunks after the F or x unit, dF/dx after F when x is a unit of its own):
-// those are kept in L2, last uses are evicted first.
-__device__ __forceinline__ bool chunk_reused(int first, int k, int KP) {
-  if (k < 1 || k > 3) return false;
-  const int next = first + KP;  // first kind of the next unit
-  return next <= 3 && k >= next;
+// ------------------------------------------------------------- radial sums
+// Per geometry: one thread per (group, point) of a 128-point tile; for every
+// shell (simple function) of the group the contracted radial sums at the point
+// (g2g/cpu/functions.cpp:68-79: primitives with a_k r^2 > 70 skipped),
+//   t = sum_k c_k e^(-a_k r^2),  tg2 = -2 sum_k a_k c_k e^(..),  th4 = 4 sum_k a_k^2 c_k e^(..)
+// (t only for LDA, NR = 1). Layout per group and tile: [shell][NR][128 points],
+// so the shells of one function tile are contiguous.
+template <int NR>
+__global__ void __launch_bounds__(kTcPoints) k_radial(const int2* __restrict__ tiles,
+                                                      const GroupDev* __restrict__ groups,
+                                                      const double* __restrict__ px, const double* __restrict__ py,
+                                                      const double* __restrict__ pz, const int* __restrict__ sf_glob,
+                                                      const int* __restrict__ nuc, const int* __restrict__ ncont,
+                                                      const double* __restrict__ ca, const double* __restrict__ cc,
+                                                      const double* __restrict__ ax, const double* __restrict__ ay,
+                                                      const double* __restrict__ az, double* __restrict__ rad) {
+  const int2 t = tiles[blockIdx.x];
+  const GroupDev G = groups[t.x];
+  const int r = threadIdx.x;
+  const long long p = G.pt_off + t.y * kTcPoints + r;
+  const double x = px[p], y = py[p], z = pz[p];
+  double* out = rad + G.rad_off + (long long)t.y * G.nsimple * NR * kTcPoints + r;
+  for (int sh = 0; sh < G.nsimple; sh++) {
+    const int gf = sf_glob[G.sf_off + sh];
+    const int atom = nuc[gf];
+    const double dx = x - ax[atom], dy = y - ay[atom], dz = z - az[atom];
+    const double dist = dx * dx + dy * dy + dz * dz;
+    double tt = 0.0, tg = 0.0, th = 0.0;
+    const int nc = ncont[gf];
+    for (int k = 0; k < nc; k++) {
+      const double a = ca[gf * 13 + k], c = cc[gf * 13 + k];
+      const double expo = a * dist;
+      if (expo > 70.0) continue;
+      const double t0 = exp(-expo) * c;
+      tt += t0;
+      tg += t0 * a;
+      th += t0 * (a * a);
+    }
+    out[(long long)sh * NR * kTcPoints] = tt;
+    if (NR == 3) {
+      out[((long long)sh * NR + 1) * kTcPoints] = -2.0 * tg;
+      out[((long long)sh * NR + 2) * kTcPoints] = 4.0 * th;
+    }
+  }
 }
 
-// FP64 basis kinds whose chunks a unit with first contraction kind `first`
-// consumes, in order: F unit: all NK; x: dF/dx..dF/dz; y: dF/dy, dF/dz; z: dF/dz.
-__host__ __device__ __forceinline__ int unit_klo(int first) { return first == 0 ? 0 : first; }
-__host__ __device__ __forceinline__ int unit_khi(int first, int NK) { return first == 0 ? NK - 1 : 3; }
-
-// Adds the row dots of basis-kind chunk k, d[sp][kp] = sum_i v_ki G^(kp)_i over
-// this warp's columns, to the point's q = (rho; grad rho; d2rho xx, yy, zz, xy,
-// xz, yz) per spin:
-//   unit F : k = F: rho += d;  k = dF_a: grad_a += 2 d;  k = d2F_ab: d2_ab += 2 d
-//            with KP = 2 also G^x: xx += 2 d(Fx), xy += 2 d(Fy), xz += 2 d(Fz)
-//   unit x : xx += 2 d(Fx), xy += 2 d(Fy), xz += 2 d(Fz)   (Fy Gx = Fx Gy: D is symmetric)
-//   unit y : yy += 2 d(Fy), yz += 2 d(Fz)   (with KP = 2 also zz += 2 d(Fz) of G^z)
-//   unit z : zz += 2 d(Fz)
-template <bool GGA, int NS, int NQ, int KP>
-__device__ __forceinline__ void apply_chunk(int first, int k, const double (&d)[NS][KP], double (&q)[NS][NQ]) {
-#pragma unroll
-  for (int sp = 0; sp < NS; sp++) {
-    if (!GGA) {
-      q[sp][0] += d[sp][0];
-      continue;
-    }
-    const double d0 = 2.0 * d[sp][0], d1 = 2.0 * d[sp][KP - 1];
-    if (first == 0) {
-      // kinds F, dF/dx, dF/dy, dF/dz, d2F xx .. yz map onto q[0 .. 9] in order
-      switch (k) {
-        case 0: q[sp][0] += d[sp][0]; break;
-        case 1: q[sp][1 % NQ] += d0; if (KP == 2) q[sp][4 % NQ] += d1; break;
-        case 2: q[sp][2 % NQ] += d0; if (KP == 2) q[sp][7 % NQ] += d1; break;
-        case 3: q[sp][3 % NQ] += d0; if (KP == 2) q[sp][8 % NQ] += d1; break;
-        case 4: q[sp][4 % NQ] += d0; break;
-        case 5: q[sp][5 % NQ] += d0; break;
-        case 6: q[sp][6 % NQ] += d0; break;
-        case 7: q[sp][7 % NQ] += d0; break;
-        case 8: q[sp][8 % NQ] += d0; break;
-        default: q[sp][9 % NQ] += d0; break;
-      }
-    } else if (first == 1) {
-      if (k == 1) q[sp][4 % NQ] += d0;
-      else if (k == 2) q[sp][7 % NQ] += d0;
-      else q[sp][8 % NQ] += d0;
-    } else if (first == 2) {
-      if (k == 2) {
-        q[sp][5 % NQ] += d0;
-      } else {
-        q[sp][9 % NQ] += d0;
-        if (KP == 2) q[sp][6 % NQ] += d1;
-      }
+// ------------------------------------------------ one shell's contribution
+// Monomial sums of one shell for one (spin, kind) from its components' G values
+// g[c] (0 for components outside this warp's columns): S0 = sum_c P_c g_c,
+// S1[a] = sum_c dP_c/da g_c, S2 = sum_c d2P_c/da db g_c in the order xx, yy,
+// zz, xy, xz, yz. TYPE 0 s (P = 1), 1 p (P = x, y, z), 2 d (P = xx, xy, yy,
+// xz, yz, zz with xx, yy, zz times the normalisation n).
+template <int TYPE>
+struct ShellSums {
+  double S0, S1[3], S2[6];
+  __device__ __forceinline__ ShellSums(const double* g, const double (&r)[3], double n) {
+    if constexpr (TYPE == 0) {
+      S0 = g[0];
+    } else if constexpr (TYPE == 1) {
+      S0 = fma(r[0], g[0], fma(r[1], g[1], r[2] * g[2]));
+      S1[0] = g[0];
+      S1[1] = g[1];
+      S1[2] = g[2];
     } else {
-      q[sp][6 % NQ] += d0;
+      const double gxx = n * g[0], gxy = g[1], gyy = n * g[2], gxz = g[3], gyz = g[4], gzz = n * g[5];
+      const double x = r[0], y = r[1], z = r[2];
+      S0 = fma(x * x, gxx, fma(y * y, gyy, fma(z * z, gzz, fma(x * y, gxy, fma(x * z, gxz, (y * z) * gyz)))));
+      S1[0] = fma(2.0 * x, gxx, fma(y, gxy, z * gxz));
+      S1[1] = fma(2.0 * y, gyy, fma(x, gxy, z * gyz));
+      S1[2] = fma(2.0 * z, gzz, fma(x, gxz, y * gyz));
+      S2[0] = 2.0 * gxx;
+      S2[1] = 2.0 * gyy;
+      S2[2] = 2.0 * gzz;
+      S2[3] = gxy;
+      S2[4] = gxz;
+      S2[5] = gyz;
     }
+  }
+};
+
+// A shell at this thread's point: displacement from its atom and radial sums.
+struct ShellPoint {
+  double r[3], t, tg2, th4;
+};
+
+// Adds a shell's contribution of kind KIND (0 F, 1 dF/dx, 2 dF/dy, 3 dF/dz of
+// the unit's G) to the point's q = (rho; grad rho; d2rho xx, yy, zz, xy, xz, yz);
+// the factor 2 of every derivative term is applied once when q is written:
+//   F : rho += t S0, grad_a += t S1_a + r_a tg2 S0,
+//       d2_ab += t S2_ab + tg2 (r_b S1_a + r_a S1_b + delta_ab S0) + r_a r_b th4 S0
+//   x : xx, xy, xz += t S1_(x, y, z) + r_(x, y, z) tg2 S0   (F_y G^x = F_x G^y: D is symmetric)
+//   y : yy, yz += t S1_(y, z) + r_(y, z) tg2 S0
+//   z : zz += t S1_z + r_z tg2 S0
+template <int TYPE, int KIND, bool GGA, int NQ>
+__device__ __forceinline__ void shell_finish(const ShellSums<TYPE>& S, const ShellPoint& sp, double (&q)[NQ]) {
+  if constexpr (!GGA) {
+    q[0] = fma(sp.t, S.S0, q[0]);
+  } else if constexpr (KIND == 0) {
+    q[0] = fma(sp.t, S.S0, q[0]);
+    const double tg0 = sp.tg2 * S.S0, th0 = sp.th4 * S.S0;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      double v = sp.r[a] * tg0;
+      if constexpr (TYPE > 0) v = fma(sp.t, S.S1[a], v);
+      q[(1 + a) % NQ] += v;
+    }
+#pragma unroll
+    for (int h = 0; h < 6; h++) {
+      constexpr int ha[6] = {0, 1, 2, 0, 0, 1}, hb[6] = {0, 1, 2, 1, 2, 2};
+      const int a = ha[h], b = hb[h];
+      double v = (sp.r[a] * sp.r[b]) * th0;     // r_a r_b th4 S0
+      if (h < 3) v += tg0;                      // delta_ab tg2 S0
+      if constexpr (TYPE > 0) v = fma(sp.tg2, fma(sp.r[b], S.S1[a], sp.r[a] * S.S1[b]), v);
+      if constexpr (TYPE == 2) v = fma(sp.t, S.S2[h], v);
+      q[(4 + h) % NQ] += v;
+    }
+  } else {
+    // gradient kinds: rows xx, xy, xz (x); yy, yz (y); zz (z)
+    constexpr int na = KIND == 1 ? 3 : (KIND == 2 ? 2 : 1);
+    constexpr int qa[3][3] = {{4, 7, 8}, {5, 9, 0}, {6, 0, 0}};
+    const double tg0 = sp.tg2 * S.S0;
+#pragma unroll
+    for (int j = 0; j < na; j++) {
+      const int a = KIND - 1 + j;  // dF/da dotted with G^KIND
+      double v = sp.r[a] * tg0;
+      if constexpr (TYPE > 0) v = fma(sp.t, S.S1[a], v);
+      q[qa[KIND - 1][j] % NQ] += v;
+    }
+  }
+}
+
+// One shell of this warp's columns for the current unit: its components' G
+// (NS x KP doubles per column, parked in TMEM at gbase + column * GPER by the
+// unit's read-out; columns outside [0, wlen) belong to another warp or function
+// tile and count as 0), the monomial sums per (spin, kind) and their finishing
+// step. `pass` selects the unit's first kind (F, x, y, z in units of KP).
+template <int TYPE, bool GGA, int NS, int KP, int NQ, int GPER>
+__device__ __forceinline__ void shell_unit(int pass, uint32_t gbase, int fcol, int wlen, const ShellPoint& spt,
+                                           double dnorm, double (&q)[NS][NQ]) {
+  constexpr int NC = TYPE == 0 ? 1 : (TYPE == 1 ? 3 : 6);
+  uint32_t raw[NC][4];
+#pragma unroll
+  for (int c = 0; c < NC; c++) {
+    const int col = fcol + c;
+    if (col >= 0 && col < wlen) {  // warp-uniform
+      if constexpr (GPER == 4)
+        lio::umma::tmem_ld4u(gbase + (uint32_t)(col * GPER), raw[c][0], raw[c][1], raw[c][2], raw[c][3]);
+      else
+        lio::umma::tmem_ld2(gbase + (uint32_t)(col * GPER), raw[c][0], raw[c][1]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; k++) raw[c][k] = 0u;  // the bits of +0.0
+    }
+  }
+  lio::umma::tmem_wait_ld();
+  auto run = [&](auto first_tag) {
+    constexpr int FIRST = decltype(first_tag)::value;
+#pragma unroll
+    for (int kp = 0; kp < KP; kp++)
+#pragma unroll
+      for (int sp = 0; sp < NS; sp++) {
+        const int sk = sp * KP + kp;
+        double g[NC];
+#pragma unroll
+        for (int c = 0; c < NC; c++) g[c] = __hiloint2double((int)raw[c][2 * sk + 1], (int)raw[c][2 * sk]);
+        const ShellSums<TYPE> S(g, spt.r, dnorm);
+        if (kp == 0)
+          shell_finish<TYPE, FIRST, GGA, NQ>(S, spt, q[sp]);
+        else
+          shell_finish<TYPE, (FIRST + 1 < 4 ? FIRST + 1 : 3), GGA, NQ>(S, spt, q[sp]);
+      }
+  };
+  if constexpr (!GGA) {
+    run(std::integral_constant<int, 0>{});
+  } else if constexpr (KP == 2) {
+    if (pass == 0) run(std::integral_constant<int, 0>{});  // F and x
+    else run(std::integral_constant<int, 2>{});            // y and z
+  } else {
+    if (pass == 0) run(std::integral_constant<int, 0>{});
+    else if (pass == 1) run(std::integral_constant<int, 1>{});
+    else if (pass == 2) run(std::integral_constant<int, 2>{});
+    else run(std::integral_constant<int, 3>{});
   }
 }
 
@@ -334,30 +481,34 @@ __device__ __forceinline__ void apply_chunk(int first, int k, const double (&d)[
 //               the unit's A slices (KP x kTcStepA) and every spin's stacked D
 //               slices (kTcStepD), one bulk copy each;
 //   warp 9      MMA issuer: per stage NS x KP x S MMAs into the unit's
-//               NS x KP x S x 32 level columns in TMEM;
-//   warp 10     basis producer: per unit the FP64 basis chunks its row dots
-//               need (unit_klo .. unit_khi), one 32 KB bulk copy each, into a
-//               three-slot ring.
-// The epilogue reads the unit's levels (tfull), forms G in FP64 in registers,
-// hands TMEM back (tempty) so the next unit's MMAs overlap its row dots, and
-// consumes the basis chunks from shared memory. Every wait is bounded; a
-// timeout sets `fail`, which the other roles poll, and the kernel drains its
-// copies and MMAs before it frees TMEM and reports the error.
+//               NS x KP x S x 32 level columns in TMEM.
+// Per 32-function tile each epilogue warp copies the radial sums of the shells
+// its 16 columns touch (at its own points) into its part of shared memory
+// while the tile's first unit runs. Per unit it reads the levels (tfull),
+// forms G in FP64 and parks it in the TMEM columns after the levels, hands the
+// level columns back (tempty) so the next unit's MMAs overlap its work, and
+// contracts G shell by shell. The warps of a tile meet only at its start and
+// end. Every wait is bounded; a timeout sets `fail`, which the other roles poll,
+// and the kernel drains its copies and MMAs before it frees TMEM and reports
+// the error.
 template <bool GGA, int NS>
 __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
     k_density_tc(const int2* __restrict__ tiles, int ntiles, const GroupDev* __restrict__ groups,
                  const int8_t* __restrict__ aslices, const int16_t* __restrict__ aexp,
                  const int8_t* __restrict__ dsl_a, const int16_t* __restrict__ dexp_a,
-                 const int8_t* __restrict__ dsl_b, const int16_t* __restrict__ dexp_b,
-                 const double* __restrict__ bblk, int fcap, double* __restrict__ part_a,
-                 double* __restrict__ part_b, int* __restrict__ err) {
+                 const int8_t* __restrict__ dsl_b, const int16_t* __restrict__ dexp_b, int fcap,
+                 const double* __restrict__ px, const double* __restrict__ py, const double* __restrict__ pz,
+                 const int* __restrict__ fn_sh, const int* __restrict__ sf_glob, const int* __restrict__ sf_type,
+                 const int* __restrict__ sf_fn, const int* __restrict__ nuc, const double* __restrict__ ax,
+                 const double* __restrict__ ay, const double* __restrict__ az, const double* __restrict__ rad,
+                 double dnorm, double* __restrict__ part_a, double* __restrict__ part_b, int* __restrict__ err) {
   using Cfg = TcCfg<GGA, NS>;
-  constexpr int KP = Cfg::KP, NP = Cfg::NP, NA = Cfg::NA, NK = Cfg::NK, NQ = Cfg::NQ, CPW = kTcCpw;
-  constexpr int kStages = Cfg::kStages, kBStages = Cfg::kBStages;
+  constexpr int KP = Cfg::KP, NP = Cfg::NP, NA = Cfg::NA, NQ = Cfg::NQ, NR = Cfg::NR, CPW = kTcCpw;
+  constexpr int kStages = Cfg::kStages;
   extern __shared__ __align__(128) uint8_t tc_smem[];
-  __shared__ uint64_t full[kStages], empty[kStages], bfull[kBStages], bempty[kBStages], tfull, tempty, drain;
+  __shared__ uint64_t full[kStages], empty[kStages], tfull, tempty, drain;
   __shared__ uint32_t tmem_base;
-  __shared__ int fail, consumed, bconsumed;
+  __shared__ int fail, consumed;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (warp == 0) lio::umma::tmem_alloc(&tmem_base, Cfg::kTmem);
   if (tid == 0) {
@@ -365,32 +516,19 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
       lio::umma::mbar_init(&full[b], 1);
       lio::umma::mbar_init(&empty[b], 1);
     }
-    for (int b = 0; b < kBStages; b++) {
-      lio::umma::mbar_init(&bfull[b], 1);
-      lio::umma::mbar_init(&bempty[b], kTcEpiWarps);
-    }
     lio::umma::mbar_init(&tfull, 1);
     lio::umma::mbar_init(&tempty, kTcEpiWarps);
     lio::umma::mbar_init(&drain, 1);
     lio::umma::fence_mbar_init();
     fail = 0;
     consumed = 0;
-    bconsumed = 0;
-  }
-  {
-    // The basis ring starts zeroed: a chunk of a group's last function tile is
-    // copied for its m - 32 ft valid functions only, and the rows after them
-    // keep the finite values of earlier chunks, which meet G = 0 in the dots.
-    double* ring = reinterpret_cast<double*>(tc_smem + Cfg::kBRing);
-    for (int i = tid; i < kBStages * kTcChunk; i += blockDim.x) ring[i] = 0.0;
-    lio::umma::fence_proxy_async_smem();
   }
   lio::umma::fence_before_sync();
   __syncthreads();
   lio::umma::fence_after_sync();
   const uint32_t tbase = tmem_base;
   volatile int* vfail = &fail;
-  int issued = 0;  // producers: stages / chunks issued
+  int issued = 0;  // producer: stages issued
 
   if (warp == Cfg::kProd) {
     // ------------------------------------------------------------ operand producer
@@ -423,35 +561,6 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
                   stage + Cfg::kStageA + sp * kTcStepD,
                   (sp == 0 ? dsl_a : dsl_b) + G.ds_off + ((long long)ft * nks + kk) * kTcStepD, kTcStepD, &full[buf],
                   keep);
-            issued = cnt + 1;
-          }
-        }
-      }
-    }
-  } else if (warp == Cfg::kBasisProd) {
-    // ------------------------------------------------------------ basis producer
-    if (lane == 0) {
-      const uint64_t keep = lio::umma::l2_evict_last(), drop = lio::umma::l2_evict_first();
-      int cnt = 0;
-      for (int w = blockIdx.x; w < ntiles && !*vfail; w += gridDim.x) {
-        const int2 t = tiles[w];
-        const GroupDev& G = groups[t.x];
-        const int nft = G.nftc;
-        for (int tt = 0; tt < nft * NP && !*vfail; tt++) {
-          const int ft = tt / NP, first = (tt - ft * NP) * KP;
-          const double* src = bblk + G.bb_off + (long long)(t.y * nft + ft) * NK * kTcChunk;
-          // rows (functions) of the chunk that exist: 1 KB each, contiguous from row 0
-          const uint32_t bytes = (uint32_t)min(kTcFuncs, G.m - ft * kTcFuncs) * kTcPoints * 8;
-          for (int k = unit_klo(first); k <= unit_khi(first, NK); k++, cnt++) {
-            const int buf = cnt % kBStages, use = cnt / kBStages;
-            if (use > 0 && (*vfail || !lio::umma::mbar_wait(&bempty[buf], (use - 1) & 1))) {
-              *vfail = 1;
-              break;
-            }
-            lio::umma::mbar_expect_tx(&bfull[buf], bytes);
-            lio::umma::bulk_copy_g2s_hint(tc_smem + Cfg::kBRing + (size_t)buf * kTcChunk * 8,
-                                          src + (long long)k * kTcChunk, bytes, &bfull[buf],
-                                          chunk_reused(first, k, KP) ? keep : drop);
             issued = cnt + 1;
           }
         }
@@ -510,19 +619,22 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
   } else {
     // ------------------------------------------------------------ epilogue
     const int quad = warp & 3, colg = warp >> 2;
-    const int row = quad * 32 + lane;
-    const int etid = tid;  // 0 .. 255
+    const int row = quad * 32 + lane;  // this thread's point of the tile
+    const int etid = tid;              // 0 .. 255
     const uint32_t lane_base = tbase + ((uint32_t)(quad * 32) << 16);
-    const double* bring = reinterpret_cast<const double*>(tc_smem + Cfg::kBRing);
-    double* red = reinterpret_cast<double*>(tc_smem + Cfg::kRed);
+    // this warp's radial sums, [shell][NR][lane]: every thread reads only its own values
+    double* wrad = reinterpret_cast<double*>(tc_smem + Cfg::kRad + (size_t)warp * Cfg::kWarpRad) + lane;
+    const uint32_t wrad_s = lio::umma::smem_u32(wrad);
+    // column group 1 -> 0 hand-off at the end of a tile: warp 4 + quad's radial area, [spin][lane][NQ]
+    double* red = reinterpret_cast<double*>(tc_smem + Cfg::kRad + (size_t)(4 + quad) * Cfg::kWarpRad);
     double* tsa = reinterpret_cast<double*>(tc_smem + Cfg::kTab);  // 2^f_T per function, spin a
     double* tsb = tsa + fcap;                                        // spin b (NS = 2 only)
     bool lfail = false;
-    int ucnt = 0, bcnt = 0;
+    int ucnt = 0;
     for (int w = blockIdx.x; w < ntiles; w += gridDim.x) {
       const int2 t = tiles[w];
       const GroupDev& G = groups[t.x];
-      const int m = G.m, ldp = G.ldp, nft = G.nftc, ntt = nft * NP;
+      const int m = G.m, ldp = G.ldp, nft = G.nftc;
       const int p = t.y * kTcPoints + row;
       // per-function scales of this group (the previous tile's readers are past the last barrier)
       const int mt = nft * kTcFuncs;  // <= fcap: fcap covers the largest padded m
@@ -530,91 +642,122 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
         tsa[i] = i < m ? pow2(dexp_a[G.dexp_off + i]) : 0.0;
         if (NS == 2) tsb[i] = i < m ? pow2(dexp_b[G.dexp_off + i]) : 0.0;
       }
-      epi_sync_or(false);
       double spx[NA];  // 2^(point exponent - 7(S+1)) per kind
 #pragma unroll
       for (int a = 0; a < NA; a++) spx[a] = pow2(aexp[G.aexp_off + (long long)a * ldp + p] - 7 * (kSlices + 1));
+      const double xp = px[G.pt_off + p], yp = py[G.pt_off + p], zp = pz[G.pt_off + p];
       double q[NS][NQ];
 #pragma unroll
       for (int sp = 0; sp < NS; sp++)
 #pragma unroll
         for (int k = 0; k < NQ; k++) q[sp][k] = 0.0;
       const bool narrow = G.m32 <= kTcNarrowK;
-      for (int tt = 0; tt < ntt; tt++, ucnt++) {
-        const int ft = tt / NP, pass = tt - ft * NP, first = pass * KP;
-        const int cb = ft * kTcFuncs + colg * CPW;  // first function of this warp's columns
-        // ---- the unit's accumulators -> G / 2^(e_p + f_T - 7(S+1)) (FP64) in registers; the
-        // scale is applied to each row dot
-        double sc[NS][KP];
+      const int* fsh = fn_sh + G.fn_off;
+      const double* trad = rad + G.rad_off + (long long)t.y * G.nsimple * NR * kTcPoints + row;
+      epi_sync_or(false);  // the scale table is complete
+      for (int ft = 0; ft < nft; ft++) {
+        const int i0 = ft * kTcFuncs;
+        // ---- this warp's columns [w0, w0 + wlen) and the shells they touch (lane s holds shell s)
+        const int w0 = i0 + colg * CPW, wlen = min(CPW, m - w0);
+        int nsl = 0, sh_a = 0;
+        double s_ax = 0.0, s_ay = 0.0, s_az = 0.0;
+        int s_type = 0, s_fcol = 0;
+        if (wlen > 0) {
+          sh_a = fsh[w0];
+          nsl = fsh[w0 + wlen - 1] - sh_a + 1;  // <= 16: one shell per function at most
+          if (lane < nsl) {
+            const int sh = sh_a + lane;
+            const int atom = nuc[sf_glob[G.sf_off + sh]];
+            s_ax = ax[atom];
+            s_ay = ay[atom];
+            s_az = az[atom];
+            s_type = sf_type[G.sf_off + sh];
+            s_fcol = sf_fn[G.sf_off + sh] - w0;  // first component's column in the window (may be < 0)
+          }
+          // their radial sums at this thread's point, copied while the unit's MMAs run
+          for (int s2 = 0; s2 < nsl; s2++)
 #pragma unroll
-        for (int sp = 0; sp < NS; sp++)
-#pragma unroll
-          for (int kp = 0; kp < KP; kp++) sc[sp][kp] = spx[first + kp] * (sp == 0 ? tsa : tsb)[ft * kTcFuncs];
-        bool ok = !lfail && !*vfail && lio::umma::mbar_wait(&tfull, ucnt & 1);
-        ok = __all_sync(0xffffffffu, ok);
-        lio::umma::fence_after_sync();
-        double g[CPW][NS][KP];
-        if (ok) {
+            for (int k = 0; k < NR; k++)
+              asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(wrad_s + (uint32_t)((s2 * NR + k) * 32 * 8)),
+                           "l"(trad + ((long long)(sh_a + s2) * NR + k) * kTcPoints)
+                           : "memory");
+          asm volatile("cp.async.commit_group;" ::: "memory");
+        }
+        for (int pass = 0; pass < NP; pass++, ucnt++) {
+          const int first = pass * KP;
+          const int cb = colg * CPW;  // this warp's first column of the function tile
+          // ---- the unit's accumulators -> G (FP64), parked in the TMEM columns after the levels
+          double sc[NS][KP];
 #pragma unroll
           for (int sp = 0; sp < NS; sp++)
 #pragma unroll
-            for (int kp = 0; kp < KP; kp++)
+            for (int kp = 0; kp < KP; kp++) sc[sp][kp] = spx[first + kp] * (sp == 0 ? tsa : tsb)[i0];
+          bool ok = !lfail && !*vfail && lio::umma::mbar_wait(&tfull, ucnt & 1);
+          ok = __all_sync(0xffffffffu, ok);
+          lio::umma::fence_after_sync();
+          const uint32_t gbase = lane_base + Cfg::kCols + (uint32_t)cb * Cfg::kGPer;  // this warp's columns
+          if (ok && wlen > 0) {
 #pragma unroll
-              for (int h = 0; h < CPW / 8; h++) {
-                int32_t lv[kSlices][8];
+            for (int h = 0; h < CPW / 8; h++) {
+              double gh[8][NS][KP];
 #pragma unroll
-                for (int l = 0; l < kSlices; l++)
-                  lio::umma::tmem_ld8(
-                      lane_base + (uint32_t)(((sp * KP + kp) * kSlices + l) * kTcFuncs + colg * CPW + h * 8), lv[l]);
-                lio::umma::tmem_wait_ld();
+              for (int sp = 0; sp < NS; sp++)
 #pragma unroll
-                for (int c = 0; c < 8; c++) g[h * 8 + c][sp][kp] = level_sum(lv, c, narrow);
+                for (int kp = 0; kp < KP; kp++) {
+                  int32_t lv[kSlices][8];
+#pragma unroll
+                  for (int l = 0; l < kSlices; l++)
+                    lio::umma::tmem_ld8(lane_base + (uint32_t)(((sp * KP + kp) * kSlices + l) * kTcFuncs + cb + h * 8),
+                                        lv[l]);
+                  lio::umma::tmem_wait_ld();
+#pragma unroll
+                  for (int c = 0; c < 8; c++) gh[c][sp][kp] = level_sum(lv, c, narrow) * sc[sp][kp];
+                }
+              // 8 columns x NS x KP doubles: 8 * kGPer consecutive 32-bit TMEM columns
+#pragma unroll
+              for (int part = 0; part < (8 * (int)Cfg::kGPer) / 16; part++) {
+                uint32_t v[16];
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                  const int idx = part * 8 + e;  // double index within the block: c * NS * KP + sp * KP + kp
+                  const int c = idx / (NS * KP), sk = idx % (NS * KP);
+                  const double x = gh[c][sk / KP][sk % KP];
+                  v[2 * e] = (uint32_t)__double2loint(x);
+                  v[2 * e + 1] = (uint32_t)__double2hiint(x);
+                }
+                lio::umma::tmem_st16(gbase + (uint32_t)(h * 8 * Cfg::kGPer + part * 16), v);
               }
-        } else {
-          lfail = true;
-          *vfail = 1;
-        }
-        // accumulators read: hand TMEM back to the MMA issuer
-        lio::umma::fence_before_sync();
-        __syncwarp();
-        if (lane == 0 && ok) lio::umma::mbar_arrive(&tempty);
-        // ---- row dots against the unit's basis chunks (none for a column half past m)
-        const int klo = unit_klo(first), khi = unit_khi(first, NK);
-        const bool cols = cb < m;
-        for (int k = klo; k <= khi; k++, bcnt++) {
-          const int buf = bcnt % kBStages, use = bcnt / kBStages;
-          bool okb = !lfail && !*vfail && lio::umma::mbar_wait(&bfull[buf], use & 1);
-          okb = __all_sync(0xffffffffu, okb);
-          if (!okb) {
+            }
+            lio::umma::tmem_wait_st();
+          } else if (!ok) {
             lfail = true;
             *vfail = 1;
-          } else if (cols) {
-            const double* ch = bring + (size_t)buf * kTcChunk + (colg * CPW) * kTcPoints + row;
-            double d4[4][NS][KP];
-#pragma unroll
-            for (int c = 0; c < 4; c++)
-#pragma unroll
-              for (int sp = 0; sp < NS; sp++)
-#pragma unroll
-                for (int kp = 0; kp < KP; kp++) d4[c][sp][kp] = ch[c * kTcPoints] * g[c][sp][kp];
-#pragma unroll
-            for (int c = 4; c < CPW; c++) {
-              const double v = ch[c * kTcPoints];
-#pragma unroll
-              for (int sp = 0; sp < NS; sp++)
-#pragma unroll
-                for (int kp = 0; kp < KP; kp++) d4[c & 3][sp][kp] = fma(v, g[c][sp][kp], d4[c & 3][sp][kp]);
-            }
-            double d[NS][KP];
-#pragma unroll
-            for (int sp = 0; sp < NS; sp++)
-#pragma unroll
-              for (int kp = 0; kp < KP; kp++)
-                d[sp][kp] = ((d4[0][sp][kp] + d4[1][sp][kp]) + (d4[2][sp][kp] + d4[3][sp][kp])) * sc[sp][kp];
-            apply_chunk<GGA, NS, NQ, KP>(first, k, d, q);
           }
+          // levels read: hand their columns back to the MMA issuer (G stays in the columns after them)
+          lio::umma::fence_before_sync();
           __syncwarp();
-          if (lane == 0 && okb) lio::umma::mbar_arrive(&bempty[buf]);
+          if (lane == 0 && ok) lio::umma::mbar_arrive(&tempty);
+          if (!ok || wlen <= 0) continue;
+          if (pass == 0) asm volatile("cp.async.wait_all;" ::: "memory");  // this thread's radial sums landed
+          // ---- shell by shell over this warp's columns
+#pragma unroll 1
+          for (int s2 = 0; s2 < nsl; s2++) {
+            const int type = __shfl_sync(0xffffffffu, s_type, s2);
+            const int fcol = __shfl_sync(0xffffffffu, s_fcol, s2);
+            ShellPoint spt;
+            spt.r[0] = xp - __shfl_sync(0xffffffffu, s_ax, s2);
+            spt.r[1] = yp - __shfl_sync(0xffffffffu, s_ay, s2);
+            spt.r[2] = zp - __shfl_sync(0xffffffffu, s_az, s2);
+            spt.t = wrad[(s2 * NR) * 32];
+            spt.tg2 = GGA ? wrad[(s2 * NR + 1) * 32] : 0.0;
+            spt.th4 = GGA ? wrad[(s2 * NR + 2) * 32] : 0.0;
+            if (type == 0)
+              shell_unit<0, GGA, NS, KP, NQ, Cfg::kGPer>(pass, gbase, fcol, wlen, spt, dnorm, q);
+            else if (type == 1)
+              shell_unit<1, GGA, NS, KP, NQ, Cfg::kGPer>(pass, gbase, fcol, wlen, spt, dnorm, q);
+            else
+              shell_unit<2, GGA, NS, KP, NQ, Cfg::kGPer>(pass, gbase, fcol, wlen, spt, dnorm, q);
+          }
         }
       }
       // tile done: column group 1 hands its sums to column group 0, which writes them
@@ -622,7 +765,7 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
 #pragma unroll
         for (int sp = 0; sp < NS; sp++)
 #pragma unroll
-          for (int k = 0; k < NQ; k++) red[(sp * kTcPoints + row) * NQ + k] = q[sp][k];
+          for (int k = 0; k < NQ; k++) red[(sp * 32 + lane) * NQ + k] = q[sp][k];
       }
       const bool anyfail = epi_sync_or(lfail || *vfail);
       if (anyfail) break;
@@ -631,20 +774,21 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
         for (int sp = 0; sp < NS; sp++) {
           double* dst = (sp == 0 ? part_a : part_b) + G.part_off;
 #pragma unroll
-          for (int k = 0; k < NQ; k++) dst[(long long)k * ldp + p] = q[sp][k] + red[(sp * kTcPoints + row) * NQ + k];
+          for (int k = 0; k < NQ; k++) {
+            const double v = q[sp][k] + red[(sp * 32 + lane) * NQ + k];
+            dst[(long long)k * ldp + p] = k == 0 ? v : 2.0 * v;  // the factor 2 of the derivative terms
+          }
         }
       }
       epi_sync_or(false);  // the table and the reduction area are free again
     }
-    if (etid == 0) bconsumed = bcnt;
+    asm volatile("cp.async.wait_all;" ::: "memory");  // nothing in flight into shared memory at exit
   }
   __syncthreads();  // every role done
-  if ((warp == Cfg::kProd || warp == Cfg::kBasisProd) && lane == 0) {
+  if (warp == Cfg::kProd && lane == 0) {
     // copies issued but never consumed (after a timeout) land before the CTA exits
-    const bool basis = warp == Cfg::kBasisProd;
-    const int nb = basis ? kBStages : kStages;
-    for (int k = basis ? bconsumed : consumed; k < issued; k++)
-      if (!lio::umma::mbar_wait(basis ? &bfull[k % nb] : &full[k % nb], (k / nb) & 1)) break;
+    for (int k = consumed; k < issued; k++)
+      if (!lio::umma::mbar_wait(&full[k % kStages], (k / kStages) & 1)) break;
   }
   lio::umma::fence_before_sync();
   __syncthreads();

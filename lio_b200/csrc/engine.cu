@@ -72,6 +72,7 @@ struct GroupDev {
   long long fa_off;    // int8 slices of F by function row for the Kohn-Sham contraction (bytes)
   long long fae_off;   // their per-row exponents (elements): nI x 128
   long long fbe_off;   // per-row exponents of f*F (elements): nJ x 32
+  long long rad_off;   // radial sums of the tensor-core density (elements): per 128-point tile, shell, NR values
 };
 
 // Process-wide pinned host staging of the grid build (grow-only, one buffer per
@@ -790,12 +791,16 @@ struct DeviceEngine::Impl {
   int M = 0, natoms = 0;
   bool lda = false, open = false;
   int iexch = 9;
-  int nk = 1;
+  int nk = 1;   // kinds of the FP64 form's function-major basis cache: 1 (LDA) or 10 (GGA)
+  int nkb = 1;  // kinds of the tensor-core form's blocked basis: F (LDA), or F and its gradient (GGA)
   long long npoints = 0, ngroups = 0, total_ldp = 0;
   std::vector<GroupDev> hgroups;
   DevBuf<GroupDev> groups;
   DevBuf<double> px, py, pz, pw;
   DevBuf<int> fn_glob, sf_glob, sf_type, nuc, ncont, fn_sh, fn_atom;
+  DevBuf<int> sf_fn;  // per simple function (shell) of a group: the local index of its first component
+  DevBuf<double> rad;  // radial sums per (tile, shell, point) of the tensor-core density
+  long long rad_elems = 0;
   DevBuf<int8_t> fn_cp;
   // tensor-core form (built on first use per geometry)
   DevBuf<int2> slice_basis_tiles, slice_dens_tiles;
@@ -859,8 +864,8 @@ struct DeviceEngine::Impl {
     if (basis_tiles.n > 0 && ngroups > 0) {
       k_basis<<<(unsigned)basis_tiles.n, kBasisBlock, 0, stream>>>(basis_tiles.p, groups.p, px.p, py.p, pz.p,
                                                                     sf_glob.p, sf_type.p, nuc.p, ncont.p, ca.p, cc.p,
-                                                                    ax.p, ay.p, az.p, basis_norm, nk, dst.p,
-                                                                    blocked ? nk : 0);
+                                                                    ax.p, ay.p, az.p, basis_norm, blocked ? nkb : nk,
+                                                                    dst.p, blocked ? nkb : 0);
       LIO_CUDA(cudaGetLastError());
     }
     LIO_CUDA(cudaStreamSynchronize(stream));
@@ -1081,19 +1086,21 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
   d->open = sys.open;
   d->iexch = sys.iexch;
   d->nk = sys.lda ? 1 : 10;
+  d->nkb = sys.lda ? 1 : 4;
   d->max_nftc = 0;
   d->d_norm = sys.d_norm;
   const int NQ = sys.lda ? 1 : kNQ;
 
   std::vector<GroupDev> gd;
   std::vector<int> src_group;  // partition group of each device group
-  std::vector<int> hfn, hsf, hst, hfsh, hfat;
+  std::vector<int> hfn, hsf, hst, hfsh, hfat, hsffn;
   std::vector<int8_t> hfcp;
   std::vector<int2> btiles, ftiles, sbtiles, sdtiles;
   std::vector<int4> dtiles, ktiles, tctiles;
   long long pt_off = 0, fn_off = 0, sf_off = 0, bas_off = 0, part_off = 0;
   long long bb_off = 0, sl_off = 0, aexp_off = 0, ds_off = 0, dexp_off = 0;
-  long long fa_off = 0, fae_off = 0, fbe_off = 0;
+  long long fa_off = 0, fae_off = 0, fbe_off = 0, rad_off = 0;
+  const int NR = sys.lda ? 1 : 3;  // radial sums per (shell, point)
   std::vector<int2> farows, fbrows, fat32;
   std::vector<int4> fktiles, frtiles;
   long long npts_total = 0;
@@ -1125,6 +1132,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
     G.fa_off = fa_off;
     G.fae_off = fae_off;
     G.fbe_off = fbe_off;
+    G.rad_off = rad_off;
     const int nI = (G.m + kFkRows - 1) / kFkRows, nJ = (G.m + kFkCols - 1) / kFkCols;
     for (int i = 0; i < nI * kFkRows; i++) farows.push_back({gdev, i});
     for (int j = 0; j < nJ * kFkCols; j++) fbrows.push_back({gdev, j});
@@ -1138,6 +1146,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
       const int type = f < sys.s_funcs ? 0 : (f < sys.s_funcs + 3 * sys.p_funcs ? 1 : 2);
       hsf.push_back(f);
       hst.push_back(type);
+      hsffn.push_back((int)((long long)hfn.size() - G.fn_off));
       const int ncomp = type == 0 ? 1 : (type == 1 ? 3 : 6);
       const int c0 = type == 0 ? 0 : (type == 1 ? 1 : 4);
       for (int k = 0; k < ncomp; k++) {
@@ -1165,7 +1174,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
     sf_off += G.nsimple;
     bas_off += (long long)d->nk * G.m * G.ldp;
     part_off += (long long)G.nft * NQ * G.ldp;
-    bb_off += (long long)(G.ldp / kTcPoints) * G.nftc * d->nk * kTcChunk;
+    bb_off += (long long)(G.ldp / kTcPoints) * G.nftc * d->nkb * kTcChunk;
     d->max_nftc = std::max(d->max_nftc, G.nftc);
     sl_off += (long long)(G.ldp / kTcPoints) * NA * (G.m32 / 32) * kTcStepA;
     aexp_off += (long long)NA * G.ldp;
@@ -1174,6 +1183,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
     fa_off += (long long)nI * kSlices * kFkRows * G.ldp;
     fae_off += (long long)nI * kFkRows;
     fbe_off += (long long)nJ * kFkCols;
+    rad_off += (long long)G.ldp * G.nsimple * NR;
     npts_total += G.npts;
     gd.push_back(G);
   }
@@ -1247,6 +1257,8 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
   (void)tctiles;
   d->sf_glob.upload(hsf);
   d->sf_type.upload(hst);
+  d->sf_fn.upload(hsffn);
+  d->rad_elems = rad_off;
   d->nuc.upload(hnuc);
   d->ncont.upload(hnc);
   d->ca.upload(sys.a);
@@ -1357,12 +1369,24 @@ void DeviceEngine::prepare_tensor_core() {
   }
   d->tc_err.alloc(1);
   LIO_CUDA(cudaMemsetAsync(d->tc_err.p, 0, sizeof(int), st));
+  // radial sums of every shell at every point, read by the density contraction's epilogue
+  d->rad.alloc(d->rad_elems);
+  if (d->lda)
+    k_radial<1><<<(unsigned)d->slice_basis_tiles.n, kTcPoints, 0, st>>>(
+        d->slice_basis_tiles.p, d->groups.p, d->px.p, d->py.p, d->pz.p, d->sf_glob.p, d->nuc.p, d->ncont.p, d->ca.p,
+        d->cc.p, d->ax.p, d->ay.p, d->az.p, d->rad.p);
+  else
+    k_radial<3><<<(unsigned)d->slice_basis_tiles.n, kTcPoints, 0, st>>>(
+        d->slice_basis_tiles.p, d->groups.p, d->px.p, d->py.p, d->pz.p, d->sf_glob.p, d->nuc.p, d->ncont.p, d->ca.p,
+        d->cc.p, d->ax.p, d->ay.p, d->az.p, d->rad.p);
+  LIO_CUDA(cudaGetLastError());
   if (d->lda)
     k_slice_basis<1><<<(unsigned)d->slice_basis_tiles.n, kTcPoints, 0, st>>>(d->slice_basis_tiles.p, d->groups.p,
                                                                             d->bblk.p, 1, d->aslices.p, d->aexp.p);
   else
     k_slice_basis<4><<<(unsigned)d->slice_basis_tiles.n, kTcPoints, 0, st>>>(d->slice_basis_tiles.p, d->groups.p,
-                                                                            d->bblk.p, 10, d->aslices.p, d->aexp.p);
+                                                                            d->bblk.p, d->nkb, d->aslices.p,
+                                                                            d->aexp.p);
   LIO_CUDA(cudaGetLastError());
   d->fa_slices.alloc(d->fk_sizes[0]);
   d->fa_exp.alloc(d->fk_sizes[1]);
@@ -1373,10 +1397,10 @@ void DeviceEngine::prepare_tensor_core() {
   {
     const int nrows = (int)d->fa_rows.n;
     k_fock_rowexp<1><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(d->fa_rows.p, nrows, d->groups.p, d->bblk.p,
-                                                                  nullptr, nullptr, d->fa_exp.p, nullptr, 0, d->nk);
+                                                                  nullptr, nullptr, d->fa_exp.p, nullptr, 0, d->nkb);
     LIO_CUDA(cudaGetLastError());
     k_fock_aslices<<<(unsigned)d->fa_tiles32.n, 256, 0, st>>>(d->fa_tiles32.p, d->groups.p, d->bblk.p,
-                                                                d->fa_exp.p, d->fa_slices.p, d->nk);
+                                                                d->fa_exp.p, d->fa_slices.p, d->nkb);
     LIO_CUDA(cudaGetLastError());
   }
   LIO_CUDA(cudaFuncSetAttribute(k_fock_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FkCfg<1>::kSmem));
@@ -1440,7 +1464,8 @@ int DeviceEngine::run_kernels(bool compute_rmm, bool ext) {
 #define LIO_DENSITY_TC(GGA, NS)                                                                                    \
   k_density_tc<GGA, NS><<<nt, TcCfg<GGA, NS>::kThreads, TcCfg<GGA, NS>::smem(cap), st>>>(                          \
       d->dens_tc_tiles.p, ntiles, d->groups.p, d->aslices.p, d->aexp.p, d->dslices_a.p, d->dexp_a.p,               \
-      d->dslices_b.p, d->dexp_b.p, d->bblk.p, cap, d->part_a.p, d->part_b.p, d->tc_err.p)
+      d->dslices_b.p, d->dexp_b.p, cap, d->px.p, d->py.p, d->pz.p, d->fn_sh.p, d->sf_glob.p, d->sf_type.p,            \
+      d->sf_fn.p, d->nuc.p, d->ax.p, d->ay.p, d->az.p, d->rad.p, d->basis_norm, d->part_a.p, d->part_b.p, d->tc_err.p)
     if (d->lda) {
       if (d->open) LIO_DENSITY_TC(false, 2); else LIO_DENSITY_TC(false, 1);
     } else {
@@ -1486,21 +1511,21 @@ int DeviceEngine::run_kernels(bool compute_rmm, bool ext) {
       if (d->open)
         k_fock_rowexp<2><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(d->fb_rows.p, nrows, d->groups.p, d->bblk.p,
                                                                       d->fac_a.p, d->fac_b.p, d->fb_exp_a.p,
-                                                                      d->fb_exp_b.p, 1, d->nk);
+                                                                      d->fb_exp_b.p, 1, d->nkb);
       else
         k_fock_rowexp<1><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(d->fb_rows.p, nrows, d->groups.p, d->bblk.p,
                                                                       d->fac_a.p, nullptr, d->fb_exp_a.p, nullptr, 1,
-                                                                      d->nk);
+                                                                      d->nkb);
       LIO_CUDA(cudaGetLastError());
       launches++;
       d->mark(4);
       if (d->open)
         k_fock_tc<2><<<(unsigned)d->fk_tiles.n, FkCfg<2>::kThreads, FkCfg<2>::kSmem, st>>>(
-            d->fk_tiles.p, d->groups.p, d->fn_glob.p, d->fa_slices.p, d->fa_exp.p, d->bblk.p, d->nk, d->fac_a.p,
+            d->fk_tiles.p, d->groups.p, d->fn_glob.p, d->fa_slices.p, d->fa_exp.p, d->bblk.p, d->nkb, d->fac_a.p,
             d->fac_b.p, d->fb_exp_a.p, d->fb_exp_b.p, d->M, Ka, Kb, d->tc_err.p);
       else
         k_fock_tc<1><<<(unsigned)d->fk_tiles.n, FkCfg<1>::kThreads, FkCfg<1>::kSmem, st>>>(
-            d->fk_tiles.p, d->groups.p, d->fn_glob.p, d->fa_slices.p, d->fa_exp.p, d->bblk.p, d->nk, d->fac_a.p,
+            d->fk_tiles.p, d->groups.p, d->fn_glob.p, d->fa_slices.p, d->fa_exp.p, d->bblk.p, d->nkb, d->fac_a.p,
             nullptr, d->fb_exp_a.p, nullptr, d->M, Ka, nullptr, d->tc_err.p);
     } else if (d->open) {
       d->mark(4);  // no operand preparation in the FP64 form
@@ -1550,7 +1575,7 @@ void DeviceEngine::prepare() {
 
 size_t DeviceEngine::cache_bytes() const {
   const Impl* d = impl_.get();
-  size_t b = (d->basis.cap + d->bblk.cap) * sizeof(double);
+  size_t b = (d->basis.cap + d->bblk.cap + d->rad.cap) * sizeof(double);
   for (const auto* x : {&d->aslices, &d->dslices_a, &d->dslices_b, &d->fa_slices})
     b += x->cap;
   for (const auto* x : {&d->aexp, &d->dexp_a, &d->dexp_b, &d->fa_exp, &d->fb_exp_a, &d->fb_exp_b})
@@ -1574,6 +1599,7 @@ void DeviceEngine::drop_tensor_core() {
     b->free();
   for (auto* b : {&d->aexp, &d->dexp_a, &d->dexp_b, &d->fa_exp, &d->fb_exp_a, &d->fb_exp_b}) b->free();
   d->bblk.free();
+  d->rad.free();
   d->tc_ready = false;
   d->drop_graph();
 }
@@ -1661,7 +1687,8 @@ size_t DeviceEngine::estimate_device_bytes(const System& sys, const Partition& p
     b += ldp * (6 * 8 + nspin * (nq * (double)nft * 8 + 8));  // points, partials, factors
     if (prec == Precision::FP64) b += ldp * nk * (double)m * 8;  // function-major basis cache
     if (prec == Precision::TensorCore)
-      b += ldp * ((double)nftc * kTcFuncs * nk * 8 + (double)na * m32 * kSlices + na * 2 +
+      b += ldp * ((double)nftc * kTcFuncs * (sys.lda ? 1 : 4) * 8 + (double)pg.funcs.size() * (sys.lda ? 1 : 3) * 8 +
+                  (double)na * m32 * kSlices + na * 2 +
                   (double)nI * kFkRows * kSlices) +
            (double)nspin * nftc * m32 * kTcTall;
   }
@@ -1878,7 +1905,7 @@ SolveResult DeviceEngine::solve_forces(const SolveRequest& req, double* forces, 
     LIO_CUDA(cudaGetLastError());
     bv = BasisView{grad.p, 0, 4};
   } else if (precision_ == Precision::TensorCore) {
-    bv = BasisView{d->bblk.p, d->nk, 1};
+    bv = BasisView{d->bblk.p, d->nkb, 1};
   } else {
     bv = BasisView{d->basis.p, 0, 1};
   }
@@ -1894,7 +1921,7 @@ SolveResult DeviceEngine::solve_forces(const SolveRequest& req, double* forces, 
     const int nu = (int)d->force_tc_tiles.n;
     k_force_tc<<<(unsigned)std::min(nu, 2 * d->nsm), FtCfg::kThreads, FtCfg::kSmem, st>>>(
         d->force_tc_tiles.p, nu, d->groups.p, 4, d->aslices.p, d->aexp.p, d->dslices_a.p, d->dexp_a.p,
-        d->open ? d->dslices_b.p : nullptr, d->open ? d->dexp_b.p : nullptr, d->bblk.p, d->nk, d->fac_a.p,
+        d->open ? d->dslices_b.p : nullptr, d->open ? d->dexp_b.p : nullptr, d->bblk.p, d->nkb, d->fac_a.p,
         d->open ? d->fac_b.p : nullptr, d->fn_atom.p, frc.p, d->tc_err.p);
   } else if (d->open)
     k_force_fp64<2><<<nd, 256, 0, st>>>(d->dens_tiles.p, d->groups.p, d->fn_glob.p, d->fn_atom.p, bv, d->P_a.p,
