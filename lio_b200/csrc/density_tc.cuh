@@ -569,7 +569,15 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
   } else if (warp == Cfg::kMma) {
     // ------------------------------------------------------------ MMA issuer
     if (lane == 0) {
+      // descriptors of the first A slice and of the stacked D of each stage; an
+      // operand further into the stage adds its byte offset / 16 to the start
+      // address field (bits 0-13: shared addresses stay below 2^18 bytes)
       const uint32_t smem0 = lio::umma::smem_u32(tc_smem);
+      const uint64_t ad0 = lio::umma::smem_desc(smem0, 16u * kTcPoints, 128u);
+      const uint64_t ad1 = lio::umma::smem_desc(smem0 + Cfg::kStage, 16u * kTcPoints, 128u);
+      const uint64_t dd0 = lio::umma::smem_desc(smem0 + Cfg::kStageA, 16u * kTcTall, 128u);
+      const uint64_t dd1 = lio::umma::smem_desc(smem0 + Cfg::kStage + Cfg::kStageA, 16u * kTcTall, 128u);
+      static_assert(Cfg::kStages == 2, "two descriptor bases");
       int cnt = 0, ucnt = 0;
       bool stop = false;
       for (int w = blockIdx.x; w < ntiles && !stop; w += gridDim.x) {
@@ -592,19 +600,19 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
             }
             consumed = cnt + 1;
             lio::umma::fence_after_sync();
-            const uint32_t sa = smem0 + buf * Cfg::kStage;
+            const uint64_t ad = buf ? ad1 : ad0, dd = buf ? dd1 : dd0;
 #pragma unroll
             for (int sp = 0; sp < NS; sp++) {
               // stacked D of this spin: K-major, 192 rows (LBO = 16 * 192 bytes between K halves)
-              const uint64_t bd = lio::umma::smem_desc(sa + Cfg::kStageA + sp * kTcStepD, 16u * kTcTall, 128u);
+              const uint64_t bd = dd + (uint64_t)((sp * kTcStepD) >> 4);
 #pragma unroll
               for (int kp = 0; kp < KP; kp++)
 #pragma unroll
                 for (int s = 0; s < kSlices; s++)
-                  lio::umma::mma_i8(
-                      tbase + (uint32_t)(((sp * KP + kp) * kSlices + s) * kTcFuncs),
-                      lio::umma::smem_desc(sa + kp * kTcStepA + s * kTcSliceA, 16u * kTcPoints, 128u), bd,
-                      lio::umma::idesc_i8(kTcPoints, (kSlices - s) * kTcFuncs), (kk > 0 || s > 0) ? 1u : 0u);
+                  lio::umma::mma_i8(tbase + (uint32_t)(((sp * KP + kp) * kSlices + s) * kTcFuncs),
+                                    ad + (uint64_t)((kp * kTcStepA + s * kTcSliceA) >> 4), bd,
+                                    lio::umma::idesc_i8(kTcPoints, (kSlices - s) * kTcFuncs),
+                                    (kk > 0 || s > 0) ? 1u : 0u);
             }
             lio::umma::commit(&empty[buf]);
             if (kk == nks - 1) lio::umma::commit(&tfull);
