@@ -188,27 +188,66 @@ def stage_times(L, steps: int):
     return [stage[i] / max(1, nsol.value) for i in range(5)]
 
 
-def measured_traffic(workload: str, tc: bool):
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary
-    (profiles/density_launch_traffic.md: 'workload | kernel | bytes' rows), or None."""
-    p = os.path.join(ROOT, "profiles", "density_launch_traffic.md")
-    if not os.path.exists(p):
-        return None
-    want = "k_density_tc" if tc else "k_density_fp64"
-    key = workload.split(":")[0]
-    with open(p) as f:
-        for ln in f:
-            parts = [x.strip() for x in ln.strip().strip("|").split("|")]
-            if len(parts) >= 3 and parts[0] == key and parts[1] == want:
-                try:
-                    return float(parts[2])
-                except ValueError:
-                    return None
-    return None
+# DRAM traffic of the dominant kernel. A full-size capture of DRAM counters is
+# not taken (too large a workload for a multi-pass capture); the 64-atom
+# open-shell case (bench.py --workload cfg2-open, 711,684 points, ncu --set full
+# on one k_density_tc launch) moved 1.731 GB (1.634 read + 0.097 written)
+# against the 1.285 GB its algorithmic-bytes model below gives: 1.35x. A full
+# launch's traffic is estimated as that ratio times its own algorithmic bytes
+# (the same byte classes grow with the same partition sums).
+SMALL_CASE_TRAFFIC_RATIO = 1.731 / 1.2851
+FP64_PEAK_NOMINAL = 37.0e12  # FLOP/s, the B200's nominal FP64 rate (no measured figure exists for it)
 
 
-def cpu_baseline(wl: W.Workload):
-    """Reference CPU g2g path on the same molecule (194-point grid), one warm-up and one timed build."""
+def partition_sums(lib):
+    """Partition statistics, plus the sum over groups of points x shells (simple functions)."""
+    st = lib.partition_stats()
+    meta = (C.c_int * 8)()
+    pns = 0
+    for g in range(st["groups"]):
+        lib.lib.g2g_partition_group_(C.byref(C.c_int(g)), meta, None, None, None)
+        pns += meta[0] * meta[1]
+    st["pns"] = pns
+    return st
+
+
+def roofline_model(st, gga: bool, nspin: int, tc: bool, stage_ms, hbm_gbs: float, bf16_tflops: float):
+    """Per-stage algorithmic bytes and FLOPs of one XC build and its roofline time
+    (the sum over stages of max(FLOPs / peak, bytes / HBM bandwidth), FLOPs as the
+    nominal GEMM counts 2 n m^2 per kind and spin against the measured bf16 rate).
+    Bytes count what each stage must read and write once."""
+    pts, pm, pm2, pns = st["points"], st["pm"], st["pm2"], st["pns"]
+    na, nr, nq = (4, 3, 10) if gga else (1, 1, 1)
+    b = {}
+    f = {}
+    # density operands (tensor-core form): the groups' dense density blocks gathered and cut into slices
+    b["density_operands"] = 0.0
+    # density: the int8 slices of the basis (na kinds x 6 slices per point and function), the radial sums
+    # (nr per point and shell) in the tensor-core form; the FP64 basis values (10 or 1 kinds) in the FP64 form;
+    # the per-point quantities written per spin and the point coordinates
+    b["density"] = (pm * na * 6.0 + pns * nr * 8.0 if tc else pm * (10 if gga else 1) * 8.0) + \
+        pts * (nq * 8.0 * nspin + 24.0)
+    f["density"] = 2.0 * pm2 * na * nspin
+    b["functional"] = pts * (nq * 8.0 * nspin + 8.0 + 8.0 * nspin)
+    # Kohn-Sham operands: F read once with the factors (tensor-core form)
+    b["ks_operands"] = (pm * 8.0 + pts * 8.0 * nspin) if tc else 0.0
+    # Kohn-Sham: F (and its int8 slices in the tensor-core form) and the factors
+    b["ks"] = pm * (8.0 + (6.0 if tc else 0.0)) + pts * 8.0 * nspin
+    f["ks"] = 2.0 * pm2 * nspin
+    bw = hbm_gbs * 1e9
+    stages = {}
+    total = 0.0
+    for i, name in enumerate(STAGES):
+        t = max(f.get(name, 0.0) / (bf16_tflops * 1e12), b.get(name, 0.0) / bw)
+        stages[name] = {"bytes": b.get(name, 0.0), "flops": f.get(name, 0.0), "roofline_ms": t * 1e3,
+                        "measured_ms": stage_ms[i]}
+        total += t
+    return stages, total * 1e3
+
+
+def cpu_baseline(wl: W.Workload, builds: int = 5):
+    """Reference CPU g2g path on the same molecule (194-point grid): one warm-up,
+    then the median of `builds` timed builds."""
     if not os.path.exists(REF_LIB):
         return None
     wl = W.Workload(**{**wl.__dict__, "n_ang": 194})
@@ -219,13 +258,16 @@ def cpu_baseline(wl: W.Workload):
     L.reload_atom_positions(gt)
     npts = sum(int(L.partition_group(g, ref=True)["meta"][0]) for g in range(L.num_groups(ref=True)))
     L.solve_groups(0)
-    t0 = time.perf_counter()
-    L.solve_groups(0)
-    dt = time.perf_counter() - t0
+    times = []
+    for _ in range(builds):
+        t0 = time.perf_counter()
+        L.solve_groups(0)
+        times.append(time.perf_counter() - t0)
     L.deinit()
+    dt = statistics.median(times)
     return {"value": npts / dt, "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": f"one timed full XC build (after one warm-up) of the same molecule on the reference's "
-                      f"40x194 grid, {npts} points, {dt:.2f} s"}
+            "sample": f"median of {builds} timed full XC builds (after one warm-up) of the same molecule on the "
+                      f"reference's 40x194 grid, {npts} points, {dt:.2f} s each"}
 
 
 def ours(args, rank, world):
@@ -254,6 +296,7 @@ def ours(args, rank, world):
     grid_s = time.perf_counter() - t0
     st = lib.partition_stats()
     npts = st["points"]  # the whole molecule's points (the partition is built whole on every rank)
+    st_main = partition_sums(lib) if rank == 0 else st
     npacked = wl.basis.M * (wl.basis.M + 1) // 2
     nspin = 2 if wl.open_shell else 1
     # the N > 1 exchange: one all-reduce of [E_xc, K_alpha (, K_beta)] per build
@@ -356,21 +399,50 @@ def ours(args, rank, world):
                 "stage_ms": dict(zip(STAGES, fp64_stage))}
         lib.set_precision(args.precision)
 
+    # the same molecule on the reference's 40 x 194 grid (its largest table), beside the 302-point headline
+    same_grid = None
+    if world == 1 and not args.no_same_grid:
+        same_grid = same_grid_run(args, lib, wl, stream)
+
     if rank != 0:
         return None
     hbm, bf16, src = load_peaks()
-    # dominant kernel: the density contraction (stage 1), one launch per build
-    pm = st["pm"]
-    nk = 10 if wl.iexch > 3 else 1
-    na = 4 if wl.iexch > 3 else 1
-    nq = 10 if wl.iexch > 3 else 1
+    gga = wl.iexch > 3
     tc = args.precision == 1
-    # algorithmic bytes of one launch: the FP64 basis values (nk per point and
-    # function), the int8 slices of the basis (na kinds x 6 slices) in the
-    # tensor-core form, and the per-point density quantities written per spin
-    dens_bytes = pm * (nk * 8.0 + (na * 6.0 if tc else 0.0)) + nq * 8.0 * npts * nspin
+    st = st_main
+    stages, roof_ms = roofline_model(st, gga, nspin, tc, stage_ms, hbm, bf16)
+    na = 4 if gga else 1
+    # dominant kernel: the density contraction (stage 1), one launch per build. In the tensor-core form its
+    # binding resource by this model is the int8 tensor work: 21 slice-pair products (pairs s + t <= 5 of
+    # six slices per operand) per nominal product, at the int8 dense rate, twice the measured bf16 rate
     t_dens = stage_ms[1] * 1e-3
-    traffic = measured_traffic(wl.name, tc)
+    dens_bytes = stages["density"]["bytes"]
+    if tc:
+        int8_ops = 21.0 * stages["density"]["flops"]
+        int8_peak = 2.0 * bf16
+        t_tensor, t_hbm = int8_ops / (int8_peak * 1e12), dens_bytes / (hbm * 1e9)
+        roof = {"bound": "tensor" if t_tensor >= t_hbm else "hbm", "kernel": "k_density_tc",
+                "traffic": SMALL_CASE_TRAFFIC_RATIO * dens_bytes}
+        if t_tensor >= t_hbm:
+            roof.update(achieved=int8_ops / t_dens / 1e12, peak=int8_peak, unit="TOP/s (int8)",
+                        frac=int8_ops / t_dens / 1e12 / int8_peak,
+                        peak_source=src + " bf16 x 2 (the int8 dense rate of this part)")
+        else:
+            roof.update(achieved=dens_bytes / t_dens / 1e9, peak=hbm, unit="GB/s",
+                        frac=dens_bytes / t_dens / 1e9 / hbm, peak_source=src)
+        roof["hbm_frac"] = dens_bytes / t_dens / 1e9 / hbm
+        roof["algorithmic_bytes"] = dens_bytes
+    else:
+        roof = {"bound": "hbm", "kernel": "k_density_fp64", "achieved": dens_bytes / t_dens / 1e9, "peak": hbm,
+                "unit": "GB/s", "frac": dens_bytes / t_dens / 1e9 / hbm, "traffic": None, "peak_source": src}
+    # the Kohn-Sham contraction: the larger of its byte and int8-work times against its measured time
+    ks = stages["ks"]
+    t_ks = stage_ms[4] * 1e-3
+    ks_roof = {"kernel": "k_fock_tc" if tc else "k_fock_fp64", "bytes": ks["bytes"],
+               "hbm_frac": ks["bytes"] / t_ks / 1e9 / hbm if t_ks > 0 else None}
+    if tc and t_ks > 0:
+        ks_ops = 21.0 * ks["flops"]
+        ks_roof["int8_frac"] = ks_ops / t_ks / 1e12 / (2.0 * bf16)
     result = {
         "metric": METRIC, "value": total_pts / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -379,23 +451,66 @@ def ours(args, rank, world):
         "config": {"workload": wl.name,
                    "points": npts, "groups": st["groups"], "M": wl.basis.M,
                    "precision": "fp64" if not tc else "tensor (int8 Ozaki slices, exact int32, FP64 outside)",
-                   "l2": "inputs larger than L2 (resident basis cache of %.1f GB)" % (nk * pm * 8 / 1e9),
+                   "l2": "inputs larger than L2 (%.1f GB read per build by the density contraction)" % (
+                       dens_bytes / 1e9),
                    "grid_build_s": round(grid_s, 3), "E_xc": E},
         "e2e": {"value": total_pts / (e2e_ms * 1e-3), "unit": UNIT,
                 "h2d_bytes_per_step": h2d_b, "d2h_bytes_per_step": d2h_b},
         "gpu_launches": int(launches) * args.steps,
         "stage_ms": dict(zip(STAGES, stage_ms)),
-        "roofline": {"bound": "hbm", "achieved": dens_bytes / t_dens / 1e9, "peak": hbm,
-                     "unit": "GB/s", "frac": dens_bytes / t_dens / 1e9 / hbm,
-                     "traffic": traffic, "kernel": "k_density_tc" if tc else "k_density_fp64",
-                     "peak_source": src},
+        "roofline": roof,
+        "build_roofline": {"roofline_ms": roof_ms, "measured_ms": ms, "frac": roof_ms / ms,
+                           "model": "sum over stages of max(nominal GEMM FLOPs / measured bf16 peak, "
+                                    "algorithmic bytes / measured HBM bandwidth)",
+                           "stages": stages},
+        "ks_roofline": ks_roof,
         "clocks": clk.summary(),
     }
     if fp64 is not None:
+        fp64_flops = stages["density"]["flops"] + stages["ks"]["flops"]
+        fp64["fp64_frac"] = fp64_flops / (fp64["ms_per_step"] * 1e-3) / FP64_PEAK_NOMINAL
+        fp64["fp64_peak"] = "%.0f TFLOP/s nominal" % (FP64_PEAK_NOMINAL / 1e12)
         result["fp64_plain"] = fp64
+    if same_grid is not None:
+        result["same_grid"] = same_grid
     if world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(wl)
     return result
+
+
+def same_grid_run(args, lib, wl, stream):
+    """The GPU arm on the same molecule's 40 x 194 grid (the grid the reference
+    arm runs): device-resident and end-to-end points/s through the same ABI."""
+    import torch
+
+    wl194 = W.Workload(**{**wl.__dict__, "n_ang": 194})
+    L = lib.lib
+    gt = bind(lib, wl194)
+    msg = lib.reload_atom_positions(gt)
+    if msg:
+        raise RuntimeError(msg)
+    npts = lib.partition_stats()["points"]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(args.warmup):
+        lib.solve_groups(0)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        lib.solve_groups(0)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    for _ in range(args.warmup):
+        L.g2g_solve_resident_()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        L.g2g_solve_resident_()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    res_ms = e0.elapsed_time(e1) / args.steps
+    return {"grid": "40x194", "points": npts, "value": npts / (res_ms * 1e-3), "ms_per_step": res_ms,
+            "e2e": npts / (e2e_ms * 1e-3), "e2e_ms_per_step": e2e_ms}
 
 
 def forces_mode(args):
@@ -518,16 +633,17 @@ def batch_mode(args):
     srv.close()
     tuned = {"fp64_ms_sum": sum(f[1] for f in forms), "tensor_ms_sum": sum(f[2] for f in forms)}
     forms = [f[0] for f in forms]
-    # the same builds in the plain FP64 form: per-molecule differences and its throughput
+    # the same builds in the plain FP64 form: its throughput
     ref = S.XCServer(precision=0, max_inflight=args.inflight)
     rmids = [ref.add(wl) for wl in wls]
     S.run_all(ref, rmids, {r: dens[m] for r, m in zip(rmids, mids)})
     t0 = time.perf_counter()
-    res0 = S.run_all(ref, rmids, {r: dens[m] for r, m in zip(rmids, mids)})
+    S.run_all(ref, rmids, {r: dens[m] for r, m in zip(rmids, mids)})
     dt0 = time.perf_counter() - t0
     ref.close()
-    de = max(abs(res[m][0] - res0[r][0]) for m, r in zip(mids, rmids))
-    dk = max(float(np.max(np.abs(res[m][1] - res0[r][1]))) for m, r in zip(mids, rmids))
+    # every molecule's E_xc and Kohn-Sham matrix against the oracle (the reference's CPU g2g path on
+    # the same 194-point grid), serially on the host cores
+    errs = oracle_errors([(wl, res[m]) for wl, m in zip(wls, mids)]) if not args.no_oracle else None
     nlda = sum(1 for wl in wls if wl.iexch <= 3)
     return {"metric": METRIC, "value": pts / dt, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
@@ -542,7 +658,25 @@ def batch_mode(args):
                        "service_precision": args.service_precision},
             "e2e": {"value": pts / dt, "unit": UNIT, "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
             "fp64_plain": {"value": pts / dt0, "ms_per_step": dt0 * 1e3},
-            "max_abs_dE_vs_fp64": de, "max_abs_dK_vs_fp64": dk}
+            "oracle": errs}
+
+
+def oracle_errors(cases):
+    """Per-molecule |dE_xc| and max |dK| of (workload, (E, K, ...)) results against
+    the oracle: the reference CPU g2g path for 194-point grids, the C
+    restatement for 302-point grids. Returns the worst of each, how many were
+    checked and how many met the tolerances (1e-6 Ha, 1e-7)."""
+    from tests import helpers as H
+
+    de, dk, ok = [], [], 0
+    for wl, r in cases:
+        E_ref, K_ref, _ = H.oracle_result(wl)
+        de.append(abs(r[0] - E_ref))
+        dk.append(float(np.max(np.abs(r[1] - K_ref))))
+        ok += int(de[-1] <= H.E_TOL and dk[-1] <= H.K_TOL)
+    return {"checked": len(cases), "within_tolerance": ok, "max_abs_dE": max(de) if de else None,
+            "max_abs_dK": max(dk) if dk else None,
+            "oracle": "reference CPU g2g path (194-point grids) / C restatement (302-point grids)"}
 
 
 def serve_mode(args):
@@ -586,11 +720,16 @@ def serve_mode(args):
             samples.append(sample)
         forms = [srv.form(m)[0] for m in mids]
         srv.close()
-        if prec == args.service_precision:  # after the server has released the GPU's memory
+        if prec == args.service_precision and not args.no_oracle:
+            # 1 % of the requests were sampled; at most `oracle_spots` of them per rate are checked against the
+            # oracle (the C restatement, single-threaded, seconds per molecule on these 302-point grids)
             for row, sample in zip(sweep, samples):
                 if sample:
-                    row["spot_checks"] = len(sample)
-                    row["spot_max_abs_dE_vs_fp64"], row["spot_max_abs_dK_vs_fp64"] = spot_check(wls, mids, sample)
+                    picked = sample[:args.oracle_spots]
+                    cases = [(W.Workload(**{**wls[mids.index(mid)].__dict__, "rho": rho}), (e, ka))
+                             for mid, rho, e, ka in picked]
+                    row["oracle_spot_checks"] = oracle_errors(cases)
+                    row["sampled_requests"] = len(sample)
         out["tensor" if prec else "fp64_plain"] = {
             "capacity_builds_per_s": cap, "sweep": sweep,
             "forms": {"tensor": sum(1 for f in forms if f == 1), "fp64": sum(1 for f in forms if f == 0)}}
@@ -598,22 +737,6 @@ def serve_mode(args):
     out.update(value=top["points_per_s"], p50_ms=top["p50_ms"], p99_ms=top["p99_ms"],
                dtype="i8-split/f64" if args.service_precision else "f64")
     return out
-
-
-def spot_check(wls, mids, sample):
-    """FP64 single-molecule C ABI on the sampled requests' molecules and densities."""
-    from tests import helpers as H
-
-    L = G2GLibrary()
-    de = dk = 0.0
-    for mid, rho, e, ka in sample:
-        wl = wls[mids.index(mid)]
-        wl2 = W.Workload(**{**wl.__dict__, "rho": rho})
-        E0, K0, _ = H.run(L, wl2, precision=0)
-        de = max(de, abs(e - E0))
-        dk = max(dk, float(np.max(np.abs(ka - K0))))
-    L.deinit()  # the single-molecule engine's device memory goes before the next server
-    return de, dk
 
 
 def main():
@@ -625,6 +748,8 @@ def main():
     ap.add_argument("--precision", type=int, default=1, help="1 = tensor-core form (default), 0 = FP64 plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 form's comparison timing")
+    ap.add_argument("--no-same-grid", action="store_true",
+                    help="skip the timing on the molecule's 40x194 grid (the reference arm's grid)")
     ap.add_argument("--mode", default="single", choices=["single", "batch", "serve", "forces"],
                     help="single = the headline 256-atom build; batch = the 512-molecule batch; "
                          "serve = Poisson-arrival serving of 64 resident molecules; "
@@ -636,6 +761,9 @@ def main():
     ap.add_argument("--inflight", type=int, default=32, help="builds on the GPU at once (batch / serve)")
     ap.add_argument("--service-precision", type=int, default=2,
                     help="form of the batch / serve modes: 0 FP64, 1 tensor core, 2 autotuned per molecule")
+    ap.add_argument("--no-oracle", action="store_true", help="batch / serve: skip the checks against the oracle")
+    ap.add_argument("--oracle-spots", type=int, default=3,
+                    help="serve: sampled requests checked against the oracle per arrival rate")
     ap.add_argument("--workload", default="cfg3", choices=["cfg3", "cfg2", "cfg2-open"],
                     help="cfg3 = the 256-atom headline workload; cfg2 / cfg2-open = the 64-atom closed- and "
                          "open-shell cases used for ncu captures")

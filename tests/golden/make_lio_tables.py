@@ -7,7 +7,7 @@ weights multiplied by 4 pi).
 
 Run from the repository root in a tree that holds the reference:
 
-    python tests/golden/make_lio_tables.py <reference root>
+    python tests/golden/make_lio_tables.py [<reference root>]   (default: beside the repository)
 
 The statements of that subroutine are literal assignments, `do` loops that fill
 weight ranges and whole-array scalings; this script evaluates exactly those
@@ -96,4 +96,5 @@ def main(ref_root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    here = os.path.dirname(os.path.abspath(__file__))
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(here, os.pardir, os.pardir, os.pardir, "reference"))
