@@ -608,56 +608,52 @@ def forces_mode(args):
 
 
 def batch_mode(args):
-    """Many-molecule batch: every build of the batch submitted at once to the
-    XC service (continuous batching over per-molecule streams); value = grid
-    points / wall second from first submission to last result (host arrays in
-    and out, so this is also the end-to-end figure)."""
+    """Many-molecule batch through lio_batch_* (include/lio_serve.h): the
+    molecules joined per functional class, one kernel launch per stage and
+    class, the classes concurrent. value = grid points / wall seconds of one
+    build of every molecule with host arrays in and out (density gather, device
+    work, Kohn-Sham scatter), so it is also the end-to-end figure; the same
+    batch in the plain FP64 form beside it."""
     from lio_b200 import serve as S
 
     wls = S.batch_molecules(args.batch)
-    srv = S.XCServer(precision=args.service_precision, max_inflight=args.inflight)
-    t0 = time.perf_counter()
-    mids = [srv.add(wl) for wl in wls]
-    grid_s = time.perf_counter() - t0
-    dens = {m: S.densities(srv.mols[m][0]) for m in mids}
-    pts = sum(srv.info(m)["points"] for m in mids)
-    for _ in range(max(1, args.warmup)):
-        res = S.run_all(srv, mids, dens)
-    srv.reset_stats()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        res = S.run_all(srv, mids, dens)
-    dt = (time.perf_counter() - t0) / args.steps
-    st = srv.stats()
-    forms = [srv.form(m) for m in mids]
-    srv.close()
-    tuned = {"fp64_ms_sum": sum(f[1] for f in forms), "tensor_ms_sum": sum(f[2] for f in forms)}
-    forms = [f[0] for f in forms]
-    # the same builds in the plain FP64 form: its throughput
-    ref = S.XCServer(precision=0, max_inflight=args.inflight)
-    rmids = [ref.add(wl) for wl in wls]
-    S.run_all(ref, rmids, {r: dens[m] for r, m in zip(rmids, mids)})
-    t0 = time.perf_counter()
-    S.run_all(ref, rmids, {r: dens[m] for r, m in zip(rmids, mids)})
-    dt0 = time.perf_counter() - t0
-    ref.close()
-    # every molecule's E_xc and Kohn-Sham matrix against the oracle (the reference's CPU g2g path on
-    # the same 194-point grid), serially on the host cores
-    errs = oracle_errors([(wl, res[m]) for wl, m in zip(wls, mids)]) if not args.no_oracle else None
+    dens = [S.densities(wl) for wl in wls]
+
+    def run(precision):
+        b = S.XCBatch(wls, precision=precision)
+        st = b.stats()
+        for _ in range(max(1, args.warmup)):
+            b.solve(dens)
+        dev = 0.0
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            _, _, _, ms = b.solve(dens)
+            dev += ms
+        dt = (time.perf_counter() - t0) / args.steps
+        E, Ka, _, _ = b.solve(dens)
+        res = [(float(E[i]), Ka[i].copy()) for i in range(len(wls))]
+        b.close()
+        return st, dt, dev / args.steps, res
+
+    st, dt, dev_ms, res = run(args.batch_precision)
+    st0, dt0, dev_ms0, _ = run(0)
+    pts = st["points"]
+    # every molecule's E_xc and Kohn-Sham matrix against the oracle (the reference's CPU g2g path on the
+    # same 194-point grid), serially on the host cores, after the timing
+    errs = oracle_errors(list(zip(wls, res))) if not args.no_oracle else None
     nlda = sum(1 for wl in wls if wl.iexch <= 3)
     return {"metric": METRIC, "value": pts / dt, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "i8-split/f64" if args.service_precision else "f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": "i8-split/f64" if args.batch_precision else "f64", "data": "synthetic",
             "mode": "batch",
             "config": {"workload": f"cfg4: {len(wls)} clusters, 3-40 atoms log-uniform (H:C:N:O 10:4:1:1), "
                                    f"30x194 grids, closed shell, {nlda} LDA-VWN / {len(wls) - nlda} PBE",
-                       "points": pts, "grid_build_s": round(grid_s, 2), "max_inflight": args.inflight,
-                       "peak_inflight": st["peak_inflight"], "evictions": st["evictions"],
-                       "forms": {"tensor": sum(1 for f in forms if f == 1), "fp64": sum(1 for f in forms if f == 0)},
-                       "autotune_device_ms_per_build": tuned,
-                       "service_precision": args.service_precision},
+                       "points": pts, "grid_build_s": round(st["build_s"], 2), "classes": st["classes"],
+                       "class_forms": st["forms"], "class_members": st["members"],
+                       "batch_precision": args.batch_precision},
+            "device_ms_per_step": dev_ms,
             "e2e": {"value": pts / dt, "unit": UNIT, "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
-            "fp64_plain": {"value": pts / dt0, "ms_per_step": dt0 * 1e3},
+            "fp64_plain": {"value": pts / dt0, "ms_per_step": dt0 * 1e3, "device_ms_per_step": dev_ms0},
             "oracle": errs}
 
 
@@ -762,6 +758,8 @@ def main():
     ap.add_argument("--service-precision", type=int, default=2,
                     help="form of the batch / serve modes: 0 FP64, 1 tensor core, 2 autotuned per molecule")
     ap.add_argument("--no-oracle", action="store_true", help="batch / serve: skip the checks against the oracle")
+    ap.add_argument("--batch-precision", type=int, default=1,
+                    help="batch: 0 FP64, 1 tensor core (classes it cannot run take FP64), 2 autotuned per class")
     ap.add_argument("--oracle-spots", type=int, default=3,
                     help="serve: sampled requests checked against the oracle per arrival rate")
     ap.add_argument("--workload", default="cfg3", choices=["cfg3", "cfg2", "cfg2-open"],

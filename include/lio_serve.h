@@ -113,6 +113,42 @@ int lio_srv_plan_admission(int n, const unsigned long long* footprint, const int
                            const unsigned long long* last_use, unsigned long long budget,
                            unsigned long long used, unsigned long long need, int* evict, int* nevict);
 
+/* ---- many molecules per launch --------------------------------------------
+ * No counterpart in the reference, whose CPU path runs the point groups of one
+ * molecule in one OpenMP loop (g2g/partition.cpp:441-511). A batch joins many
+ * molecules into one device layout per functional class (LDA or GGA, closed or
+ * open shell, one iexch): the point groups of all its molecules form one tile
+ * list, so each stage of an XC build (density operands, density contraction,
+ * functional, Kohn-Sham operands and contraction) is one kernel launch for the
+ * whole class, however small its molecules. Each group carries its molecule's
+ * packed-matrix dimension and offset; the densities of the molecules are read
+ * from, and their Kohn-Sham matrices added into, one concatenated vector per
+ * spin, and each molecule's E_xc is summed from its own groups' partials.
+ *
+ * lio_batch_create builds every molecule's grid and partition (host threads,
+ * Becke weights on the host) and uploads one engine per class to `device`;
+ * precision 0 FP64, 1 tensor core, 2 the faster of both per class (timed once).
+ * It returns NULL on failure (message in lio_batch_create_error).
+ * lio_batch_solve runs one XC build of every molecule: rho_a[i] (closed shell:
+ * the packed total density; open shell: alpha) and rho_b[i] (open shell: beta,
+ * else ignored) are molecule i's packed densities (doubled off-diagonals), its
+ * packed Kohn-Sham matrices are WRITTEN (=) into fock_a[i] / fock_b[i] and its
+ * E_xc into energies[i]; the classes run concurrently on their own streams.
+ * *device_ms (optional) receives the sum over classes of their device time.
+ * Returns 0, or a nonzero status with the message in lio_batch_last_error.
+ * lio_batch_stats writes the grid points of all molecules, the number of
+ * classes, the seconds the grids and uploads took and, per class (up to
+ * max_classes), its form (0 FP64, 1 tensor core) and molecule count. */
+typedef struct lio_batch lio_batch;
+lio_batch* lio_batch_create(int device, int nmol, const lio_molecule* mols, int precision);
+const char* lio_batch_create_error(void);
+int lio_batch_solve(lio_batch* b, const double* const* rho_a, const double* const* rho_b, double* const* fock_a,
+                    double* const* fock_b, double* energies, double* device_ms);
+const char* lio_batch_last_error(lio_batch* b);
+int lio_batch_stats(lio_batch* b, long long* points, int* nclasses, double* build_s, int max_classes, int* form,
+                    int* members);
+void lio_batch_destroy(lio_batch* b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -23,9 +23,9 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
-HOST_SRCS = ["partition.cpp", "g2g_abi.cpp", "serve.cpp"]
+HOST_SRCS = ["partition.cpp", "g2g_abi.cpp", "serve.cpp", "batch.cpp"]
 CUDA_SRCS = ["engine.cu", "tc_selftest.cu"]
-HEADERS = ["system.h", "partition.h", "engine.h", "xc_functionals.cuh", "umma.cuh", "density_tc.cuh", "fock_tc.cuh", "force_tc.cuh"]
+HEADERS = ["system.h", "partition.h", "engine.h", "molecule.h", "xc_functionals.cuh", "umma.cuh", "density_tc.cuh", "fock_tc.cuh", "force_tc.cuh"]
 
 CXXFLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-fopenmp", "-fvisibility=hidden",
             "-I" + os.path.join(CUDA_HOME, "include"),

@@ -209,7 +209,7 @@ __global__ void k_slice_density(const int2* __restrict__ tiles, const GroupDev* 
   if (i < G.m)
     for (int j = 0; j < G.m; j++) {
       const int gj = fg[j];
-      double v = P[packed_index(gi, gj, M)];
+      double v = P[G.pk_off + packed_index(gi, gj, G.pk_M)];
       if (gi != gj) v *= 0.5;
       amax = fmax(amax, fabs(v));
     }
@@ -229,7 +229,7 @@ __global__ void k_slice_density(const int2* __restrict__ tiles, const GroupDev* 
       double v = 0.0;
       if (i < G.m && j < G.m) {
         const int gj = fg[j];
-        v = P[packed_index(gi, gj, M)];
+        v = P[G.pk_off + packed_index(gi, gj, G.pk_M)];
         if (gi != gj) v *= 0.5;
       }
       digits_m(v, s42, lo[k], hi[k]);

@@ -73,6 +73,10 @@ struct GroupDev {
   long long fae_off;   // their per-row exponents (elements): nI x 128
   long long fbe_off;   // per-row exponents of f*F (elements): nJ x 32
   long long rad_off;   // radial sums of the tensor-core density (elements): per 128-point tile, shell, NR values
+  // the packed density / Kohn-Sham matrices the group reads and adds into: dimension pk_M, starting at
+  // element pk_off of the engine's vectors (a batch of molecules keeps one per molecule, one after the other)
+  int pk_M, pk_pad;
+  long long pk_off;
 };
 
 // Process-wide pinned host staging of the grid build (grow-only, one buffer per
@@ -334,7 +338,7 @@ __global__ void __launch_bounds__(256) k_density_fp64(const int4* __restrict__ t
       double v = 0.0;
       if (j < G.m && i < G.m) {
         const int gj = fg[j], gi = fg[i];
-        v = P[packed_index(gi, gj, M)];
+        v = P[G.pk_off + packed_index(gi, gj, G.pk_M)];
         if (gi != gj) v *= 0.5;
       }
       Bs[kk][ii] = v;
@@ -534,7 +538,7 @@ __global__ void __launch_bounds__(256) k_force_fp64(const int4* __restrict__ til
         double v = 0.0;
         if (j < G.m && i < G.m) {
           const int gj = fg[j], gi = fg[i];
-          v = (sp == 0 ? P_a : P_b)[packed_index(gi, gj, M)];
+          v = (sp == 0 ? P_a : P_b)[G.pk_off + packed_index(gi, gj, G.pk_M)];
           if (gi != gj) v *= 0.5;
         }
         Bs[sp][kk][ii] = v;
@@ -710,6 +714,18 @@ __global__ void k_sum_blocks(const double* __restrict__ in, int n, double* __res
   }
 }
 
+// E_xc of every molecule of a batch: block k sums the per-block partials of
+// its molecule, [seg[k].x, seg[k].y)
+__global__ void k_sum_segments(const double* __restrict__ in, const int2* __restrict__ seg,
+                               double* __restrict__ out) {
+  __shared__ double sh[32];
+  const int2 r = seg[blockIdx.x];
+  double v = 0.0;
+  for (int i = r.x + threadIdx.x; i < r.y; i += blockDim.x) v += in[i];
+  v = block_sum(v, sh);
+  if (threadIdx.x == 0) out[blockIdx.x] = v;
+}
+
 // ------------------------------------------------ Kohn-Sham update (FP64 GEMM)
 // Tile = (group, i tile, j tile) with i tile <= j tile; K_ij = sum_p F_ip f_p F_jp
 // for i <= j, scattered with FP64 atomics into the packed accumulator(s).
@@ -773,7 +789,7 @@ __global__ void __launch_bounds__(256) k_fock_fp64(const int4* __restrict__ tile
     for (int c = 0; c < 4; c++) {
       const int j = j0 + tx + 16 * c;
       if (j >= G.m || (t.y == t.z && i > j)) continue;
-      const long long o = packed_index(gi, fg[j], M);
+      const long long o = G.pk_off + packed_index(gi, fg[j], G.pk_M);
       atomicAdd(K_a + o, acc[0][r][c]);
       if (NS == 2) atomicAdd(K_b + o, acc[NS - 1][r][c]);
     }
@@ -826,6 +842,14 @@ struct DeviceEngine::Impl {
   DevBuf<int2> basis_tiles, func_tiles;
   DevBuf<int4> dens_tiles, fock_tiles;
   DevBuf<double> P_a, P_b, K_a, K_b, part_a, part_b, fac_a, fac_b, eblocks, energy;
+  size_t npacked = 0;  // elements of the packed matrices per spin (a batch: its molecules' together)
+  // a batch: per molecule the range of its energy partials, its E_xc (device, pinned copy)
+  int nmembers = 0;
+  DevBuf<int2> member_blocks;
+  DevBuf<double> member_energy;
+  std::vector<double> h_member_energy;
+  double* hME = nullptr;
+  size_t hme_elems = 0;
   // packed entries the groups touch (sorted); when they are at most half of the
   // packed matrix, host-array solves move only these (Pc, Kc: nspin x npairs)
   std::vector<long long> hpidx;
@@ -878,6 +902,9 @@ struct DeviceEngine::Impl {
     pinned_elems = 0;
     if (hE) cudaFreeHost(hE);
     if (hErr) cudaFreeHost(hErr);
+    if (hME) cudaFreeHost(hME);
+    hME = nullptr;
+    hme_elems = 0;
     hK = hE = nullptr;
     hErr = nullptr;
   }
@@ -1078,7 +1105,8 @@ int DeviceEngine::stage_times(double* ms, int max_stages, int* solves) const {
 }
 long long DeviceEngine::groups() const { return impl_->ngroups; }
 
-void DeviceEngine::upload(const System& sys, const Partition& part, const std::vector<char>* keep) {
+void DeviceEngine::upload(const System& sys, const Partition& part, const std::vector<char>* keep,
+                          const std::vector<BatchMember>* batch) {
   Impl* d = impl_.get();
   d->M = sys.M;
   d->natoms = sys.natoms;
@@ -1107,9 +1135,19 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
   int maxm = 0;
   const int NA = sys.lda ? 1 : 4;
   const int ngr = part.total_groups();
+  if (batch && keep) throw std::runtime_error("a batch of molecules is not sharded across devices");
+  size_t member = 0;                        // the batch member of group g
+  std::vector<int2> member_ft;              // per member: its range of energy-partial blocks
   for (int g = 0; g < ngr; g++) {
     if (keep && !(*keep)[g]) continue;  // another rank's group
     const int gdev = (int)gd.size();    // its index on this device
+    if (batch) {
+      while (member < batch->size() && g >= (*batch)[member].g_end) member++;
+      if (member >= batch->size() || g < (*batch)[member].g_begin)
+        throw std::runtime_error("batch members must cover the partition's groups in order");
+      if (member_ft.size() <= member) member_ft.resize(member + 1, make_int2(0, 0));
+    }
+    const BatchMember* bm = batch ? &(*batch)[member] : nullptr;
     const PointGroup& pg = part.group(g);
     GroupDev G{};
     G.npts = (int)pg.points.size();
@@ -1133,6 +1171,8 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
     G.fae_off = fae_off;
     G.fbe_off = fbe_off;
     G.rad_off = rad_off;
+    G.pk_M = bm ? bm->M : sys.M;
+    G.pk_off = bm ? bm->pk_off : 0;
     const int nI = (G.m + kFkRows - 1) / kFkRows, nJ = (G.m + kFkCols - 1) / kFkCols;
     for (int i = 0; i < nI * kFkRows; i++) farows.push_back({gdev, i});
     for (int j = 0; j < nJ * kFkCols; j++) fbrows.push_back({gdev, j});
@@ -1143,14 +1183,15 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
     src_group.push_back(g);  // its points are packed after this loop, all groups at once
     for (size_t i = 0; i < pg.funcs.size(); i++) {
       const int f = pg.funcs[i];
-      const int type = f < sys.s_funcs ? 0 : (f < sys.s_funcs + 3 * sys.p_funcs ? 1 : 2);
+      const int type = !sys.ftype.empty() ? sys.ftype[f]
+                                          : (f < sys.s_funcs ? 0 : (f < sys.s_funcs + 3 * sys.p_funcs ? 1 : 2));
       hsf.push_back(f);
       hst.push_back(type);
       hsffn.push_back((int)((long long)hfn.size() - G.fn_off));
       const int ncomp = type == 0 ? 1 : (type == 1 ? 3 : 6);
       const int c0 = type == 0 ? 0 : (type == 1 ? 1 : 4);
       for (int k = 0; k < ncomp; k++) {
-        hfn.push_back(f + k);
+        hfn.push_back(f + k - (bm ? bm->f_off : 0));  // its index in its molecule's packed matrices
         hfsh.push_back((int)i);
         hfat.push_back(sys.nuc[f]);
         const bool normed = type == 2 && (k == 0 || k == 2 || k == 5);
@@ -1158,7 +1199,9 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
       }
     }
     for (int b = 0; b < G.ldp / kBasisBlock + (G.ldp % kBasisBlock ? 1 : 0); b++) btiles.push_back({gdev, b});
+    if (bm && member_ft[member].y == 0) member_ft[member] = make_int2((int)ftiles.size(), (int)ftiles.size());
     for (int b = 0; b < (G.ldp + kFuncBlock - 1) / kFuncBlock; b++) ftiles.push_back({gdev, b});
+    if (bm) member_ft[member].y = (int)ftiles.size();
     for (int pt = 0; pt < G.ldp / kTile; pt++)
       for (int ft = 0; ft < G.nft; ft++) dtiles.push_back({gdev, pt, ft, 0});
     for (int it = 0; it < G.nft; it++)
@@ -1271,8 +1314,30 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
   d->dens_tiles.upload(dtiles);
   d->fock_tiles.upload(ktiles);
 
-  const size_t npacked = (size_t)sys.M * (sys.M + 1) / 2;
-  {
+  size_t npacked = (size_t)sys.M * (sys.M + 1) / 2;
+  if (batch) {
+    npacked = 0;
+    for (const BatchMember& b : *batch) {
+      if (b.pk_off != (long long)npacked) throw std::runtime_error("batch members' packed matrices must follow each other");
+      npacked += (size_t)b.M * (b.M + 1) / 2;
+    }
+  }
+  d->npacked = npacked;
+  d->nmembers = batch ? (int)batch->size() : 0;
+  if (batch) {
+    member_ft.resize(batch->size(), make_int2(0, 0));
+    d->member_blocks.upload(member_ft);
+    d->member_energy.alloc(batch->size());
+    d->h_member_energy.assign(batch->size(), 0.0);
+  }
+  if (batch) {
+    // every molecule's whole matrices travel (small molecules' groups touch most of them)
+    d->hpidx.clear();
+    d->compact = false;
+    d->pidx.free();
+    d->Pc.free();
+    d->Kc.free();
+  } else {
     // the packed entries this engine's groups touch (fn_glob is increasing within a group)
     std::vector<unsigned char> touched(npacked, 0);
     const long long Ml = sys.M;
@@ -1326,6 +1391,12 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
     LIO_CUDA(cudaMallocHost(&d->hE, sizeof(double)));
     LIO_CUDA(cudaMallocHost(&d->hErr, sizeof(int)));
     d->pinned_elems = pinned;
+  }
+  if (batch && d->hme_elems < batch->size()) {
+    if (d->hME) cudaFreeHost(d->hME);
+    d->hME = nullptr;
+    LIO_CUDA(cudaMallocHost(&d->hME, batch->size() * sizeof(double)));
+    d->hme_elems = batch->size();
   }
   *d->hErr = 0;
 
@@ -1438,7 +1509,7 @@ int DeviceEngine::run_kernels(bool compute_rmm, bool ext) {
   Impl* d = impl_.get();
   double* Ka = ext ? d->ext_ka : d->K_a.p;
   double* Kb = ext ? d->ext_kb : d->K_b.p;
-  const size_t npacked = (size_t)d->M * (d->M + 1) / 2;
+  const size_t npacked = d->npacked;
   cudaStream_t st = d->stream;
   int launches = 0;
   const unsigned nd = (unsigned)d->dens_tiles.n, nf = (unsigned)d->func_tiles.n,
@@ -1498,6 +1569,11 @@ int DeviceEngine::run_kernels(bool compute_rmm, bool ext) {
   k_sum_blocks<<<1, 1024, 0, st>>>(d->eblocks.p, (int)nf, ext ? d->ext_e : d->energy.p, ext ? 1 : 0);
   LIO_CUDA(cudaGetLastError());
   launches += 2;
+  if (d->nmembers > 0) {  // a batch: each molecule's E_xc as well
+    k_sum_segments<<<(unsigned)d->nmembers, 256, 0, st>>>(d->eblocks.p, d->member_blocks.p, d->member_energy.p);
+    LIO_CUDA(cudaGetLastError());
+    launches++;
+  }
   d->mark(3);
   if (compute_rmm) {
     if (!ext) {  // an external accumulator is zeroed by its owner, once for all shards
@@ -1552,7 +1628,7 @@ void DeviceEngine::set_graphs_dirty() { impl_->drop_graph(); }
 
 void DeviceEngine::copy_results(double* d_fock_a, double* d_fock_b, double* d_energy) {
   Impl* d = impl_.get();
-  const size_t npacked = (size_t)d->M * (d->M + 1) / 2;
+  const size_t npacked = d->npacked;
   if (d_fock_a)
     LIO_CUDA(cudaMemcpyAsync(d_fock_a, d->K_a.p, npacked * sizeof(double), cudaMemcpyDeviceToDevice, d->stream));
   if (d_fock_b && d->open)
@@ -1697,7 +1773,7 @@ size_t DeviceEngine::estimate_device_bytes(const System& sys, const Partition& p
 
 void DeviceEngine::enqueue(const SolveRequest& req) {
   Impl* d = impl_.get();
-  const size_t npacked = (size_t)d->M * (d->M + 1) / 2;
+  const size_t npacked = d->npacked;
   d->enqueued = false;
   if (d->ngroups == 0) return;
   cudaStream_t st = d->stream;
@@ -1780,6 +1856,9 @@ void DeviceEngine::enqueue(const SolveRequest& req) {
   if (!req.resident) {
     const int nspin = d->open ? 2 : 1;
     LIO_CUDA(cudaMemcpyAsync(d->hE, d->energy.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (d->nmembers > 0)
+      LIO_CUDA(cudaMemcpyAsync(d->hME, d->member_energy.p, (size_t)d->nmembers * sizeof(double),
+                               cudaMemcpyDeviceToHost, st));
     if (tc) LIO_CUDA(cudaMemcpyAsync(d->hErr, d->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     d->nchunks = 0;
     d->last_d2h = (long long)sizeof(double);  // the energy
@@ -1832,7 +1911,7 @@ SolveResult DeviceEngine::finish(const SolveRequest& req) {
   if (!d->enqueued) return res;
   d->enqueued = false;
   if (req.resident) return res;
-  const size_t npacked = (size_t)d->M * (d->M + 1) / 2;
+  const size_t npacked = d->npacked;
   // the energy and the error flag are downloaded before the first Kohn-Sham piece
   LIO_CUDA(cudaEventSynchronize(req.compute_rmm && d->nchunks > 0 ? d->kev[0] : d->ev1));
   if (precision_ == Precision::TensorCore && *d->hErr) {
@@ -1876,8 +1955,17 @@ SolveResult DeviceEngine::finish(const SolveRequest& req) {
   LIO_CUDA(cudaEventElapsedTime(&ms, d->ev0, d->ev1));
   res.energy = *d->hE;
   res.device_ms = ms;
+  for (int k = 0; k < d->nmembers; k++) d->h_member_energy[k] = d->hME[k];
   return res;
 }
+
+int DeviceEngine::batch_energies(double* out) const {
+  const Impl* d = impl_.get();
+  for (int k = 0; k < d->nmembers; k++) out[k] = d->h_member_energy[k];
+  return d->nmembers;
+}
+
+size_t DeviceEngine::packed_size() const { return impl_->npacked; }
 
 SolveResult DeviceEngine::solve(const SolveRequest& req) {
   enqueue(req);

@@ -36,6 +36,17 @@ struct SolveResult {
   double device_ms = 0.0;
 };
 
+// One molecule of a batch uploaded as one system (DeviceEngine::upload with
+// `batch`): its functions are [f_off, f_off + M) of the joined system's, its
+// packed density and Kohn-Sham matrices occupy [pk_off, pk_off + M(M+1)/2) of
+// the engine's vectors, and its point groups are [g_begin, g_end) of the
+// joined partition (each molecule's groups one after the other).
+struct BatchMember {
+  int f_off = 0, M = 0;
+  long long pk_off = 0;
+  int g_begin = 0, g_end = 0;
+};
+
 class DeviceEngine {
  public:
   DeviceEngine();
@@ -46,7 +57,16 @@ class DeviceEngine {
   // Uploads basis parameters, points and function lists and evaluates the
   // basis values; with `keep`, only the groups g with (*keep)[g] (this rank's
   // shard of a multi-GPU build).
-  void upload(const System& sys, const Partition& part, const std::vector<char>* keep = nullptr);
+  // With `batch`, the system and partition join several molecules (see
+  // BatchMember): one set of kernel launches per stage covers all of them, the
+  // density and Kohn-Sham vectors of solve() are the molecules' packed
+  // matrices one after the other, and batch_energies() gives each one's E_xc.
+  void upload(const System& sys, const Partition& part, const std::vector<char>* keep = nullptr,
+              const std::vector<BatchMember>* batch = nullptr);
+  // E_xc of every batch member in the last host-array solve; returns their number
+  int batch_energies(double* out) const;
+  // elements of the packed density / Kohn-Sham vectors per spin
+  size_t packed_size() const;
   // One XC build: enqueue() puts all of its device work on the engine's stream
   // (density upload unless resident, the kernels, result download into pinned
   // buffers) and returns; ready() polls it; finish() waits for it and delivers

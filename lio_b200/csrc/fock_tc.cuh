@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
             // each level converted on its own (the reduction runs over all the
             // group's points, so level pairs need not fit int32), one rounding
             const double v = level_sum(lv, c, false) * pow2(ea + bexp[G.fbe_off + j] - 7 * (kSlices + 1));
-            atomicAdd(K + packed_index(gi, fn_glob[G.fn_off + j], M), v);
+            atomicAdd(K + G.pk_off + packed_index(gi, fn_glob[G.fn_off + j], G.pk_M), v);
           }
         }
       }

@@ -450,8 +450,8 @@ void lio_server::loop() {
   cv_done.notify_all();
 }
 
-namespace {
-lio::System to_system(const lio_molecule* d) {
+namespace lio {
+System system_from_molecule(const lio_molecule* d) {
   if (d->natoms <= 0 || d->M <= 0) throw std::runtime_error("empty molecule");
   if (d->iexch < 1 || d->iexch > 9) throw std::runtime_error("iexch must be 1-3 (LDA) or 4-9 (GGA)");
   if (d->s_funcs + 3 * d->p_funcs + 6 * d->d_funcs != d->M) throw std::runtime_error("s/p/d counts do not add up to M");
@@ -497,7 +497,7 @@ lio::System to_system(const lio_molecule* d) {
   y.open = d->open != 0;
   return y;
 }
-}  // namespace
+}  // namespace lio
 
 extern "C" {
 
@@ -543,7 +543,7 @@ int lio_srv_add_molecule(lio_server* srv, const lio_molecule* mol) {
   if (!srv || !mol) return -1;
   try {
     std::unique_ptr<Molecule> m(new Molecule());
-    m->sys = to_system(mol);
+    m->sys = lio::system_from_molecule(mol);
     m->ang.x.assign(mol->ang_x, mol->ang_x + mol->nang);
     m->ang.y.assign(mol->ang_y, mol->ang_y + mol->nang);
     m->ang.z.assign(mol->ang_z, mol->ang_z + mol->nang);

@@ -39,6 +39,10 @@ struct System {
 
   int M = 0;                 // total (expanded) functions
   int s_funcs = 0, p_funcs = 0, d_funcs = 0;  // simple counts
+  // shell type of every (expanded) function (0 s, 1 p, 2 d); empty: from the
+  // counts above (all s, then p, then d). A batch of molecules joined into one
+  // system keeps each molecule's own order, so it sets these explicitly.
+  std::vector<int8_t> ftype;
   std::vector<int> nuc;      // per expanded function, 0-based atom
   std::vector<int> ncont;    // per expanded function
   std::vector<double> a, c;  // per expanded function x kMaxContractions (row-major)

@@ -156,6 +156,77 @@ class XCServer:
             pass
 
 
+class XCBatch:
+    """One lio_batch: many molecules joined per functional class, each XC build
+    stage one kernel launch per class (include/lio_serve.h)."""
+
+    def __init__(self, wls: list, device: int = 0, precision: int = 1, path: str = DEFAULT_LIB):
+        L = C.CDLL(path)
+        L.lio_batch_create.restype = C.c_void_p
+        L.lio_batch_create.argtypes = [C.c_int, C.c_int, C.POINTER(LioMolecule), C.c_int]
+        L.lio_batch_create_error.restype = C.c_char_p
+        L.lio_batch_last_error.restype = C.c_char_p
+        L.lio_batch_last_error.argtypes = [C.c_void_p]
+        L.lio_batch_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.lio_batch_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_int),
+                                      C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.lio_batch_destroy.argtypes = [C.c_void_p]
+        self.L = L
+        self.wls = list(wls)
+        structs, self._keep = [], []
+        for wl in self.wls:
+            st, keep = molecule_struct(wl)
+            structs.append(st)
+            self._keep.append(keep)
+        arr = (LioMolecule * len(structs))(*structs)
+        self._arr = arr
+        self.h = L.lio_batch_create(device, len(structs), arr, precision)
+        if not self.h:
+            raise RuntimeError(L.lio_batch_create_error().decode(errors="replace"))
+        n = len(self.wls)
+        npk = [wl.basis.M * (wl.basis.M + 1) // 2 for wl in self.wls]
+        self.fock_a = [np.zeros(k) for k in npk]
+        self.fock_b = [np.zeros(k) if wl.open_shell else None for k, wl in zip(npk, self.wls)]
+        self.energies = np.zeros(n)
+        self._pa = (C.c_void_p * n)(*[f.ctypes.data for f in self.fock_a])
+        self._pb = (C.c_void_p * n)(*[(f.ctypes.data if f is not None else None) for f in self.fock_b])
+
+    def stats(self) -> dict:
+        pts, ncl, bs = C.c_longlong(0), C.c_int(0), C.c_double(0)
+        form, mem = (C.c_int * 16)(), (C.c_int * 16)()
+        self.L.lio_batch_stats(self.h, C.byref(pts), C.byref(ncl), C.byref(bs), 16, form, mem)
+        return dict(points=pts.value, classes=ncl.value, build_s=bs.value,
+                    forms=[form[k] for k in range(min(16, ncl.value))],
+                    members=[mem[k] for k in range(min(16, ncl.value))])
+
+    def solve(self, dens: list):
+        """dens[i] = (rho_a, rho_b or None): molecule i's packed densities. Returns
+        (energies, Kohn-Sham alpha list, beta list, device ms); the Kohn-Sham
+        arrays are written (=) and reused by the next call."""
+        keep = [(np.ascontiguousarray(a, dtype=np.float64),
+                 None if b is None else np.ascontiguousarray(b, dtype=np.float64)) for a, b in dens]
+        ra = (C.c_void_p * len(keep))(*[a.ctypes.data for a, _ in keep])
+        rb = (C.c_void_p * len(keep))(*[(b.ctypes.data if b is not None else None) for _, b in keep])
+        ms = C.c_double(0)
+        rc = self.L.lio_batch_solve(self.h, ra, rb, self._pa, self._pb,
+                                    self.energies.ctypes.data_as(C.POINTER(C.c_double)), C.byref(ms))
+        if rc:
+            raise RuntimeError(self.L.lio_batch_last_error(self.h).decode(errors="replace"))
+        return self.energies, self.fock_a, self.fock_b, ms.value
+
+    def close(self):
+        if self.h:
+            self.L.lio_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def densities(wl: W.Workload):
     return (wl.rho_a, wl.rho_b) if wl.open_shell else (wl.rho, None)
 
