@@ -1488,15 +1488,25 @@ void DeviceEngine::prepare_tensor_core() {
     if (need + 256 > (size_t)optin)
       throw std::runtime_error("tensor-core density: a group with " + std::to_string(cap) +
                                " functions needs more shared memory than a block can have; use precision 0");
-    // only the variant this system runs (the others may not fit at this cap)
+    // only the variant this system runs (the others may not fit at this cap), and
+    // only ever raised: the limit belongs to the kernel, which every engine of the
+    // process shares, and an engine with larger groups may launch it later
+    auto raise_limit = [&](const void* fn) {
+      static std::mutex mu;
+      std::lock_guard<std::mutex> lock(mu);
+      cudaFuncAttributes fa;
+      LIO_CUDA(cudaFuncGetAttributes(&fa, fn));
+      if ((int)need > fa.maxDynamicSharedSizeBytes)
+        LIO_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+    };
     if (d->lda && d->open)
-      LIO_CUDA(cudaFuncSetAttribute(k_density_tc<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+      raise_limit((const void*)k_density_tc<false, 2>);
     else if (d->lda)
-      LIO_CUDA(cudaFuncSetAttribute(k_density_tc<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+      raise_limit((const void*)k_density_tc<false, 1>);
     else if (d->open)
-      LIO_CUDA(cudaFuncSetAttribute(k_density_tc<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+      raise_limit((const void*)k_density_tc<true, 2>);
     else
-      LIO_CUDA(cudaFuncSetAttribute(k_density_tc<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+      raise_limit((const void*)k_density_tc<true, 1>);
   }
   d->tc_ready = true;
 }

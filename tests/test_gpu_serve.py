@@ -136,3 +136,22 @@ def test_memory_taken_by_another_user_shrinks_the_budget():
         srv.close()
         del hog
         torch.cuda.empty_cache()
+
+
+def test_large_molecule_after_smaller_ones_in_the_tensor_core_form():
+    """Engines of one process share each kernel and its shared-memory limit: a
+    molecule with larger point groups built again after smaller molecules were
+    prepared still launches (the limit is only ever raised)."""
+    big, small = W.small_workload(30, 111, 9, False), W.small_workload(4, 112, 9, False)
+    srv = S.XCServer(precision=1, max_inflight=4)
+    try:
+        mb = srv.add(big)
+        e1, k1, _, _ = srv.wait(srv.submit(mb, big.rho), mb)
+        ms = srv.add(small)
+        srv.wait(srv.submit(ms, small.rho), ms)
+        e2, k2, _, _ = srv.wait(srv.submit(mb, big.rho), mb)
+        assert abs(e2 - e1) <= MIX_E and np.max(np.abs(k2 - k1)) <= MIX_K
+        E_ref, K_ref, _ = H.oracle_result(big)
+        assert abs(e2 - E_ref) <= H.E_TOL and np.max(np.abs(k2 - K_ref)) <= H.K_TOL
+    finally:
+        srv.close()
