@@ -4,8 +4,24 @@
 // (g2g/init.cpp:27-33). Every entry point catches all exceptions: failures are
 // recorded in a sticky status (g2g_last_error_) and, at verbose > 0, printed;
 // nothing is thrown across the boundary and nothing calls exit().
+//
+// Linked beside the reference's library: lioamber also calls the reference's
+// analytic-integral entry points (aint_*: the Coulomb fit and the QM/MM
+// integrals, g2g/analytic_integral/aint_init.cpp), whose code reads the state
+// the reference's own g2g_parameter_init_ and g2g_reload_atom_positions_ fill
+// (atom positions, basis, density and Fock pointers). When this library is
+// linked ahead of the reference's, the state-setting entry points here
+// (g2g_init_, g2g_set_options_, g2g_parameter_init_,
+// g2g_reload_atom_positions_, g2g_new_grid_, g2g_deinit_) first pass the call
+// on to the next definition in the process's symbol search order (the
+// reference's), so that state is kept exactly as before; the XC build,
+// g2g_solve_groups_, is this library's alone. LIO_B200_NO_FORWARD set in the
+// environment turns the passing on off.
+#include <dlfcn.h>
+
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -214,6 +230,22 @@ void build_grid(unsigned grid_type) {
   s.grid_phase_ms[2] = s.last_grid_ms - t_up;
 }
 
+// The definition of `name` that follows this library in the symbol search
+// order (a g2g linked after it), or null (none, or passing on turned off).
+template <class F>
+F next_definition(const char* name, F self) {
+  if (std::getenv("LIO_B200_NO_FORWARD")) return nullptr;
+  F p = reinterpret_cast<F>(dlsym(RTLD_NEXT, name));
+  return p == self ? nullptr : p;
+}
+// Calls the next definition of the enclosing entry point `name` with the same
+// arguments; a failure there is recorded like one of this library's own.
+#define LIO_PASS_ON(name, ...)                                                        \
+  do {                                                                                \
+    static const auto next_ = next_definition(#name, &name);                          \
+    if (next_) guarded(#name " (passed on to the next g2g)", [&] { next_(__VA_ARGS__); }); \
+  } while (0)
+
 // ---- Fortran-named timers (g2g/timer.cpp:117-296): host wall clock
 struct NamedTimer {
   double total = 0.0;
@@ -243,6 +275,7 @@ double timer_pause(const char* n, unsigned len) {
 extern "C" {
 
 void g2g_init_(void) {
+  LIO_PASS_ON(g2g_init_);
   guarded("g2g_init_", [] {
     if (!lio::DeviceEngine::available()) throw std::runtime_error("no CUDA device visible");
     if (!st().engine) st().engine.reset(new lio::DeviceEngine());
@@ -251,6 +284,7 @@ void g2g_init_(void) {
 
 void g2g_set_options_(double* fgm, double* lcs, double* sr, bool* aaf, bool* eai, bool* rzw, unsigned* mppc,
                       unsigned* mfe, unsigned* time, unsigned* verbose) {
+  LIO_PASS_ON(g2g_set_options_, fgm, lcs, sr, aaf, eai, rzw, mppc, mfe, time, verbose);
   Options& o = st().opt;
   o.free_global_memory = *fgm;
   o.little_cube_size = *lcs;
@@ -273,6 +307,9 @@ void g2g_parameter_init_(const unsigned* norm, const unsigned* natom, const unsi
                          const unsigned* Iexch, double* e, double* e2, double* e3, double* wang,
                          double* wang2, double* wang3, bool* use_libxc, const unsigned* ex_functional_id,
                          const unsigned* ec_functional_id) {
+  LIO_PASS_ON(g2g_parameter_init_, norm, natom, max_atoms, ngaussians, r, Rm, Iz, Nr, Nr2, Nuc, M, ncont, nshell, c,
+              a, rho_vec, fock_vec, fockb_vec, rhoalpha, rhobeta, nco, OPEN, nunp, nopt, Iexch, e, e2, e3, wang, wang2,
+              wang3, use_libxc, ex_functional_id, ec_functional_id);
   guarded("g2g_parameter_init_", [&] {
     State& s = st();
     BoundArrays& b = s.arr;
@@ -341,10 +378,12 @@ void g2g_set_angular_grid_(const unsigned* grid_type, const unsigned* npoints, c
 }
 
 void g2g_reload_atom_positions_(const unsigned* grid_type) {
+  LIO_PASS_ON(g2g_reload_atom_positions_, grid_type);
   guarded("g2g_reload_atom_positions_", [&] { build_grid(*grid_type); });
 }
 
 void g2g_new_grid_(const unsigned* grid_type) {
+  LIO_PASS_ON(g2g_new_grid_, grid_type);
   guarded("g2g_new_grid_", [&] {
     if ((int)*grid_type != st().grid_type) build_grid(*grid_type);
   });
@@ -521,6 +560,7 @@ int g2g_selftest_bounded_wait_(const unsigned* polls, double* ms) {
 }
 
 void g2g_deinit_(void) {
+  LIO_PASS_ON(g2g_deinit_);
   guarded("g2g_deinit_", [] {
     State& s = st();
     s.part.cubes.clear();

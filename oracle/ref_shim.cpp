@@ -84,4 +84,8 @@ long long ref_group_cost(int g) {
 }
 
 int ref_cpu_threads(void) { return G2G::cpu_threads; }
+
+// atoms the reference's g2g_parameter_init_ recorded (the state its analytic
+// integrals read), for the link test of the drop-in
+int ref_bound_atoms(void) { return (int)G2G::fortran_vars.atoms; }
 }
