@@ -88,11 +88,14 @@ struct PinnedStaging {
   std::mutex m;
   void* host = nullptr;
   size_t bytes = 0;
+  // grows with 1/8 headroom: pinning is slow (~1 ms per 2-3 MB), and the next
+  // geometry of a molecule in motion usually has a few more points
   void reserve(size_t need) {
     if (bytes >= need) return;
     if (host) cudaFreeHost(host);
     host = nullptr;
     bytes = 0;
+    need += need / 8;
     const cudaError_t e = cudaMallocHost(&host, need);
     if (e != cudaSuccess) {
       cudaGetLastError();
@@ -111,6 +114,29 @@ PinnedStaging& point_staging() {  // the point arrays of an engine's upload
   static PinnedStaging* w = new PinnedStaging;
   return *w;
 }
+
+// Per device: a non-blocking stream for the grid build's host-to-device copies,
+// which then overlap host work (the legacy stream's synchronous copies of other
+// arrays do not wait for it). Never destroyed.
+cudaStream_t copy_stream() {
+  static std::mutex mu;
+  static cudaStream_t streams[64] = {};
+  int dev = 0;
+  LIO_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) throw std::runtime_error("device ordinal out of range for the copy stream");
+  std::lock_guard<std::mutex> lock(mu);
+  if (!streams[dev]) LIO_CUDA(cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking));
+  return streams[dev];
+}
+
+// Waits for a copy stream when leaving a scope, normally or by an exception,
+// so pinned staging is never reused, nor device buffers freed, under a copy.
+struct StreamDrain {
+  cudaStream_t s;
+  ~StreamDrain() {
+    if (cudaStreamSynchronize(s) != cudaSuccess) cudaGetLastError();
+  }
+};
 
 // device bytes held by every DevBuf of the process (footprint accounting)
 std::atomic<long long> g_devbuf_bytes{0};
@@ -415,45 +441,60 @@ __global__ void __launch_bounds__(256) k_density_fp64(const int4* __restrict__ t
 // (g2g/cpu/weight.cpp:13-112), in the operation order of the host code
 // (partition.cpp) and with every FP64 operation explicitly rounded (no fused
 // multiply-add), so the factors equal the host's, and the reference's, bit
-// for bit. The host multiplies each point's weight by its factor.
+// for bit. Two values the host code recomputes in its inner loop are computed
+// once instead, by the same operations: the size adjustment a_jk =
+// x / (x^2 - 1), x = (rm_j / rm_k - 1) / (rm_j / rm_k + 1), per atom pair
+// (becke_pair_table, three divisions out of every step), and the point's
+// distance to each nucleus of its group (a per-thread cache, one square root
+// per nucleus instead of one per pair). The host multiplies each point's
+// weight by its factor.
 __device__ __forceinline__ double len3_rn(double x, double y, double z) {
   return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
 }
 
-__device__ __forceinline__ double becke_step_rn(double u, double rm_j, double rm_k) {
-  double x = __ddiv_rn(rm_j, rm_k);
-  x = __ddiv_rn(__dsub_rn(x, 1.0), __dadd_rn(x, 1.0));
-  u = __dadd_rn(u, __dmul_rn(__ddiv_rn(x, __dsub_rn(__dmul_rn(x, x), 1.0)), __dsub_rn(1.0, __dmul_rn(u, u))));
+// s(u) with the pair's size adjustment a_jk (g2g/cpu/weight.cpp:40-48)
+__device__ __forceinline__ double becke_step_rn(double u, double a_jk) {
+  u = __dadd_rn(u, __dmul_rn(a_jk, __dsub_rn(1.0, __dmul_rn(u, u))));
 #pragma unroll
   for (int it = 0; it < 3; it++) u = __dsub_rn(__dmul_rn(1.5, u), __dmul_rn(0.5, __dmul_rn(__dmul_rn(u, u), u)));
   return __dmul_rn(0.5, __dsub_rn(1.0, u));
 }
 
+constexpr int kBeckeCache = 64;  // nuclei whose distances a thread keeps (more: recomputed per pair)
+
 __global__ void k_becke_weights(const double* __restrict__ px, const double* __restrict__ py,
                                 const double* __restrict__ pz, const int* __restrict__ patom,
-                                const int* __restrict__ pgroup, long long n, const int* __restrict__ nuc_off,
+                                const int* __restrict__ pgroup, long long i0, long long n,
+                                const int* __restrict__ nuc_off,
                                 const int* __restrict__ nucs, const double* __restrict__ ax,
                                 const double* __restrict__ ay, const double* __restrict__ az,
-                                const double* __restrict__ rm, const double* __restrict__ adist, int natoms,
+                                const double* __restrict__ pair_a, const double* __restrict__ adist, int natoms,
                                 double* __restrict__ factor) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long i = i0 + blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double x = px[i], y = py[i], z = pz[i];
   const int atom = patom[i], g = pgroup[i];
   const int* nl = nucs + nuc_off[g];
   const int nn = nuc_off[g + 1] - nuc_off[g];
+  const bool cached = nn <= kBeckeCache;
+  double dc[kBeckeCache];
+  auto dist_to = [&](int a) { return len3_rn(__dsub_rn(x, ax[a]), __dsub_rn(y, ay[a]), __dsub_rn(z, az[a])); };
+  if (cached)
+    for (int k = 0; k < nn; ++k) dc[k] = dist_to(nl[k]);
+  auto dist_k = [&](int k) { return cached ? dc[k] : dist_to(nl[k]); };
   double P_total = 0.0, P_atom = 0.0;
   bool own_found = false;
   for (int j = 0; j < nn; ++j) {
     double P_curr = 1.0;
     const int aj = nl[j];
-    const double dj = len3_rn(__dsub_rn(x, ax[aj]), __dsub_rn(y, ay[aj]), __dsub_rn(z, az[aj]));
+    const double dj = dist_k(j);
+    const double* aj_dist = adist + (long long)aj * natoms;
+    const double* aj_pair = pair_a + (long long)aj * natoms;
     for (int k = 0; k < nn; ++k) {
       const int ak = nl[k];
       if (ak == aj) continue;
-      const double u = __ddiv_rn(__dsub_rn(dj, len3_rn(__dsub_rn(x, ax[ak]), __dsub_rn(y, ay[ak]), __dsub_rn(z, az[ak]))),
-                                 adist[(long long)aj * natoms + ak]);
-      P_curr = __dmul_rn(P_curr, becke_step_rn(u, rm[aj], rm[ak]));
+      const double u = __ddiv_rn(__dsub_rn(dj, dist_k(k)), aj_dist[ak]);
+      P_curr = __dmul_rn(P_curr, becke_step_rn(u, aj_pair[ak]));
       if (P_curr == 0.0) break;
     }
     if (aj == atom) {
@@ -465,12 +506,13 @@ __global__ void k_becke_weights(const double* __restrict__ px, const double* __r
   }
   if (!own_found) {  // the point's own atom is not among the group's nuclei
     P_atom = 1.0;
-    const double da = len3_rn(__dsub_rn(x, ax[atom]), __dsub_rn(y, ay[atom]), __dsub_rn(z, az[atom]));
+    const double da = dist_to(atom);
+    const double* at_dist = adist + (long long)atom * natoms;
+    const double* at_pair = pair_a + (long long)atom * natoms;
     for (int k = 0; k < nn; ++k) {
       const int ak = nl[k];
-      const double u = __ddiv_rn(__dsub_rn(da, len3_rn(__dsub_rn(x, ax[ak]), __dsub_rn(y, ay[ak]), __dsub_rn(z, az[ak]))),
-                                 adist[(long long)atom * natoms + ak]);
-      P_atom = __dmul_rn(P_atom, becke_step_rn(u, rm[atom], rm[ak]));
+      const double u = __ddiv_rn(__dsub_rn(da, dist_k(k)), at_dist[ak]);
+      P_atom = __dmul_rn(P_atom, becke_step_rn(u, at_pair[ak]));
       if (P_atom == 0.0) break;
     }
   }
@@ -993,7 +1035,7 @@ namespace {
 size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 }  // namespace
 
-void DeviceEngine::becke_weights(const System& sys, const std::vector<PointGroup*>& groups) {
+void DeviceEngine::becke_weights(const System& sys, const std::vector<PointGroup*>& groups, bool drop_zero) {
   const long long ng = (long long)groups.size();
   std::vector<long long> first(ng + 1, 0);  // first point of each group in the flat arrays
   for (long long gi = 0; gi < ng; gi++) first[gi + 1] = first[gi] + (long long)groups[gi]->points.size();
@@ -1012,8 +1054,8 @@ void DeviceEngine::becke_weights(const System& sys, const std::vector<PointGroup
   const size_t o_atom = o_f + align256(n * 8), o_group = o_atom + align256(n * 4);
   const size_t o_off = o_group + align256(n * 4), o_nucs = o_off + align256(hoff.size() * 4);
   const size_t o_ax = o_nucs + align256(std::max<size_t>(hnucs.size(), 1) * 4);
-  const size_t o_ay = o_ax + align256(na * 8), o_az = o_ay + align256(na * 8), o_rm = o_az + align256(na * 8);
-  const size_t o_dist = o_rm + align256(na * 8), total = o_dist + align256(na * na * 8);
+  const size_t o_ay = o_ax + align256(na * 8), o_az = o_ay + align256(na * 8), o_pair = o_az + align256(na * 8);
+  const size_t o_dist = o_pair + align256(na * na * 8), total = o_dist + align256(na * na * 8);
   PinnedStaging& ws = weights_staging();
   std::lock_guard<std::mutex> lock(ws.m);  // one grid build at a time uses the staging
   ws.reserve(total);
@@ -1024,24 +1066,12 @@ void DeviceEngine::becke_weights(const System& sys, const std::vector<PointGroup
   double* hf = reinterpret_cast<double*>(h + o_f);
   int* hatom = reinterpret_cast<int*>(h + o_atom);
   int* hgroup = reinterpret_cast<int*>(h + o_group);
-#pragma omp parallel for schedule(dynamic, 4)
-  for (long long gi = 0; gi < ng; gi++) {
-    long long k = first[gi];
-    for (const GridPoint& p : groups[gi]->points) {
-      hx[k] = p.x;
-      hy[k] = p.y;
-      hz[k] = p.z;
-      hatom[k] = p.atom;
-      hgroup[k] = (int)gi;
-      k++;
-    }
-  }
   std::memcpy(h + o_off, hoff.data(), hoff.size() * 4);
   if (!hnucs.empty()) std::memcpy(h + o_nucs, hnucs.data(), hnucs.size() * 4);
   std::memcpy(h + o_ax, sys.ax.data(), na * 8);
   std::memcpy(h + o_ay, sys.ay.data(), na * 8);
   std::memcpy(h + o_az, sys.az.data(), na * 8);
-  std::memcpy(h + o_rm, sys.rm.data(), na * 8);
+  becke_pair_table(sys, reinterpret_cast<double*>(h + o_pair));
   std::memcpy(h + o_dist, sys.atom_dist.data(), na * na * 8);
   // the device block is kept per device too (grow-only, never freed): no
   // cudaMalloc / cudaFree of ~50 bytes per point on every geometry
@@ -1052,23 +1082,77 @@ void DeviceEngine::becke_weights(const System& sys, const std::vector<PointGroup
   if (!blocks[dev]) blocks[dev] = new DevBuf<char>;
   blocks[dev]->alloc(total);
   char* d = blocks[dev]->p;
-  // inputs: the points (up to the factor slot), then the small tables
-  LIO_CUDA(cudaMemcpy(d, h, o_f, cudaMemcpyHostToDevice));
-  LIO_CUDA(cudaMemcpy(d + o_atom, h + o_atom, total - o_atom, cudaMemcpyHostToDevice));
-  k_becke_weights<<<(unsigned)((n + 127) / 128), 128>>>(
-      reinterpret_cast<const double*>(d + o_x), reinterpret_cast<const double*>(d + o_y),
-      reinterpret_cast<const double*>(d + o_z), reinterpret_cast<const int*>(d + o_atom),
-      reinterpret_cast<const int*>(d + o_group), n, reinterpret_cast<const int*>(d + o_off),
-      reinterpret_cast<const int*>(d + o_nucs), reinterpret_cast<const double*>(d + o_ax),
-      reinterpret_cast<const double*>(d + o_ay), reinterpret_cast<const double*>(d + o_az),
-      reinterpret_cast<const double*>(d + o_rm), reinterpret_cast<const double*>(d + o_dist), sys.natoms,
-      reinterpret_cast<double*>(d + o_f));
-  LIO_CUDA(cudaGetLastError());
-  LIO_CUDA(cudaMemcpy(hf, d + o_f, (size_t)n * 8, cudaMemcpyDeviceToHost));
+  // A pipeline over chunks of whole groups (about 1/8 of the points each): the
+  // host packs chunk c while the device copies in, weighs and copies out the
+  // chunks before it, and multiplies chunk c's weights while the device works
+  // on the ones after it.
+  const cudaStream_t cs = copy_stream();
+  StreamDrain drain{cs};
+  LIO_CUDA(cudaMemcpyAsync(d + o_off, h + o_off, total - o_off, cudaMemcpyHostToDevice, cs));
+  constexpr int kChunks = 8;
+  std::vector<long long> cut{0};  // group boundaries of the chunks
+  for (long long gi = 0; gi < ng; gi++)
+    if (first[gi + 1] - first[cut.back()] >= (n + kChunks - 1) / kChunks || gi + 1 == ng) cut.push_back(gi + 1);
+  const int nc = (int)cut.size() - 1;
+  struct Events {
+    std::vector<cudaEvent_t> e;
+    ~Events() {
+      for (cudaEvent_t x : e) cudaEventDestroy(x);
+    }
+  } ev;
+  for (int c = 0; c < nc; c++) {
 #pragma omp parallel for schedule(dynamic, 4)
-  for (long long gi = 0; gi < ng; gi++) {
-    long long k = first[gi];
-    for (GridPoint& p : groups[gi]->points) p.w *= hf[(size_t)k++];
+    for (long long gi = cut[c]; gi < cut[c + 1]; gi++) {
+      long long k = first[gi];
+      for (const GridPoint& p : groups[gi]->points) {
+        hx[k] = p.x;
+        hy[k] = p.y;
+        hz[k] = p.z;
+        hatom[k] = p.atom;
+        hgroup[k] = (int)gi;
+        k++;
+      }
+    }
+    const long long p0 = first[cut[c]], p1 = first[cut[c + 1]], np = p1 - p0;
+    cudaEvent_t e;
+    LIO_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ev.e.push_back(e);
+    if (np == 0) {
+      LIO_CUDA(cudaEventRecord(e, cs));
+      continue;
+    }
+    for (size_t o : {o_x, o_y, o_z})
+      LIO_CUDA(cudaMemcpyAsync(d + o + p0 * 8, h + o + p0 * 8, (size_t)np * 8, cudaMemcpyHostToDevice, cs));
+    for (size_t o : {o_atom, o_group})
+      LIO_CUDA(cudaMemcpyAsync(d + o + p0 * 4, h + o + p0 * 4, (size_t)np * 4, cudaMemcpyHostToDevice, cs));
+    k_becke_weights<<<(unsigned)((np + 127) / 128), 128, 0, cs>>>(
+        reinterpret_cast<const double*>(d + o_x), reinterpret_cast<const double*>(d + o_y),
+        reinterpret_cast<const double*>(d + o_z), reinterpret_cast<const int*>(d + o_atom),
+        reinterpret_cast<const int*>(d + o_group), p0, p1, reinterpret_cast<const int*>(d + o_off),
+        reinterpret_cast<const int*>(d + o_nucs), reinterpret_cast<const double*>(d + o_ax),
+        reinterpret_cast<const double*>(d + o_ay), reinterpret_cast<const double*>(d + o_az),
+        reinterpret_cast<const double*>(d + o_pair), reinterpret_cast<const double*>(d + o_dist), sys.natoms,
+        reinterpret_cast<double*>(d + o_f));
+    LIO_CUDA(cudaGetLastError());
+    LIO_CUDA(cudaMemcpyAsync(hf + p0, d + o_f + p0 * 8, (size_t)np * 8, cudaMemcpyDeviceToHost, cs));
+    LIO_CUDA(cudaEventRecord(e, cs));
+  }
+  for (int c = 0; c < nc; c++) {
+    LIO_CUDA(cudaEventSynchronize(ev.e[c]));
+#pragma omp parallel for schedule(dynamic, 4)
+    for (long long gi = cut[c]; gi < cut[c + 1]; gi++) {
+      // weights times factors, the zero-weight points dropped in place (in order)
+      std::vector<GridPoint>& pts = groups[gi]->points;
+      const double* f = hf + first[gi];
+      size_t kept = 0;
+      for (size_t q = 0; q < pts.size(); q++) {
+        const double w = pts[q].w * f[q];
+        if (drop_zero && w == 0.0) continue;
+        if (kept != q) pts[kept] = pts[q];
+        pts[kept++].w = w;
+      }
+      pts.resize(kept);
+    }
   }
 }
 
@@ -1120,7 +1204,6 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
   const int NQ = sys.lda ? 1 : kNQ;
 
   std::vector<GroupDev> gd;
-  std::vector<int> src_group;  // partition group of each device group
   std::vector<int> hfn, hsf, hst, hfsh, hfat, hsffn;
   std::vector<int8_t> hfcp;
   std::vector<int2> btiles, ftiles, sbtiles, sdtiles;
@@ -1138,6 +1221,50 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
   if (batch && keep) throw std::runtime_error("a batch of molecules is not sharded across devices");
   size_t member = 0;                        // the batch member of group g
   std::vector<int2> member_ft;              // per member: its range of energy-partial blocks
+
+  // The point arrays first: every device group's points, SoA at its padded
+  // offset, packed on all host threads into the pinned staging (x, y, z, w one
+  // after the other; padded slots hold a copy of the first point with zero
+  // weight) and copied on the copy stream while the host builds the lists below.
+  std::vector<int> src_group;  // partition group of each device group
+  std::vector<long long> src_off;
+  long long np_pad = 0;
+  for (int g = 0; g < ngr; g++) {
+    if (keep && !(*keep)[g]) continue;  // another rank's group
+    const int npts = (int)part.group(g).points.size();
+    src_group.push_back(g);
+    src_off.push_back(np_pad);
+    np_pad += ((npts + kPointPad - 1) / kPointPad) * kPointPad;
+  }
+  PinnedStaging& ps = point_staging();
+  std::lock_guard<std::mutex> ps_lock(ps.m);  // one upload at a time: held to the end of this upload
+  ps.reserve(4 * (size_t)std::max(np_pad, 1LL) * sizeof(double));
+  double* hx = static_cast<double*>(ps.host);
+  double* hy = hx + np_pad;
+  double* hz = hy + np_pad;
+  double* hw = hz + np_pad;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (long long gi = 0; gi < (long long)src_group.size(); gi++) {
+    const PointGroup& pg = part.group(src_group[gi]);
+    const int npts = (int)pg.points.size();
+    const int ldp = ((npts + kPointPad - 1) / kPointPad) * kPointPad;
+    for (int p = 0; p < ldp; p++) {
+      const GridPoint& q = pg.points[p < npts ? p : 0];
+      const long long o = src_off[gi] + p;
+      hx[o] = q.x;
+      hy[o] = q.y;
+      hz[o] = q.z;
+      hw[o] = p < npts ? q.w : 0.0;
+    }
+  }
+  const cudaStream_t cs = copy_stream();
+  StreamDrain drain{cs};
+  for (auto [buf, src] : {std::pair<DevBuf<double>*, const double*>{&d->px, hx}, {&d->py, hy}, {&d->pz, hz},
+                          {&d->pw, hw}}) {
+    buf->alloc((size_t)np_pad);
+    LIO_CUDA(cudaMemcpyAsync(buf->p, src, (size_t)np_pad * sizeof(double), cudaMemcpyHostToDevice, cs));
+  }
+
   for (int g = 0; g < ngr; g++) {
     if (keep && !(*keep)[g]) continue;  // another rank's group
     const int gdev = (int)gd.size();    // its index on this device
@@ -1180,7 +1307,6 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
     for (int I = 0; I < nI; I++)
       for (int J = 0; J < nJ; J++)
         if (J * kFkCols + kFkCols - 1 >= I * kFkRows) fktiles.push_back({gdev, I, J, 0});
-    src_group.push_back(g);  // its points are packed after this loop, all groups at once
     for (size_t i = 0; i < pg.funcs.size(); i++) {
       const int f = pg.funcs[i];
       const int type = !sys.ftype.empty() ? sys.ftype[f]
@@ -1230,29 +1356,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
     npts_total += G.npts;
     gd.push_back(G);
   }
-  // points of every device group in parallel, SoA at the group's pt_off, into
-  // the pinned staging (x, y, z, w one after the other); padded slots hold a
-  // copy of the first point with zero weight
-  PinnedStaging& ps = point_staging();
-  std::lock_guard<std::mutex> ps_lock(ps.m);  // one upload at a time: held to the end of this upload
-  ps.reserve(4 * (size_t)pt_off * sizeof(double));
-  double* hx = static_cast<double*>(ps.host);
-  double* hy = hx + pt_off;
-  double* hz = hy + pt_off;
-  double* hw = hz + pt_off;
-#pragma omp parallel for schedule(dynamic, 4)
-  for (long long gi = 0; gi < (long long)gd.size(); gi++) {
-    const GroupDev& G = gd[gi];
-    const PointGroup& pg = part.group(src_group[gi]);
-    for (int p = 0; p < G.ldp; p++) {
-      const GridPoint& q = pg.points[p < G.npts ? p : 0];
-      const long long o = G.pt_off + p;
-      hx[o] = q.x;
-      hy[o] = q.y;
-      hz[o] = q.z;
-      hw[o] = p < G.npts ? q.w : 0.0;
-    }
-  }
+  if (pt_off != np_pad) throw std::runtime_error("upload: point offsets disagree");
   d->tc_sizes[0] = bb_off;
   d->bblk_elems = bb_off;
   d->tc_sizes[1] = sl_off;
@@ -1279,11 +1383,6 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
     hnc[i] = sys.ncont[i];
   }
   d->groups.upload(gd);
-  for (auto [buf, src] : {std::pair<DevBuf<double>*, const double*>{&d->px, hx}, {&d->py, hy}, {&d->pz, hz},
-                          {&d->pw, hw}}) {
-    buf->alloc((size_t)pt_off);
-    LIO_CUDA(cudaMemcpy(buf->p, src, (size_t)pt_off * sizeof(double), cudaMemcpyHostToDevice));
-  }
   d->fn_glob.upload(hfn);
   d->fn_sh.upload(hfsh);
   d->fn_atom.upload(hfat);
@@ -1338,19 +1437,41 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
     d->Pc.free();
     d->Kc.free();
   } else {
-    // the packed entries this engine's groups touch (fn_glob is increasing within a group)
-    std::vector<unsigned char> touched(npacked, 0);
+    // the packed entries this engine's groups touch (fn_glob is increasing
+    // within a group), marked by the groups on all host threads (relaxed
+    // atomic byte stores: groups that share entries store the same 1)
+    std::unique_ptr<std::atomic<unsigned char>[]> touched(new std::atomic<unsigned char>[npacked]);
+#pragma omp parallel for schedule(static)
+    for (long long e = 0; e < (long long)npacked; e++) touched[e].store(0, std::memory_order_relaxed);
     const long long Ml = sys.M;
-    for (const GroupDev& G : gd) {
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long gi = 0; gi < (long long)gd.size(); gi++) {
+      const GroupDev& G = gd[gi];
       const int* f = hfn.data() + G.fn_off;
       for (int a = 0; a < G.m; a++) {
         const long long lo = f[a], row = lo * Ml - (lo * (lo - 1)) / 2 - lo;
-        for (int b = a; b < G.m; b++) touched[(size_t)(row + f[b])] = 1;
+        for (int b = a; b < G.m; b++) touched[(size_t)(row + f[b])].store(1, std::memory_order_relaxed);
       }
     }
-    d->hpidx.clear();
-    for (size_t e = 0; e < npacked; e++)
-      if (touched[e]) d->hpidx.push_back((long long)e);
+    // their indices in order: counted per chunk, then written per chunk
+    constexpr long long kChunks = 256;
+    const long long chunk = ((long long)npacked + kChunks - 1) / kChunks;
+    std::vector<long long> at(kChunks + 1, 0);
+#pragma omp parallel for schedule(static)
+    for (long long c = 0; c < kChunks; c++) {
+      long long cnt = 0;
+      for (long long e = c * chunk; e < std::min((c + 1) * chunk, (long long)npacked); e++)
+        cnt += touched[e].load(std::memory_order_relaxed);
+      at[c + 1] = cnt;
+    }
+    for (long long c = 0; c < kChunks; c++) at[c + 1] += at[c];
+    d->hpidx.resize((size_t)at[kChunks]);
+#pragma omp parallel for schedule(static)
+    for (long long c = 0; c < kChunks; c++) {
+      long long o = at[c];
+      for (long long e = c * chunk; e < std::min((c + 1) * chunk, (long long)npacked); e++)
+        if (touched[e].load(std::memory_order_relaxed)) d->hpidx[(size_t)o++] = e;
+    }
     d->compact = !d->hpidx.empty() && 2 * d->hpidx.size() <= npacked;
     const size_t nsp = sys.open ? 2 : 1;
     if (d->compact) {
@@ -1407,6 +1528,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
   d->basis_norm = sys.d_norm;
   d->basis.free();
   d->basis_valid = false;
+  LIO_CUDA(cudaStreamSynchronize(cs));  // the point arrays are in place
   if (precision_ == Precision::FP64) d->compute_basis();
 }
 

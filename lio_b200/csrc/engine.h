@@ -130,7 +130,7 @@ class DeviceEngine {
   // Becke weights of a partition being built, on the current device: the
   // bit-exact device form of host_becke_weights (partition.h), for
   // build_partition's `weights` argument.
-  static void becke_weights(const System& sys, const std::vector<PointGroup*>& groups);
+  static void becke_weights(const System& sys, const std::vector<PointGroup*>& groups, bool drop_zero);
   // builds the current form's per-geometry caches now (tensor-core operands or
   // the FP64 basis cache; otherwise the next solve does)
   void prepare();

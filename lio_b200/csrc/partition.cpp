@@ -97,10 +97,15 @@ void assign_functions(const System& sys, const Options& opt, const std::vector<d
 
 // Becke fuzzy-cell partition with the atomic-size adjustment, restricted to the
 // group's nuclei: g2g/cpu/weight.cpp:13-112.
-inline double becke_step(double u, double rm_j, double rm_k) {
+// the size adjustment a_jk of the pair (g2g/cpu/weight.cpp:40-44)
+inline double becke_adjust(double rm_j, double rm_k) {
   double x = rm_j / rm_k;
   x = (x - 1.0) / (x + 1.0);
-  u += (x / (x * x - 1.0)) * (1.0 - u * u);
+  return x / (x * x - 1.0);
+}
+
+inline double becke_step(double u, double rm_j, double rm_k) {
+  u += becke_adjust(rm_j, rm_k) * (1.0 - u * u);
   u = 1.5 * u - 0.5 * (u * u * u);
   u = 1.5 * u - 0.5 * (u * u * u);
   u = 1.5 * u - 0.5 * (u * u * u);
@@ -154,13 +159,10 @@ void compute_weights(const System& sys, PointGroup& g) {
 }
 
 // zero-weight removal (g2g/cpu/weight.cpp:100-111)
-void remove_zero_weights(const Options& opt, PointGroup& g) {
-  if (!opt.remove_zero_weights) return;
-  std::vector<GridPoint> kept;
-  kept.reserve(g.points.size());
-  for (const GridPoint& p : g.points)
-    if (p.w != 0.0) kept.push_back(p);
-  g.points.swap(kept);
+void remove_zero_weights(PointGroup& g) {
+  // in place, keeping the order (no fresh buffer to fault in)
+  g.points.erase(std::remove_if(g.points.begin(), g.points.end(), [](const GridPoint& p) { return p.w == 0.0; }),
+                 g.points.end());
 }
 
 long long env_int(const char* name, long long dflt) {
@@ -170,8 +172,17 @@ long long env_int(const char* name, long long dflt) {
 
 }  // namespace
 
-void host_becke_weights(const System& sys, const std::vector<PointGroup*>& groups) {
-  for (PointGroup* g : groups) compute_weights(sys, *g);
+void becke_pair_table(const System& sys, double* out) {
+  const size_t na = (size_t)sys.natoms;
+  for (size_t j = 0; j < na; j++)
+    for (size_t k = 0; k < na; k++) out[j * na + k] = becke_adjust(sys.rm[j], sys.rm[k]);
+}
+
+void host_becke_weights(const System& sys, const std::vector<PointGroup*>& groups, bool drop_zero) {
+  for (PointGroup* g : groups) {
+    compute_weights(sys, *g);
+    if (drop_zero) remove_zero_weights(*g);
+  }
 }
 
 // Per-atom point buffers of the grid build, kept by each calling thread from one
@@ -429,9 +440,7 @@ void build_partition(const System& sys, const Options& opt, const AngularGrid& a
   all.reserve(cand_cubes.size() + cand_spheres.size());
   for (PointGroup& g : cand_cubes) all.push_back(&g);
   for (PointGroup& g : cand_spheres) all.push_back(&g);
-  (weights ? weights : host_becke_weights)(sys, all);
-#pragma omp parallel for schedule(dynamic, 4)
-  for (long long gi = 0; gi < (long long)all.size(); gi++) remove_zero_weights(opt, *all[gi]);
+  (weights ? weights : host_becke_weights)(sys, all, opt.remove_zero_weights);
   for (int pass = 0; pass < 2; pass++) {
     std::vector<PointGroup>& cand = pass == 0 ? cand_cubes : cand_spheres;
     for (PointGroup& g : cand) {

@@ -38,11 +38,15 @@ struct Partition {
 
 // Becke weights of many groups at once (g2g/cpu/weight.cpp:13-112): every
 // point's weight is multiplied by its atom's fuzzy-cell weight, restricted to
-// the group's nuclei, bit for bit as the reference computes it. The groups'
-// zero-weight points are not removed here.
-using WeightsFn = void (*)(const System& sys, const std::vector<PointGroup*>& groups);
+// the group's nuclei, bit for bit as the reference computes it. With
+// `drop_zero` the points whose weight is then 0 are removed, keeping the order
+// of the others (g2g/cpu/weight.cpp:100-111), in the same pass.
+using WeightsFn = void (*)(const System& sys, const std::vector<PointGroup*>& groups, bool drop_zero);
 // host implementation (OpenMP over each group's points)
-void host_becke_weights(const System& sys, const std::vector<PointGroup*>& groups);
+void host_becke_weights(const System& sys, const std::vector<PointGroup*>& groups, bool drop_zero);
+// the atomic-size adjustment of every atom pair (j, k), out[j * natoms + k],
+// by the operations the host weights use (compiled without FMA contraction)
+void becke_pair_table(const System& sys, double* out);
 
 // Builds the partition. `grid_type` selects the radial shell table (0: Nr,
 // otherwise Nr2) exactly as g2g/init.cpp:238-266 does. The Becke weights of all
