@@ -805,8 +805,9 @@ def main():
     ap.add_argument("--max-atoms", type=int, default=200, help="largest molecule in the serve mode")
     ap.add_argument("--duration", type=float, default=4.0, help="seconds per arrival rate in the serve mode")
     ap.add_argument("--inflight", type=int, default=32, help="builds on the GPU at once (batch / serve)")
-    ap.add_argument("--service-precision", type=int, default=2,
-                    help="form of the batch / serve modes: 0 FP64, 1 tensor core, 2 autotuned per molecule")
+    ap.add_argument("--service-precision", type=int, default=1,
+                    help="form of the serve mode: 0 FP64, 1 tensor core (lean: the whole population stays "
+                         "resident), 2 autotuned per molecule")
     ap.add_argument("--no-oracle", action="store_true", help="batch / serve: skip the checks against the oracle")
     ap.add_argument("--batch-precision", type=int, default=1,
                     help="batch: 0 FP64, 1 tensor core (classes it cannot run take FP64), 2 autotuned per class")

@@ -123,6 +123,14 @@ void g2g_set_angular_grid_(const unsigned int* grid_type, const unsigned int* np
  * functions in one group than a block's shared memory holds). */
 void g2g_set_precision_(const unsigned int* mode);
 
+/* Lean tensor-core form (no reference counterpart): *on != 0 releases the
+ * blocked FP64 basis values once the tensor-core operands are built (about a
+ * third of the form's device footprint for GGA). The Kohn-Sham contraction then
+ * forms the basis values it needs from the per-shell radial sums, and a force
+ * request (g2g_solve_groups_ types 2/3) rebuilds the blocked values for its
+ * call. Off by default; applies to the current grid at once and to later ones. */
+void g2g_set_lean_(const unsigned int* on);
+
 /* Partition statistics of the current grid: out[0] = groups, out[1] = cubes,
  * out[2] = spheres, out[3] = points kept, out[4] = sum over groups of
  * points * functions, out[5] = sum of points * functions^2. */

@@ -865,7 +865,8 @@ struct DeviceEngine::Impl {
   DevBuf<int2> dens_tc_tiles;  // (group, 128-point tile), largest function count first
   int tc_fcap = 0, nsm = 148;
 
-  DevBuf<double> bblk;  // blocked FP64 basis (tensor-core density epilogue)
+  DevBuf<double> bblk;  // blocked FP64 basis (tensor-core operands, forces)
+  bool lean = false;    // the blocked basis is dropped once the operands are built
   int max_nftc = 0;
   DevBuf<int8_t> aslices, dslices_a, dslices_b;
   DevBuf<int16_t> aexp, dexp_a, dexp_b;
@@ -1589,15 +1590,18 @@ void DeviceEngine::prepare_tensor_core() {
   }
   {
     const int nrows = (int)d->fa_rows.n;
-    k_fock_rowexp<1><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(d->fa_rows.p, nrows, d->groups.p, d->bblk.p,
-                                                                  nullptr, nullptr, d->fa_exp.p, nullptr, 0, d->nkb);
+    k_fock_rowexp<1, false><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(
+        d->fa_rows.p, nrows, d->groups.p, d->bblk.p, nullptr, nullptr, d->fa_exp.p, nullptr, 0, d->nkb,
+        RadialSource{});
     LIO_CUDA(cudaGetLastError());
     k_fock_aslices<<<(unsigned)d->fa_tiles32.n, 256, 0, st>>>(d->fa_tiles32.p, d->groups.p, d->bblk.p,
                                                                 d->fa_exp.p, d->fa_slices.p, d->nkb);
     LIO_CUDA(cudaGetLastError());
   }
-  LIO_CUDA(cudaFuncSetAttribute(k_fock_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FkCfg<1>::kSmem));
-  LIO_CUDA(cudaFuncSetAttribute(k_fock_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FkCfg<2>::kSmem));
+  LIO_CUDA(cudaFuncSetAttribute(k_fock_tc<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FkCfg<1>::kSmem));
+  LIO_CUDA(cudaFuncSetAttribute(k_fock_tc<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FkCfg<2>::kSmem));
+  LIO_CUDA(cudaFuncSetAttribute(k_fock_tc<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FkCfg<1>::kSmem));
+  LIO_CUDA(cudaFuncSetAttribute(k_fock_tc<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FkCfg<2>::kSmem));
   {
     int dev = 0;
     LIO_CUDA(cudaGetDevice(&dev));
@@ -1630,6 +1634,9 @@ void DeviceEngine::prepare_tensor_core() {
     else
       raise_limit((const void*)k_density_tc<true, 1>);
   }
+  // a lean engine keeps the operands only: the Kohn-Sham kernels then form F
+  // from the radial sums, and forces rebuild the blocked basis when asked
+  if (d->lean) d->bblk.free();  // cudaFree waits for the kernels above
   d->tc_ready = true;
 }
 
@@ -1714,27 +1721,47 @@ int DeviceEngine::run_kernels(bool compute_rmm, bool ext) {
     }
     if (tc) {
       // row exponents of f * F (both spins, one pass over F); the contraction
-      // kernel cuts the f * F slices itself
+      // kernel cuts the f * F slices itself. F from the blocked basis, or (a lean
+      // engine) from the radial sums.
       const int nrows = (int)d->fb_rows.n;
-      if (d->open)
-        k_fock_rowexp<2><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(d->fb_rows.p, nrows, d->groups.p, d->bblk.p,
-                                                                      d->fac_a.p, d->fac_b.p, d->fb_exp_a.p,
-                                                                      d->fb_exp_b.p, 1, d->nkb);
-      else
-        k_fock_rowexp<1><<<(unsigned)((nrows + 7) / 8), 256, 0, st>>>(d->fb_rows.p, nrows, d->groups.p, d->bblk.p,
-                                                                      d->fac_a.p, nullptr, d->fb_exp_a.p, nullptr, 1,
-                                                                      d->nkb);
+      const RadialSource rs{d->rad.p,    d->px.p, d->py.p, d->pz.p, d->fn_sh.p,      d->fn_cp.p,
+                            d->fn_atom.p, d->ax.p, d->ay.p, d->az.p, d->basis_norm, d->lda ? 1 : 3};
+      const unsigned nb = (unsigned)((nrows + 7) / 8);
+      const double* fb = d->fac_b.p;
+      int16_t* eb = d->fb_exp_b.p;
+      if (!d->bblk.p) {
+        if (d->open)
+          k_fock_rowexp<2, true><<<nb, 256, 0, st>>>(d->fb_rows.p, nrows, d->groups.p, nullptr, d->fac_a.p, fb,
+                                                     d->fb_exp_a.p, eb, 1, 0, rs);
+        else
+          k_fock_rowexp<1, true><<<nb, 256, 0, st>>>(d->fb_rows.p, nrows, d->groups.p, nullptr, d->fac_a.p, nullptr,
+                                                     d->fb_exp_a.p, nullptr, 1, 0, rs);
+      } else {
+        if (d->open)
+          k_fock_rowexp<2, false><<<nb, 256, 0, st>>>(d->fb_rows.p, nrows, d->groups.p, d->bblk.p, d->fac_a.p, fb,
+                                                      d->fb_exp_a.p, eb, 1, d->nkb, rs);
+        else
+          k_fock_rowexp<1, false><<<nb, 256, 0, st>>>(d->fb_rows.p, nrows, d->groups.p, d->bblk.p, d->fac_a.p,
+                                                      nullptr, d->fb_exp_a.p, nullptr, 1, d->nkb, rs);
+      }
       LIO_CUDA(cudaGetLastError());
       launches++;
       d->mark(4);
-      if (d->open)
-        k_fock_tc<2><<<(unsigned)d->fk_tiles.n, FkCfg<2>::kThreads, FkCfg<2>::kSmem, st>>>(
-            d->fk_tiles.p, d->groups.p, d->fn_glob.p, d->fa_slices.p, d->fa_exp.p, d->bblk.p, d->nkb, d->fac_a.p,
-            d->fac_b.p, d->fb_exp_a.p, d->fb_exp_b.p, d->M, Ka, Kb, d->tc_err.p);
+      const unsigned nt = (unsigned)d->fk_tiles.n;
+#define launch_fock(NS_, RAD_)                                                                                        \
+  k_fock_tc<NS_, RAD_><<<nt, FkCfg<NS_>::kThreads, FkCfg<NS_>::kSmem, st>>>(                                      \
+      d->fk_tiles.p, d->groups.p, d->fn_glob.p, d->fa_slices.p, d->fa_exp.p, d->bblk.p, d->nkb, d->fac_a.p,         \
+      NS_ == 2 ? fb : nullptr, d->fb_exp_a.p, NS_ == 2 ? eb : nullptr, d->M, Ka, NS_ == 2 ? Kb : nullptr,           \
+      d->tc_err.p, rs)
+      if (d->open && !d->bblk.p)
+        launch_fock(2, true);
+      else if (d->open)
+        launch_fock(2, false);
+      else if (!d->bblk.p)
+        launch_fock(1, true);
       else
-        k_fock_tc<1><<<(unsigned)d->fk_tiles.n, FkCfg<1>::kThreads, FkCfg<1>::kSmem, st>>>(
-            d->fk_tiles.p, d->groups.p, d->fn_glob.p, d->fa_slices.p, d->fa_exp.p, d->bblk.p, d->nkb, d->fac_a.p,
-            nullptr, d->fb_exp_a.p, nullptr, d->M, Ka, nullptr, d->tc_err.p);
+        launch_fock(1, false);
+#undef launch_fock
     } else if (d->open) {
       d->mark(4);  // no operand preparation in the FP64 form
       k_fock_fp64<2><<<nk, 256, 0, st>>>(d->fock_tiles.p, d->groups.p, d->fn_glob.p, d->basis.p, d->fac_a.p,
@@ -1880,6 +1907,28 @@ Precision DeviceEngine::autotune(bool memory_aware) {
 void DeviceEngine::tuned_times(double* fp64_ms, double* tc_ms) const {
   *fp64_ms = impl_->tuned_fp64_ms;
   *tc_ms = impl_->tuned_tc_ms;
+}
+
+void DeviceEngine::set_lean(bool on) {
+  Impl* d = impl_.get();
+  d->lean = on;
+  if (on && d->tc_ready && precision_ == Precision::TensorCore && d->bblk.p) {
+    LIO_CUDA(cudaStreamSynchronize(d->stream));  // no build in flight reads it
+    d->bblk.free();
+    d->drop_graph();  // the captured Kohn-Sham launches read it
+  }
+}
+bool DeviceEngine::lean() const { return impl_->lean; }
+
+size_t DeviceEngine::estimate_blocked_basis_bytes(const System& sys, const Partition& part) {
+  double b = 0.0;
+  for (int g = 0; g < part.total_groups(); g++) {
+    const PointGroup& pg = part.group(g);
+    const double ldp = (double)(((long long)pg.points.size() + kPointPad - 1) / kPointPad * kPointPad);
+    const int nftc = (pg.total_functions() + kTcFuncs - 1) / kTcFuncs;
+    b += ldp * nftc * kTcFuncs * (sys.lda ? 1 : 4) * 8.0;
+  }
+  return (size_t)b;
 }
 
 size_t DeviceEngine::estimate_device_bytes(const System& sys, const Partition& part, Precision prec) {
@@ -2125,6 +2174,7 @@ SolveResult DeviceEngine::solve_forces(const SolveRequest& req, double* forces, 
     LIO_CUDA(cudaGetLastError());
     bv = BasisView{grad.p, 0, 4};
   } else if (precision_ == Precision::TensorCore) {
+    if (!d->bblk.p) d->compute_basis(true);  // a lean engine: rebuilt for the forces
     bv = BasisView{d->bblk.p, d->nkb, 1};
   } else {
     bv = BasisView{d->basis.p, 0, 1};
@@ -2157,6 +2207,7 @@ SolveResult DeviceEngine::solve_forces(const SolveRequest& req, double* forces, 
   if (tc) LIO_CUDA(cudaMemcpyAsync(&terr, d->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   LIO_CUDA(cudaStreamSynchronize(st));
   if (terr) throw std::runtime_error("tensor-core forces: an MMA completion wait timed out");
+  if (d->lean && d->bblk.p) d->bblk.free();  // back to the operands-only footprint
   float fms = 0.f;
   LIO_CUDA(cudaEventElapsedTime(&fms, d->fev0, d->fev1));
   d->last_force_ms = fms;

@@ -159,6 +159,14 @@ class DeviceEngine {
   // molecule's footprint before it is uploaded
   static long long process_device_bytes();
   static size_t estimate_device_bytes(const System& sys, const Partition& part, Precision prec);
+  // lean: once the tensor-core operands are built the blocked FP64 basis is
+  // released (about a third of the form's footprint for GGA); the Kohn-Sham
+  // kernels then form F from the radial sums, and forces rebuild the blocked
+  // basis for their call. Its size, which a lean engine still needs while it
+  // builds its operands:
+  void set_lean(bool on);
+  bool lean() const;
+  static size_t estimate_blocked_basis_bytes(const System& sys, const Partition& part);
 
   // statistics of the uploaded partition
   long long points() const;

@@ -15,7 +15,9 @@
 // instead of 12, and a third less operand traffic from shared memory, which
 // bounds this kernel. The A slices are built once per geometry; the B slices
 // are cut inside the contraction kernel, a K step at a time, so they never go
-// through HBM.
+// through HBM. The F values of the B operand come from the blocked basis, or,
+// when an engine does not keep it (RAD), from each shell's radial sum times the
+// function's monomial, as k_basis forms them.
 #pragma once
 
 constexpr int kFkRows = 128;  // UMMA M: functions i per tile
@@ -32,11 +34,14 @@ struct FkCfg {
   static constexpr int kLevelRows = NS * kFkCols;           // B rows (and TMEM columns) per level
   static constexpr int kTallRows = kSlices * kLevelRows;    // rows of the stacked B operand
   static constexpr int kMaxLevels = 256 / kLevelRows;       // levels per MMA (N <= 256)
-  // ring slot: the 32 F rows of a 128-point tile, each padded to 1040 bytes so
-  // that 32 lanes reading 16 bytes of 32 different rows hit distinct banks,
-  // then each spin's 128 factors
+  // ring slot: the 32 F rows (or the radial sums of up to 32 shells) of a
+  // 128-point tile, each padded to 1040 bytes so that 32 lanes reading 16 bytes
+  // of 32 different rows hit distinct banks, then each spin's 128 factors, then
+  // the points' x, y, z (RAD)
   static constexpr int kRowBytes = kTcPoints * 8 + 16;
-  static constexpr int kSlot = kFkCols * kRowBytes + NS * kTcPoints * 8;
+  static constexpr int kFac = kFkCols * kRowBytes;
+  static constexpr int kXyz = kFac + NS * kTcPoints * 8;
+  static constexpr int kSlot = kXyz + 3 * kTcPoints * 8;
   static constexpr size_t kSmem = (size_t)kFkStages * kStage + 2 * (size_t)kSlot;
   static constexpr uint32_t kCols = NS * kSlices * kFkCols;
   static constexpr uint32_t kTmem = kCols <= 256 ? 256 : 512;
@@ -64,16 +69,55 @@ __device__ __forceinline__ const double* f_row(const GroupDev& G, const double* 
          (p & 127);
 }
 
+// F values without the blocked basis: a function's value at a point is its
+// shell's contracted radial sum t (k_radial: per group and 128-point tile,
+// [shell][nr][128 points], t first) times its monomial x^lx y^ly z^lz, times
+// dnorm for the d xx, yy, zz components ((dnorm P) t, the order of k_basis).
+struct RadialSource {
+  const double* rad;
+  const double* px;
+  const double* py;
+  const double* pz;
+  const int* fn_sh;
+  const int8_t* fn_cp;
+  const int* fn_atom;
+  const double* ax;
+  const double* ay;
+  const double* az;
+  double dnorm;
+  int nr;
+};
+// the per-function constants of that product (function i of group G, i < m)
+struct RadialRow {
+  double ax, ay, az, scale;
+  int lx, ly, lz, sh;
+  __device__ __forceinline__ void load(const RadialSource& rs, const GroupDev& G, int i) {
+    const int cp = rs.fn_cp[G.fn_off + i], c = cp & 15, atom = rs.fn_atom[G.fn_off + i];
+    lx = c_comp_l[c][0];
+    ly = c_comp_l[c][1];
+    lz = c_comp_l[c][2];
+    scale = (cp & 16) ? rs.dnorm : 1.0;
+    ax = rs.ax[atom];
+    ay = rs.ay[atom];
+    az = rs.az[atom];
+    sh = rs.fn_sh[G.fn_off + i];
+  }
+  __device__ __forceinline__ double value(double x, double y, double z, double t) const {
+    const double P = ipow(x - ax, lx) * ipow(y - ay, ly) * ipow(z - az, lz);
+    return scale * P * t;
+  }
+};
+
 // Pass 1, one warp per (group, row): the row's exponent per spin from
 // max_p |v_p|. Rows at or beyond m get exponent 0 (their slices are zeros).
 // The row is read a 128-point tile at a time, four consecutive points per lane
 // (two 16-byte loads of F and of each spin's factors), two tiles in flight.
 static_assert(kPointPad % kTcPoints == 0, "rows are read in whole 128-point tiles");
-template <int NS>
+template <int NS, bool RAD>
 __global__ void k_fock_rowexp(const int2* __restrict__ rows, int nrows, const GroupDev* __restrict__ groups,
                               const double* __restrict__ basis, const double* __restrict__ fac_a,
                               const double* __restrict__ fac_b, int16_t* __restrict__ expo_a,
-                              int16_t* __restrict__ expo_b, int use_sl_b, int nkb) {
+                              int16_t* __restrict__ expo_b, int use_sl_b, int nkb, RadialSource rs) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (warp >= nrows) return;  // whole warps only
   const int2 t = rows[warp];
@@ -83,12 +127,26 @@ __global__ void k_fock_rowexp(const int2* __restrict__ rows, int nrows, const Gr
 #pragma unroll
   for (int sp = 0; sp < NS; sp++) amax[sp] = 0.0;
   if (i < G.m) {
+    RadialRow rr{};
+    if (RAD) rr.load(rs, G, i);
 #pragma unroll 2
     for (int T = 0; T < ntl; T++) {
       const int p = T * kTcPoints + lane * 4;
-      const double* Fi = f_row(G, basis, i, p, nkb);
-      const double2 v01 = *reinterpret_cast<const double2*>(Fi);
-      const double2 v23 = *reinterpret_cast<const double2*>(Fi + 2);
+      double2 v01, v23;
+      if constexpr (RAD) {
+        const double* tr = rs.rad + G.rad_off + ((long long)(T * G.nsimple + rr.sh) * rs.nr) * kTcPoints + lane * 4;
+        const double2 t01 = *reinterpret_cast<const double2*>(tr), t23 = *reinterpret_cast<const double2*>(tr + 2);
+        const long long q = G.pt_off + p;
+        const double2 x01 = *reinterpret_cast<const double2*>(rs.px + q), x23 = *reinterpret_cast<const double2*>(rs.px + q + 2);
+        const double2 y01 = *reinterpret_cast<const double2*>(rs.py + q), y23 = *reinterpret_cast<const double2*>(rs.py + q + 2);
+        const double2 z01 = *reinterpret_cast<const double2*>(rs.pz + q), z23 = *reinterpret_cast<const double2*>(rs.pz + q + 2);
+        v01 = make_double2(rr.value(x01.x, y01.x, z01.x, t01.x), rr.value(x01.y, y01.y, z01.y, t01.y));
+        v23 = make_double2(rr.value(x23.x, y23.x, z23.x, t23.x), rr.value(x23.y, y23.y, z23.y, t23.y));
+      } else {
+        const double* Fi = f_row(G, basis, i, p, nkb);
+        v01 = *reinterpret_cast<const double2*>(Fi);
+        v23 = *reinterpret_cast<const double2*>(Fi + 2);
+      }
 #pragma unroll
       for (int sp = 0; sp < NS; sp++) {
         const double* fac = sp == 0 ? fac_a : fac_b;
@@ -173,13 +231,13 @@ __global__ void __launch_bounds__(256) k_fock_aslices(const int2* __restrict__ r
 // combines the levels of each (i, j) with i <= j and adds K_ij into the packed
 // accumulator(s) with FP64 atomics. Every wait is bounded; a timeout sets the
 // error flag, and the producer lets its copies in flight land before exiting.
-template <int NS>
+template <int NS, bool RAD>
 __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
     k_fock_tc(const int4* __restrict__ tiles, const GroupDev* __restrict__ groups, const int* __restrict__ fn_glob,
               const int8_t* __restrict__ aslices, const int16_t* __restrict__ aexp, const double* __restrict__ bblk,
               int nkb, const double* __restrict__ fac_a, const double* __restrict__ fac_b,
               const int16_t* __restrict__ bexp_a, const int16_t* __restrict__ bexp_b, int M,
-              double* __restrict__ K_a, double* __restrict__ K_b, int* __restrict__ err) {
+              double* __restrict__ K_a, double* __restrict__ K_b, int* __restrict__ err, RadialSource rs) {
   using Cfg = FkCfg<NS>;
   extern __shared__ __align__(128) uint8_t fk_smem[];
   __shared__ uint64_t afull[kFkStages], bready[kFkStages], empty[kFkStages], cfull[2], cempty[2], done;
@@ -215,6 +273,9 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
     if (lane == 0) {
       const int8_t* A = aslices + G.fa_off + (long long)I * nsteps * kFkStepA;
       const int rows = min(kFkCols, G.m - J * kFkCols);  // rows of J that exist (from row 0 of the chunk)
+      // RAD: the shells of those rows (consecutive), one radial row each
+      const int sh0 = RAD ? rs.fn_sh[G.fn_off + J * kFkCols] : 0;
+      const int nsh = RAD ? rs.fn_sh[G.fn_off + J * kFkCols + rows - 1] - sh0 + 1 : 0;
       int na = 0, nc = 0;  // A stages and F tiles issued
       for (int st = 0; st < nsteps && !*vfail; st++) {
         const int T = st >> 2;
@@ -225,12 +286,24 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
             break;
           }
           uint8_t* slot = ring + c * Cfg::kSlot;
-          const double* F = bblk + G.bb_off + (long long)(T * G.nftc + J) * nkb * kTcChunk;
-          lio::umma::mbar_expect_tx(&cfull[c], (uint32_t)((rows + NS) * kTcPoints * 8));
-          for (int r = 0; r < rows; r++)
-            lio::umma::bulk_copy_g2s(slot + r * Cfg::kRowBytes, F + r * kTcPoints, kTcPoints * 8, &cfull[c]);
+          if constexpr (RAD) {
+            const double* tr = rs.rad + G.rad_off + ((long long)(T * G.nsimple + sh0) * rs.nr) * kTcPoints;
+            lio::umma::mbar_expect_tx(&cfull[c], (uint32_t)((nsh + NS + 3) * kTcPoints * 8));
+            for (int r = 0; r < nsh; r++)
+              lio::umma::bulk_copy_g2s(slot + r * Cfg::kRowBytes, tr + (long long)r * rs.nr * kTcPoints,
+                                       kTcPoints * 8, &cfull[c]);
+            const double* xyz[3] = {rs.px, rs.py, rs.pz};
+            for (int d3 = 0; d3 < 3; d3++)
+              lio::umma::bulk_copy_g2s(slot + Cfg::kXyz + d3 * kTcPoints * 8, xyz[d3] + G.pt_off + T * kTcPoints,
+                                       kTcPoints * 8, &cfull[c]);
+          } else {
+            const double* F = bblk + G.bb_off + (long long)(T * G.nftc + J) * nkb * kTcChunk;
+            lio::umma::mbar_expect_tx(&cfull[c], (uint32_t)((rows + NS) * kTcPoints * 8));
+            for (int r = 0; r < rows; r++)
+              lio::umma::bulk_copy_g2s(slot + r * Cfg::kRowBytes, F + r * kTcPoints, kTcPoints * 8, &cfull[c]);
+          }
           for (int sp = 0; sp < NS; sp++)
-            lio::umma::bulk_copy_g2s(slot + kFkCols * Cfg::kRowBytes + sp * kTcPoints * 8,
+            lio::umma::bulk_copy_g2s(slot + Cfg::kFac + sp * kTcPoints * 8,
                                      (sp == 0 ? fac_a : fac_b) + G.pt_off + T * kTcPoints, kTcPoints * 8, &cfull[c]);
           nc = T + 1;
         }
@@ -292,6 +365,11 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
       const int pb = 4 * PPT * (warp >> 2) + PPT * q;  // first point of the lane within a K step
       const int j = J * kFkCols + row;
       const bool valid = j < G.m;  // rows past m are zeros (the ring holds stale rows there)
+      RadialRow rr{};
+      if (RAD && valid) {
+        rr.load(rs, G, j);
+        rr.sh -= rs.fn_sh[G.fn_off + J * kFkCols];  // its radial row in the ring slot
+      }
       double s42[NS];
 #pragma unroll
       for (int sp = 0; sp < NS; sp++)
@@ -317,12 +395,19 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
         uint32_t lo[SU][NS][PPT], hi[SU][NS][PPT];
 #pragma unroll
         for (int u = 0; u < SU; u++) {
-          const double* Fr = reinterpret_cast<const double*>(slot + row * Cfg::kRowBytes) + (sub + u) * 32 + pb;
-          const double* fr =
-              reinterpret_cast<const double*>(slot + kFkCols * Cfg::kRowBytes) + (sub + u) * 32 + pb;
+          const double* Fr =
+              reinterpret_cast<const double*>(slot + (RAD ? rr.sh : row) * Cfg::kRowBytes) + (sub + u) * 32 + pb;
+          const double* fr = reinterpret_cast<const double*>(slot + Cfg::kFac) + (sub + u) * 32 + pb;
+          const double* xr = reinterpret_cast<const double*>(slot + Cfg::kXyz) + (sub + u) * 32 + pb;
 #pragma unroll
           for (int k = 0; k < PPT; k += 2) {
-            const double2 v = *reinterpret_cast<const double2*>(Fr + k);
+            double2 v = *reinterpret_cast<const double2*>(Fr + k);
+            if constexpr (RAD) {  // Fr holds the radial sums t: F = monomial x t
+              const double2 x = *reinterpret_cast<const double2*>(xr + k);
+              const double2 y = *reinterpret_cast<const double2*>(xr + kTcPoints + k);
+              const double2 z = *reinterpret_cast<const double2*>(xr + 2 * kTcPoints + k);
+              v = make_double2(rr.value(x.x, y.x, z.x, v.x), rr.value(x.y, y.y, z.y, v.y));
+            }
 #pragma unroll
             for (int sp = 0; sp < NS; sp++) {
               const double2 f = *reinterpret_cast<const double2*>(fr + sp * kTcPoints + k);

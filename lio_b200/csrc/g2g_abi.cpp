@@ -78,6 +78,7 @@ struct State {
   void* stream = nullptr;
   bool graphs = true;
   bool device_weights = true;  // Becke weights of the grid build on the GPU when one is present
+  bool lean = false;           // g2g_set_lean_: the blocked basis released once the operands are built
   int shard_rank = 0, shard_world = 1;  // this process's share of the groups (multi-GPU)
 };
 
@@ -196,6 +197,7 @@ void build_grid(unsigned grid_type) {
     throw std::runtime_error("no CUDA device: the grid partition was built but the device engine is unavailable");
   }
   if (!s.engine) s.engine.reset(new lio::DeviceEngine());
+  s.engine->set_lean(s.lean);
   s.engine->set_stream(s.stream);
   s.engine->set_graphs(s.graphs);
   s.precision = s.mode == 0 ? lio::Precision::FP64 : lio::Precision::TensorCore;
@@ -580,6 +582,14 @@ int g2g_last_error_(char* msg, const unsigned* len) {
   s.status = 0;
   s.message.clear();
   return code;
+}
+
+void g2g_set_lean_(const unsigned* on) {
+  guarded("g2g_set_lean_", [&] {
+    State& s = st();
+    s.lean = *on != 0;
+    if (s.engine) s.engine->set_lean(s.lean);
+  });
 }
 
 void g2g_set_precision_(const unsigned* mode) {

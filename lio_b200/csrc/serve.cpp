@@ -162,13 +162,20 @@ bool lio_server::plan_load(int mi, std::string& why) {
   // before the first upload: the estimate of its form (autotuned: the larger of
   // the two, held one after the other while both are timed); a cold molecule
   // needs its caches back only
+  // Engines are lean: a tensor-core molecule holds its blocked basis only while
+  // its operands are built, so a (re)load of one books that room as well (the
+  // booking is replaced by the measured footprint once it is resident).
+  const bool tc_form = autotune ? m.form == 1 : precision == lio::Precision::TensorCore;
+  const unsigned long long transient =
+      (m.engine || m.measured) && tc_form ? lio::DeviceEngine::estimate_blocked_basis_bytes(m.sys, m.part) : 0;
   const unsigned long long need =
-      m.engine ? m.footprint - m.core
-      : m.measured ? m.footprint
-      : autotune ? (unsigned long long)std::max(
-                       lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, lio::Precision::FP64),
-                       lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, lio::Precision::TensorCore))
-                 : (unsigned long long)lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, precision);
+      transient +
+      (m.engine ? m.footprint - m.core
+       : m.measured ? m.footprint
+       : autotune ? (unsigned long long)std::max(
+                        lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, lio::Precision::FP64),
+                        lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, lio::Precision::TensorCore))
+                  : (unsigned long long)lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, precision));
   // Eviction in two levels, least recently used idle molecules first: their
   // caches (the bulk of a footprint; they go cold and keep their grid), and only
   // if that cannot make room, whole molecules (hot or cold).
@@ -244,6 +251,7 @@ void lio_server::loader_loop() {
       } else {
         e.reset(new lio::DeviceEngine());
         e->set_graphs(true);
+        e->set_lean(true);  // the tensor-core form keeps its operands, not the blocked basis
         if (autotune && form >= 0) {  // decided at an earlier upload
           e->set_precision(form ? lio::Precision::TensorCore : lio::Precision::FP64);
           e->upload(m.sys, m.part);

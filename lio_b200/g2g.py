@@ -192,6 +192,11 @@ class G2GLibrary:
     def set_precision(self, mode: int):
         self.lib.g2g_set_precision_(C.byref(_u(mode)))
 
+    def set_lean(self, on: bool):
+        """Lean tensor-core form: the blocked FP64 basis released once the operands are built."""
+        self.lib.g2g_set_lean_(C.byref(_u(1 if on else 0)))
+        self.check("g2g_set_lean_")
+
     def set_device_weights(self, on: bool):
         """Becke weights of the next grid builds on the GPU (default) or the host."""
         self.lib.g2g_set_device_weights_(C.byref(_u(1 if on else 0)))
