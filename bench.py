@@ -621,7 +621,8 @@ def md_mode(args):
     wl = workload(0, args.workload)
     lib = G2GLibrary()
     gt = bind(lib, wl)
-    lib.set_precision(args.precision)
+    # the default form (3: tensor core, operands built with the grid) or FP64
+    lib.set_precision(3 if args.precision else 0)
     rng = np.random.default_rng(5)
     r = lib._arrays["r"]
     ph = (C.c_double * 3)()
