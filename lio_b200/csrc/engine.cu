@@ -189,13 +189,18 @@ struct DevBuf {
 // Host copies of the packed matrices (millions of doubles for a few thousand
 // functions), threaded: dst = src, and dst += src.
 void host_copy(double* dst, const double* src, size_t n) {
-#pragma omp parallel for schedule(static) if (n > (1u << 16))
+#pragma omp parallel for schedule(static) if (n >= (1u << 15))
   for (long long i = 0; i < (long long)n; i++) dst[i] = src[i];
 }
 void host_accumulate(double* dst, const double* src, size_t n) {
-#pragma omp parallel for schedule(static) if (n > (1u << 16))
+#pragma omp parallel for schedule(static) if (n >= (1u << 15))
   for (long long i = 0; i < (long long)n; i++) dst[i] += src[i];
 }
+
+// Pieces of the compact Kohn-Sham download: eight, each added into the
+// caller's vectors on all host threads while the next is in flight (the same
+// sizes on both sides: enqueue downloads them, finish adds them)
+size_t compact_piece(size_t total) { return std::max<size_t>((total + 7) / 8, (size_t)1 << 15); }
 
 // Compact transfers of a host-array solve: only the packed entries some group
 // touches (sorted, unique `idx`, n per spin) cross PCIe. The density's are
@@ -2049,7 +2054,7 @@ void DeviceEngine::enqueue(const SolveRequest& req) {
           d->K_a.p, d->open ? d->K_b.p : nullptr, d->pidx.p, np, nspin, d->Kc.p);
       LIO_CUDA(cudaGetLastError());
       const size_t total = (size_t)nspin * np;
-      const size_t piece = std::max<size_t>((total + Impl::kMaxChunks - 1) / Impl::kMaxChunks, 1 << 16);
+      const size_t piece = compact_piece(total);
       for (size_t o = 0; o < total; o += piece, d->nchunks++) {
         LIO_CUDA(cudaMemcpyAsync(d->hK + o, d->Kc.p + o, std::min(piece, total - o) * sizeof(double),
                                  cudaMemcpyDeviceToHost, st));
@@ -2104,12 +2109,12 @@ SolveResult DeviceEngine::finish(const SolveRequest& req) {
     const long long np = (long long)d->hpidx.size();
     const long long* ix = d->hpidx.data();
     const size_t total = (size_t)nspin * np;
-    const size_t piece = std::max<size_t>((total + Impl::kMaxChunks - 1) / Impl::kMaxChunks, 1 << 16);
+    const size_t piece = compact_piece(total);
     int c = 0;
     for (size_t o = 0; o < total; o += piece, c++) {
       LIO_CUDA(cudaEventSynchronize(d->kev[c]));
       const long long k1 = (long long)std::min(o + piece, total);
-#pragma omp parallel for schedule(static) if (k1 - (long long)o > (1 << 16))
+#pragma omp parallel for schedule(static) if (k1 - (long long)o >= (1 << 12))
       for (long long k = (long long)o; k < k1; k++) {
         double* f = k < np ? req.fock : req.fock_b;  // indices are unique: no two threads add to one entry
         f[ix[k < np ? k : k - np]] += d->hK[k];

@@ -87,24 +87,33 @@ struct RadialSource {
   double dnorm;
   int nr;
 };
-// the per-function constants of that product (function i of group G, i < m)
+// the per-function constants of that product (function i of group G, i < m):
+// the monomial as up to two axes (x, y or z; -1 for none), the atom's
+// coordinates along them, and the d normalisation. P = (r_1)(r_2) is the
+// product k_basis forms (its factors of 1.0 are exact), so F is the same value.
 struct RadialRow {
-  double ax, ay, az, scale;
-  int lx, ly, lz, sh;
+  double a1, a2, scale;
+  int i1, i2, sh;
   __device__ __forceinline__ void load(const RadialSource& rs, const GroupDev& G, int i) {
     const int cp = rs.fn_cp[G.fn_off + i], c = cp & 15, atom = rs.fn_atom[G.fn_off + i];
-    lx = c_comp_l[c][0];
-    ly = c_comp_l[c][1];
-    lz = c_comp_l[c][2];
+    const double at[3] = {rs.ax[atom], rs.ay[atom], rs.az[atom]};
+    i1 = i2 = -1;
+    for (int k = 0; k < 3; k++)
+      for (int e = 0; e < c_comp_l[c][k]; e++) {
+        if (i1 < 0)
+          i1 = k;
+        else
+          i2 = k;
+      }
+    a1 = i1 >= 0 ? at[i1] : 0.0;
+    a2 = i2 >= 0 ? at[i2] : 0.0;
     scale = (cp & 16) ? rs.dnorm : 1.0;
-    ax = rs.ax[atom];
-    ay = rs.ay[atom];
-    az = rs.az[atom];
     sh = rs.fn_sh[G.fn_off + i];
   }
   __device__ __forceinline__ double value(double x, double y, double z, double t) const {
-    const double P = ipow(x - ax, lx) * ipow(y - ay, ly) * ipow(z - az, lz);
-    return scale * P * t;
+    const double p1 = i1 < 0 ? 1.0 : (i1 == 0 ? x : (i1 == 1 ? y : z)) - a1;
+    const double p2 = i2 < 0 ? 1.0 : (i2 == 0 ? x : (i2 == 1 ? y : z)) - a2;
+    return scale * (p1 * p2) * t;
   }
 };
 
