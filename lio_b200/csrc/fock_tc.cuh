@@ -96,17 +96,13 @@ struct RadialRow {
   int i1, i2, sh;
   __device__ __forceinline__ void load(const RadialSource& rs, const GroupDev& G, int i) {
     const int cp = rs.fn_cp[G.fn_off + i], c = cp & 15, atom = rs.fn_atom[G.fn_off + i];
-    const double at[3] = {rs.ax[atom], rs.ay[atom], rs.az[atom]};
-    i1 = i2 = -1;
-    for (int k = 0; k < 3; k++)
-      for (int e = 0; e < c_comp_l[c][k]; e++) {
-        if (i1 < 0)
-          i1 = k;
-        else
-          i2 = k;
-      }
-    a1 = i1 >= 0 ? at[i1] : 0.0;
-    a2 = i2 >= 0 ? at[i2] : 0.0;
+    const double ax = rs.ax[atom], ay = rs.ay[atom], az = rs.az[atom];
+    const int lx = c_comp_l[c][0], ly = c_comp_l[c][1], lz = c_comp_l[c][2];
+    // the first and second axis of x^lx y^ly z^lz (lx + ly + lz <= 2)
+    i1 = lx > 0 ? 0 : (ly > 0 ? 1 : (lz > 0 ? 2 : -1));
+    i2 = lx == 2 ? 0 : (lx + ly == 2 ? 1 : (lx + ly + lz == 2 ? 2 : -1));
+    a1 = i1 == 0 ? ax : (i1 == 1 ? ay : az);
+    a2 = i2 == 0 ? ax : (i2 == 1 ? ay : az);
     scale = (cp & 16) ? rs.dnorm : 1.0;
     sh = rs.fn_sh[G.fn_off + i];
   }
@@ -145,12 +141,22 @@ __global__ void k_fock_rowexp(const int2* __restrict__ rows, int nrows, const Gr
       if constexpr (RAD) {
         const double* tr = rs.rad + G.rad_off + ((long long)(T * G.nsimple + rr.sh) * rs.nr) * kTcPoints + lane * 4;
         const double2 t01 = *reinterpret_cast<const double2*>(tr), t23 = *reinterpret_cast<const double2*>(tr + 2);
+        // only the coordinates along the monomial's axes (the row's, one per warp)
         const long long q = G.pt_off + p;
-        const double2 x01 = *reinterpret_cast<const double2*>(rs.px + q), x23 = *reinterpret_cast<const double2*>(rs.px + q + 2);
-        const double2 y01 = *reinterpret_cast<const double2*>(rs.py + q), y23 = *reinterpret_cast<const double2*>(rs.py + q + 2);
-        const double2 z01 = *reinterpret_cast<const double2*>(rs.pz + q), z23 = *reinterpret_cast<const double2*>(rs.pz + q + 2);
-        v01 = make_double2(rr.value(x01.x, y01.x, z01.x, t01.x), rr.value(x01.y, y01.y, z01.y, t01.y));
-        v23 = make_double2(rr.value(x23.x, y23.x, z23.x, t23.x), rr.value(x23.y, y23.y, z23.y, t23.y));
+        double f1[4] = {1.0, 1.0, 1.0, 1.0}, f2[4] = {1.0, 1.0, 1.0, 1.0};
+        auto axis = [&](int ax, double a, double (&f)[4]) {
+          const double* c = (ax == 0 ? rs.px : (ax == 1 ? rs.py : rs.pz)) + q;
+          const double2 c01 = *reinterpret_cast<const double2*>(c), c23 = *reinterpret_cast<const double2*>(c + 2);
+          f[0] = c01.x - a;
+          f[1] = c01.y - a;
+          f[2] = c23.x - a;
+          f[3] = c23.y - a;
+        };
+        if (rr.i1 >= 0) axis(rr.i1, rr.a1, f1);
+        if (rr.i2 >= 0) axis(rr.i2, rr.a2, f2);
+        // scale (r_1 r_2) t, as RadialRow::value
+        v01 = make_double2(rr.scale * (f1[0] * f2[0]) * t01.x, rr.scale * (f1[1] * f2[1]) * t01.y);
+        v23 = make_double2(rr.scale * (f1[2] * f2[2]) * t23.x, rr.scale * (f1[3] * f2[3]) * t23.y);
       } else {
         const double* Fi = f_row(G, basis, i, p, nkb);
         v01 = *reinterpret_cast<const double2*>(Fi);
