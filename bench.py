@@ -196,6 +196,10 @@ def stage_times(L, steps: int):
 # launch's traffic is estimated as that ratio times its own algorithmic bytes
 # (the same byte classes grow with the same partition sums).
 SMALL_CASE_TRAFFIC_RATIO = 1.731 / 1.2851
+# The same for k_fock_tc: on the 64-atom open-shell case (ncu --set full on one
+# launch) it moved 0.879 GB (0.872 read + 0.007 written) against the 0.482 GB
+# of its model (A slices re-read once per 32-column tile, 27 % of them from L2).
+KS_SMALL_CASE_TRAFFIC_RATIO = 0.8786 / 0.4819
 FP64_PEAK_NOMINAL = 37.0e12  # FLOP/s, the B200's nominal FP64 rate (no measured figure exists for it)
 
 
@@ -443,6 +447,7 @@ def ours(args, rank, world):
     if tc and t_ks > 0:
         ks_ops = 21.0 * ks["flops"]
         ks_roof["int8_frac"] = ks_ops / t_ks / 1e12 / (2.0 * bf16)
+        ks_roof["traffic"] = KS_SMALL_CASE_TRAFFIC_RATIO * ks["bytes"]
     result = {
         "metric": METRIC, "value": total_pts / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
