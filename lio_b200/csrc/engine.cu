@@ -1235,13 +1235,43 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
   std::vector<int> src_group;  // partition group of each device group
   std::vector<long long> src_off;
   long long np_pad = 0;
+  // sizes of the lists built below, so that each is allocated once
+  size_t n_fn = 0, n_sf = 0, n_t128 = 0, n_t128f = 0, n_ftc = 0, n_dt = 0, n_kt = 0, n_fa = 0, n_fb = 0, n_fk = 0;
   for (int g = 0; g < ngr; g++) {
     if (keep && !(*keep)[g]) continue;  // another rank's group
-    const int npts = (int)part.group(g).points.size();
+    const PointGroup& pg = part.group(g);
+    const int npts = (int)pg.points.size(), ldp = ((npts + kPointPad - 1) / kPointPad) * kPointPad;
+    const int m = pg.total_functions(), nft = (m + kTile - 1) / kTile, nftc = (m + kTcFuncs - 1) / kTcFuncs;
+    const int nI = (m + kFkRows - 1) / kFkRows, nJ = (m + kFkCols - 1) / kFkCols;
     src_group.push_back(g);
     src_off.push_back(np_pad);
-    np_pad += ((npts + kPointPad - 1) / kPointPad) * kPointPad;
+    np_pad += ldp;
+    n_fn += m;
+    n_sf += pg.funcs.size();
+    n_t128 += ldp / kTcPoints;
+    n_t128f += (size_t)(ldp / kTcPoints) * nftc;
+    n_ftc += nftc;
+    n_dt += (size_t)(ldp / kTile) * nft;
+    n_kt += (size_t)nft * (nft + 1) / 2;
+    n_fa += (size_t)nI * kFkRows;
+    n_fb += (size_t)nJ * kFkCols;
+    n_fk += (size_t)nI * nJ;
   }
+  for (auto* v : {&hfn, &hfsh, &hfat}) v->reserve(n_fn);
+  hfcp.reserve(n_fn);
+  for (auto* v : {&hsf, &hst, &hsffn}) v->reserve(n_sf);
+  farows.reserve(n_fa);
+  fat32.reserve(n_fa / 32 + 1);
+  fbrows.reserve(n_fb);
+  fktiles.reserve(n_fk);
+  frtiles.reserve(n_t128f * (sys.open ? 2 : 1));
+  sbtiles.reserve(n_t128);
+  sdtiles.reserve(n_ftc);
+  dtiles.reserve(n_dt);
+  ktiles.reserve(n_kt);
+  btiles.reserve(n_t128 * kTcPoints / kBasisBlock + src_group.size());
+  ftiles.reserve(n_t128 * kTcPoints / kFuncBlock + src_group.size());
+  gd.reserve(src_group.size());
   PinnedStaging& ps = point_staging();
   std::lock_guard<std::mutex> ps_lock(ps.m);  // one upload at a time: held to the end of this upload
   ps.reserve(4 * (size_t)std::max(np_pad, 1LL) * sizeof(double));

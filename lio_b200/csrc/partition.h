@@ -12,6 +12,11 @@ namespace lio {
 struct GridPoint {
   int atom, shell, point;
   double x, y, z, w;
+  // no zeroing when a point array is sized before it is filled (the grid build
+  // places every point of a geometry, ~140 MB at 256 atoms, into sized arrays)
+  GridPoint() {}
+  GridPoint(int a, int s, int p, double x_, double y_, double z_, double w_)
+      : atom(a), shell(s), point(p), x(x_), y(y_), z(z_), w(w_) {}
 };
 
 struct PointGroup {
