@@ -1385,7 +1385,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
     aexp_off += (long long)NA * G.ldp;
     ds_off += (long long)G.nftc * (G.m32 / 32) * kTcStepD;
     dexp_off += (long long)G.nftc * kTcFuncs;
-    fa_off += (long long)nI * kSlices * kFkRows * G.ldp;
+    for (int I = 0; I < nI; I++) fa_off += (long long)kSlices * fk_tile_rows(G.m, I) * G.ldp;
     fae_off += (long long)nI * kFkRows;
     fbe_off += (long long)nJ * kFkCols;
     rad_off += (long long)G.ldp * G.nsimple * NR;
@@ -1981,7 +1981,7 @@ size_t DeviceEngine::estimate_device_bytes(const System& sys, const Partition& p
     if (prec == Precision::TensorCore)
       b += ldp * ((double)nftc * kTcFuncs * (sys.lda ? 1 : 4) * 8 + (double)pg.funcs.size() * (sys.lda ? 1 : 3) * 8 +
                   (double)na * m32 * kSlices + na * 2 +
-                  (double)nI * kFkRows * kSlices) +
+                  (double)(nI > 0 ? (nI - 1) * kFkRows + fk_tile_rows(m, nI - 1) : 0) * kSlices) +
            (double)nspin * nftc * m32 * kTcTall;
   }
   return (size_t)(b * 1.05) + (16u << 20);

@@ -51,6 +51,17 @@ struct FkCfg {
   static constexpr int kThreads = 32 * (kSlicers + 2);
 };
 static_assert(FkCfg<2>::kSmem <= 227 * 1024, "shared memory of the Kohn-Sham kernel");
+
+// Rows of the A operand kept for 128-row tile I of a group of m functions:
+// whole tiles 128, the last its functions rounded up to a core matrix (8 rows).
+// The MMA still reads 128 rows (M = 128); with the shorter leading-dimension
+// offset of the stored rows, rows past them read the next bytes of the same
+// stage (the other K half, the next slice, the stage's B block), which feed
+// only TMEM lanes of functions past m, never read out.
+__host__ __device__ __forceinline__ int fk_tile_rows(int m, int I) {
+  const int left = m - I * kFkRows;
+  return left >= kFkRows ? kFkRows : ((left + 7) / 8) * 8;
+}
 static_assert(FkCfg<1>::kSlot % 128 == 0 && FkCfg<2>::kSlot % 128 == 0 && FkCfg<2>::kStage % 128 == 0,
               "ring slots and stages stay 128-byte aligned");
 
@@ -204,6 +215,8 @@ __global__ void __launch_bounds__(256) k_fock_aslices(const int2* __restrict__ r
   const bool valid = i < G.m;
   const double s42 = digit_scale(expo[G.fae_off + i]);
   const int tile = i / kFkRows, r = i % kFkRows;
+  const int R = fk_tile_rows(G.m, tile);  // rows stored for this tile
+  if (r >= R) return;                     // past them: not stored (no shuffles below)
   for (int b = warp; b < ldp / 16; b += blockDim.x / 32) {
     const int p0 = b * 16;
     const double* Fi = f_row(G, basis, valid ? i : 0, p0, nkb);  // 16 values within one 128-point tile
@@ -214,7 +227,7 @@ __global__ void __launch_bounds__(256) k_fock_aslices(const int2* __restrict__ r
       digits_m(v.x, s42, lo[k], hi[k]);
       digits_m(v.y, s42, lo[k + 1], hi[k + 1]);
     }
-    int8_t* blk = sl + G.fa_off + ((long long)tile * nkp + (p0 >> 5)) * kFkStepA;
+    int8_t* blk = sl + G.fa_off + (long long)tile * nkp * kFkStepA + (long long)(p0 >> 5) * kSlices * 32 * R;
 #pragma unroll
     for (int s = 0; s < kSlices; s++) {
       uint32_t w[4];
@@ -223,7 +236,7 @@ __global__ void __launch_bounds__(256) k_fock_aslices(const int2* __restrict__ r
         w[k4] = pack_digits(digit_field(lo[4 * k4], hi[4 * k4], s), digit_field(lo[4 * k4 + 1], hi[4 * k4 + 1], s),
                             digit_field(lo[4 * k4 + 2], hi[4 * k4 + 2], s),
                             digit_field(lo[4 * k4 + 3], hi[4 * k4 + 3], s), s == 0);
-      *reinterpret_cast<uint4*>(blk + s * kFkSliceA + lio::umma::kmajor_offset(r, p0 & 31, kFkRows)) =
+      *reinterpret_cast<uint4*>(blk + s * 32 * R + lio::umma::kmajor_offset(r, p0 & 31, R)) =
           make_uint4(w[0], w[1], w[2], w[3]);
     }
   }
@@ -287,6 +300,7 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
   if (warp == Cfg::kProd) {
     if (lane == 0) {
       const int8_t* A = aslices + G.fa_off + (long long)I * nsteps * kFkStepA;
+      const int stepA = kSlices * 32 * fk_tile_rows(G.m, I);  // A bytes of a K step
       const int rows = min(kFkCols, G.m - J * kFkCols);  // rows of J that exist (from row 0 of the chunk)
       // RAD: the shells of those rows (consecutive), one radial row each
       const int sh0 = RAD ? rs.fn_sh[G.fn_off + J * kFkCols] : 0;
@@ -327,8 +341,8 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
           *vfail = 1;
           break;
         }
-        lio::umma::mbar_expect_tx(&afull[buf], (uint32_t)kFkStepA);
-        lio::umma::bulk_copy_g2s(fk_smem + buf * Cfg::kStage, A + (long long)st * kFkStepA, kFkStepA, &afull[buf]);
+        lio::umma::mbar_expect_tx(&afull[buf], (uint32_t)stepA);
+        lio::umma::bulk_copy_g2s(fk_smem + buf * Cfg::kStage, A + (long long)st * stepA, stepA, &afull[buf]);
         na = st + 1;
       }
       // copies in flight land before the CTA exits (each is the latest phase of its barrier)
@@ -340,6 +354,7 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
   } else if (warp == Cfg::kMma) {
     if (lane == 0) {
       const uint32_t smem0 = lio::umma::smem_u32(fk_smem);
+      const uint32_t R = (uint32_t)fk_tile_rows(G.m, I);  // A rows stored per K half
       for (int st = 0; st < nsteps; st++) {
         const int buf = st % kFkStages, use = st / kFkStages;
         if (*vfail || !lio::umma::mbar_wait(&afull[buf], use & 1) || !lio::umma::mbar_wait(&bready[buf], use & 1)) {
@@ -353,7 +368,7 @@ __global__ void __launch_bounds__(FkCfg<NS>::kThreads, 1)
         // MMAs of slice 0 (levels 0 .. S-1, disjoint columns) write every column first.
 #pragma unroll
         for (int s = 0; s < kSlices; s++) {
-          const uint64_t ad = lio::umma::smem_desc(sa + s * kFkSliceA, 16u * kFkRows, 128u);
+          const uint64_t ad = lio::umma::smem_desc(sa + s * 32u * R, 16u * R, 128u);
 #pragma unroll
           for (int t0 = 0; t0 < kSlices - s; t0 += Cfg::kMaxLevels) {
             const int nl = min(Cfg::kMaxLevels, kSlices - s - t0);
