@@ -1966,7 +1966,7 @@ size_t DeviceEngine::estimate_blocked_basis_bytes(const System& sys, const Parti
   return (size_t)b;
 }
 
-size_t DeviceEngine::estimate_device_bytes(const System& sys, const Partition& part, Precision prec) {
+size_t DeviceEngine::estimate_device_bytes(const System& sys, const Partition& part, Precision prec, bool lean) {
   const int nk = sys.lda ? 1 : 10, na = sys.lda ? 1 : 4, nq = sys.lda ? 1 : kNQ, nspin = sys.open ? 2 : 1;
   const size_t npacked = (size_t)sys.M * (sys.M + 1) / 2;
   double b = (double)npacked * 8 * 2 * nspin;  // densities and Kohn-Sham accumulators
@@ -1979,7 +1979,8 @@ size_t DeviceEngine::estimate_device_bytes(const System& sys, const Partition& p
     b += ldp * (6 * 8 + nspin * (nq * (double)nft * 8 + 8));  // points, partials, factors
     if (prec == Precision::FP64) b += ldp * nk * (double)m * 8;  // function-major basis cache
     if (prec == Precision::TensorCore)
-      b += ldp * ((double)nftc * kTcFuncs * (sys.lda ? 1 : 4) * 8 + (double)pg.funcs.size() * (sys.lda ? 1 : 3) * 8 +
+      b += ldp * ((lean ? 0.0 : (double)nftc * kTcFuncs * (sys.lda ? 1 : 4) * 8) +  // blocked basis
+                  (double)pg.funcs.size() * (sys.lda ? 1 : 3) * 8 +
                   (double)na * m32 * kSlices + na * 2 +
                   (double)(nI > 0 ? (nI - 1) * kFkRows + fk_tile_rows(m, nI - 1) : 0) * kSlices) +
            (double)nspin * nftc * m32 * kTcTall;

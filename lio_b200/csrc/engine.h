@@ -158,7 +158,8 @@ class DeviceEngine {
   // device bytes held by all engines of the process, and an estimate of one
   // molecule's footprint before it is uploaded
   static long long process_device_bytes();
-  static size_t estimate_device_bytes(const System& sys, const Partition& part, Precision prec);
+  // (lean: without the blocked basis, which a lean engine keeps only while it builds its operands)
+  static size_t estimate_device_bytes(const System& sys, const Partition& part, Precision prec, bool lean = false);
   // lean: once the tensor-core operands are built the blocked FP64 basis is
   // released (about a third of the form's footprint for GGA); the Kohn-Sham
   // kernels then form F from the radial sums, and forces rebuild the blocked

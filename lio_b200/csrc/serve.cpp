@@ -163,19 +163,21 @@ bool lio_server::plan_load(int mi, std::string& why) {
   // the two, held one after the other while both are timed); a cold molecule
   // needs its caches back only
   // Engines are lean: a tensor-core molecule holds its blocked basis only while
-  // its operands are built, so a (re)load of one books that room as well (the
-  // booking is replaced by the measured footprint once it is resident).
-  const bool tc_form = autotune ? m.form == 1 : precision == lio::Precision::TensorCore;
+  // its operands are built, so every load that may build them books that room
+  // as well (the booking is replaced by the measured footprint once resident).
+  const bool may_tc = autotune ? m.form != 0 : precision == lio::Precision::TensorCore;
   const unsigned long long transient =
-      (m.engine || m.measured) && tc_form ? lio::DeviceEngine::estimate_blocked_basis_bytes(m.sys, m.part) : 0;
-  const unsigned long long need =
-      transient +
+      may_tc ? lio::DeviceEngine::estimate_blocked_basis_bytes(m.sys, m.part) : 0;
+  const unsigned long long resident_need =
       (m.engine ? m.footprint - m.core
        : m.measured ? m.footprint
        : autotune ? (unsigned long long)std::max(
-                        lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, lio::Precision::FP64),
-                        lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, lio::Precision::TensorCore))
-                  : (unsigned long long)lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, precision));
+                        lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, lio::Precision::FP64, true),
+                        lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, lio::Precision::TensorCore, true))
+                  : (unsigned long long)lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, precision, true));
+  // a molecule that fits the budget only without its transient books what it
+  // keeps (a load that then runs out of device memory is retried as below)
+  const unsigned long long need = resident_need + transient > budget ? resident_need : resident_need + transient;
   // Eviction in two levels, least recently used idle molecules first: their
   // caches (the bulk of a footprint; they go cold and keep their grid), and only
   // if that cannot make room, whole molecules (hot or cold).
@@ -581,7 +583,7 @@ int lio_srv_molecule_info(lio_server* srv, int mol, long long* points, unsigned 
   if (points) *points = m.points;
   if (footprint)
     *footprint = m.measured ? m.footprint
-                            : (unsigned long long)lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, srv->precision);
+                            : (unsigned long long)lio::DeviceEngine::estimate_device_bytes(m.sys, m.part, srv->precision, true);
   if (resident) *resident = m.engine && !m.cold ? 1 : 0;
   return 0;
 }
