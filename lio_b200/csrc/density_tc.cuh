@@ -366,6 +366,16 @@ struct ShellSums {
   }
 };
 
+// A shell of a group as the density epilogue reads it, one 32-byte record per
+// (group, shell), written per geometry: its atom's position, its type (0 s, 1 p,
+// 2 d) and the group-local column of its first component. One load per shell
+// instead of a chain through the shell's function, its atom and the positions.
+struct ShellInfo {
+  double x, y, z;
+  int type, fcol;
+};
+static_assert(sizeof(ShellInfo) == 32, "one 32-byte record per shell");
+
 // A shell at this thread's point: displacement from its atom and radial sums.
 struct ShellPoint {
   double r[3], t, tg2, th4;
@@ -498,9 +508,7 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
                  const int8_t* __restrict__ dsl_a, const int16_t* __restrict__ dexp_a,
                  const int8_t* __restrict__ dsl_b, const int16_t* __restrict__ dexp_b, int fcap,
                  const double* __restrict__ px, const double* __restrict__ py, const double* __restrict__ pz,
-                 const int* __restrict__ fn_sh, const int* __restrict__ sf_glob, const int* __restrict__ sf_type,
-                 const int* __restrict__ sf_fn, const int* __restrict__ nuc, const double* __restrict__ ax,
-                 const double* __restrict__ ay, const double* __restrict__ az, const double* __restrict__ rad,
+                 const int* __restrict__ fn_sh, const ShellInfo* __restrict__ sinfo, const double* __restrict__ rad,
                  double dnorm, double* __restrict__ part_a, double* __restrict__ part_b, int* __restrict__ err) {
   using Cfg = TcCfg<GGA, NS>;
   constexpr int KP = Cfg::KP, NP = Cfg::NP, NA = Cfg::NA, NQ = Cfg::NQ, NR = Cfg::NR, CPW = kTcCpw;
@@ -674,13 +682,12 @@ __global__ void __launch_bounds__(TcCfg<GGA, NS>::kThreads, 1)
           sh_a = fsh[w0];
           nsl = fsh[w0 + wlen - 1] - sh_a + 1;  // <= 16: one shell per function at most
           if (lane < nsl) {
-            const int sh = sh_a + lane;
-            const int atom = nuc[sf_glob[G.sf_off + sh]];
-            s_ax = ax[atom];
-            s_ay = ay[atom];
-            s_az = az[atom];
-            s_type = sf_type[G.sf_off + sh];
-            s_fcol = sf_fn[G.sf_off + sh] - w0;  // first component's column in the window (may be < 0)
+            const ShellInfo si = sinfo[G.sf_off + sh_a + lane];
+            s_ax = si.x;
+            s_ay = si.y;
+            s_az = si.z;
+            s_type = si.type;
+            s_fcol = si.fcol - w0;  // first component's column in the window (may be < 0)
           }
           // their radial sums at this thread's point, copied while the unit's MMAs run
           for (int s2 = 0; s2 < nsl; s2++)

@@ -862,6 +862,7 @@ struct DeviceEngine::Impl {
   DevBuf<double> px, py, pz, pw;
   DevBuf<int> fn_glob, sf_glob, sf_type, nuc, ncont, fn_sh, fn_atom;
   DevBuf<int> sf_fn;  // per simple function (shell) of a group: the local index of its first component
+  DevBuf<ShellInfo> sinfo;  // per (group, shell): atom position, type, first column (density epilogue)
   DevBuf<double> rad;  // radial sums per (tile, shell, point) of the tensor-core density
   long long rad_elems = 0;
   DevBuf<int8_t> fn_cp;
@@ -1211,6 +1212,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
 
   std::vector<GroupDev> gd;
   std::vector<int> hfn, hsf, hst, hfsh, hfat, hsffn;
+  std::vector<ShellInfo> hsinfo;
   std::vector<int8_t> hfcp;
   std::vector<int2> btiles, ftiles, sbtiles, sdtiles;
   std::vector<int4> dtiles, ktiles, tctiles;
@@ -1260,6 +1262,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
   for (auto* v : {&hfn, &hfsh, &hfat}) v->reserve(n_fn);
   hfcp.reserve(n_fn);
   for (auto* v : {&hsf, &hst, &hsffn}) v->reserve(n_sf);
+  hsinfo.reserve(n_sf);
   farows.reserve(n_fa);
   fat32.reserve(n_fa / 32 + 1);
   fbrows.reserve(n_fb);
@@ -1350,6 +1353,8 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
       hsf.push_back(f);
       hst.push_back(type);
       hsffn.push_back((int)((long long)hfn.size() - G.fn_off));
+      hsinfo.push_back(ShellInfo{sys.ax[sys.nuc[f]], sys.ay[sys.nuc[f]], sys.az[sys.nuc[f]], type,
+                                 (int)((long long)hfn.size() - G.fn_off)});
       const int ncomp = type == 0 ? 1 : (type == 1 ? 3 : 6);
       const int c0 = type == 0 ? 0 : (type == 1 ? 1 : 4);
       for (int k = 0; k < ncomp; k++) {
@@ -1436,6 +1441,7 @@ void DeviceEngine::upload(const System& sys, const Partition& part, const std::v
   d->sf_glob.upload(hsf);
   d->sf_type.upload(hst);
   d->sf_fn.upload(hsffn);
+  d->sinfo.upload(hsinfo);
   d->rad_elems = rad_off;
   d->nuc.upload(hnuc);
   d->ncont.upload(hnc);
@@ -1709,8 +1715,8 @@ int DeviceEngine::run_kernels(bool compute_rmm, bool ext) {
 #define LIO_DENSITY_TC(GGA, NS)                                                                                    \
   k_density_tc<GGA, NS><<<nt, TcCfg<GGA, NS>::kThreads, TcCfg<GGA, NS>::smem(cap), st>>>(                          \
       d->dens_tc_tiles.p, ntiles, d->groups.p, d->aslices.p, d->aexp.p, d->dslices_a.p, d->dexp_a.p,               \
-      d->dslices_b.p, d->dexp_b.p, cap, d->px.p, d->py.p, d->pz.p, d->fn_sh.p, d->sf_glob.p, d->sf_type.p,            \
-      d->sf_fn.p, d->nuc.p, d->ax.p, d->ay.p, d->az.p, d->rad.p, d->basis_norm, d->part_a.p, d->part_b.p, d->tc_err.p)
+      d->dslices_b.p, d->dexp_b.p, cap, d->px.p, d->py.p, d->pz.p, d->fn_sh.p, d->sinfo.p, d->rad.p, d->basis_norm,    \
+      d->part_a.p, d->part_b.p, d->tc_err.p)
     if (d->lda) {
       if (d->open) LIO_DENSITY_TC(false, 2); else LIO_DENSITY_TC(false, 1);
     } else {
